@@ -1,0 +1,332 @@
+/*
+ * traceon_b200.h -- C ABI of libtraceon_b200.so, the B200 (sm_100a) CUDA
+ * implementation of Traceon's radially symmetric BEM path.
+ *
+ * Two families of entry points:
+ *
+ *  1. Reference-compatible entry points.  Same names, argument order and
+ *     meaning as the functions the reference binds with ctypes in its
+ *     `backend_functions` table (traceon/backend/__init__.py:287-328).  They
+ *     take HOST pointers exactly like the reference C backend, copy to the
+ *     device, run the CUDA kernels and copy back, so that a maintainer can
+ *     point `backend_lib = C.CDLL(...)` at this library.  Where the reference
+ *     would call exit(1) or assert, these leave outputs untouched and record a
+ *     status readable with tb_last_status().  Scalar geometry helpers
+ *     (elliptic integrals, element points, normals, single ring kernels) are
+ *     evaluated on the host by the same __host__ __device__ code the kernels
+ *     use; all array work runs on the GPU.
+ *
+ *  2. Batched device entry points (prefix tb_).  All pointers are DEVICE
+ *     pointers (e.g. torch.Tensor.data_ptr()), work is enqueued on `stream`,
+ *     and every function returns a status code (TB_OK on success).  Nothing
+ *     here allocates device memory unless its comment says so.
+ *
+ * Array layouts (row-major, FP64 unless noted), N = number of line elements:
+ *   vertices  (N, 4, 3)  line4 rows [start, end, 1/3-point, 2/3-point], (r, 0, z)
+ *   jac       (N, 16)    Gauss weight x |dx/dalpha|
+ *   pos       (N, 16, 2) (r, z) of the Gauss nodes
+ *   charges   (N,)       surface charge / eps0 (the reference's unit)
+ *   sources   (3, Nq)    packed rings for field sums: r[Nq], z[Nq], w[Nq],
+ *                        w = charge * jac, Nq = 16 N (tb_pack_sources)
+ */
+#ifndef TRACEON_B200_H
+#define TRACEON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *tb_stream_t;
+
+/* status codes */
+#define TB_OK 0
+#define TB_BAD_ARG 1
+#define TB_CUDA_ERR 2
+#define TB_NONFINITE 3
+#define TB_UNSUPPORTED 4
+#define TB_SINGULAR 5
+
+/* per-particle tracer status */
+#define TB_TRACE_EXITED 0
+#define TB_TRACE_MAX_ATTEMPTS 1
+#define TB_TRACE_ROWS_FULL 2
+#define TB_TRACE_NONFINITE 3
+
+/* ======================================================================
+ * 1. Reference-compatible entry points (host pointers)
+ * ====================================================================== */
+
+/* Compile-time constants read with ctypes in_dll
+ * (traceon/backend/__init__.py:58-66). */
+extern const size_t TRACING_BLOCK_SIZE;   /* 100000, tracing.c:7 */
+extern const int DERIV_2D_MAX_SYM;        /* 9, radial_ring.c:2 / utilities_2d.c */
+extern const int N_QUAD_2D_SYM;           /* 16, utilities_2d.c:2 */
+extern const int N_TRIANGLE_QUAD_SYM;     /* 12, utilities_3d.c */
+extern const int NU_MAX_SYM;              /* 4, three_d.c:4 */
+extern const int M_MAX_SYM;               /* 8, three_d.c:5 */
+
+/* Status of the last reference-compatible call on this thread (TB_OK,
+ * TB_BAD_ARG, TB_CUDA_ERR, TB_UNSUPPORTED).  No reference counterpart: the
+ * reference reports errors by exit(1) (radial.c:305-308). */
+int tb_last_status(void);
+
+/* Elliptic integrals, replaces elliptic.c:9-75 (host scalar). */
+double ellipkm1(double p);
+double ellipk(double k);
+double ellipem1(double p);
+double ellipe(double k);
+
+/* Replaces utilities_2d.c:18-29 normal_2d (host scalar). */
+void normal_2d(const double *p1, const double *p2, double *normal);
+/* Replaces utilities_2d.c:31-48; called with rows v[0], v[2], v[3], v[1]
+ * (traceon/backend/__init__.py:373-377). */
+void higher_order_normal_radial(double alpha, const double *v1, const double *v2, const double *v3,
+                                const double *v4, double *normal);
+/* Replace utilities_2d.c:50-66 and :68-87 (host scalar). */
+void position_and_jacobian_radial(double alpha, const double *v1, const double *v2, const double *v3,
+                                  const double *v4, double *pos, double *jac);
+void delta_position_and_jacobian_radial(double alpha, const double *v1, const double *v2, const double *v3,
+                                        const double *v4, double *pos, double *jac);
+
+/* Ring kernels, replace radial_ring.c:21-53 (host scalar; the trailing
+ * void* is ignored as in the reference). */
+double potential_radial_ring(double r0, double z0, double delta_r, double delta_z, void *unused);
+double dr1_potential_radial_ring(double r0, double z0, double delta_r, double delta_z, void *unused);
+double dz1_potential_radial_ring(double r0, double z0, double delta_r, double delta_z, void *unused);
+/* Replaces utilities_2d.c:91-105. */
+double flux_density_to_charge_factor(double K);
+/* Replaces radial.c:123-148 (host scalar). */
+double charge_radial(const double *vertices, double charge);
+/* Replaces radial_ring.c:78-107 (host scalar). */
+void current_field_radial_ring(double x0, double y0, double x, double y, double *result);
+/* Replaces radial_ring.c:73-76 (host scalar). */
+double current_potential_axial_radial_ring(double z0, double r, double z);
+
+/* Self-integrands for SciPy LowLevelCallable (radial.c:182-196, :203-222).
+ * Host scalar; the solver of this library does not use them -- its
+ * diagonal is integrated on the GPU (tb_self_integrals). */
+double self_potential_radial(double alpha, void *line_points);
+double self_field_dot_normal_radial(double alpha, void *args);
+
+/* GPU: replaces radial.c:224-246 fill_jacobian_buffer_radial. */
+void fill_jacobian_buffer_radial(double *jac, double *pos, const double *vertices, size_t N_lines);
+
+/* GPU: replaces radial.c:249-310 fill_matrix_radial.  Accumulates (+=) rows
+ * [start, end] of `matrix` (row stride N_matrix) exactly like the reference,
+ * including its 16-point Gauss diagonal that the solver later overwrites.
+ * Unknown excitation types leave the matrix unchanged and set TB_BAD_ARG. */
+void fill_matrix_radial(double *matrix, const double *lines, const uint8_t *types, const double *values,
+                        const double *jac, const double *pos, size_t N_lines, size_t N_matrix, int start,
+                        int end);
+
+/* GPU: replace radial.c:105-121 and :150-173 (one point per call). */
+double potential_radial(const double *point, const double *charges, const double *jac, const double *pos,
+                        size_t N);
+void field_radial(const double *point, double *result, const double *charges, const double *jac,
+                  const double *pos, size_t N);
+/* GPU: replaces radial.c:18-36 (accumulates into derivs (N_z, 9)). */
+void axial_derivatives_radial(double *derivs, const double *charges, const double *jac, const double *pos,
+                              size_t N, const double *z, size_t N_z);
+/* GPU: replaces radial.c:55-83 (positions (N, 12, 3)). */
+void current_field_radial(const double *point, double *result, const double *currents, const double *jac,
+                          const double *pos, size_t N);
+/* GPU: replaces radial.c:85-103 (accumulates). */
+void current_axial_derivatives_radial(double *derivs, const double *currents, const double *jac,
+                                      const double *pos, size_t N, const double *z, size_t N_z);
+/* GPU: replaces radial.c:38-53. */
+double current_potential_axial(double z0, const double *currents, const double *jac, const double *pos,
+                               size_t N);
+/* Replace radial.c:312-344 and :347-384 (host scalar: O(1) table lookup). */
+double potential_radial_derivs(const double *point, const double *z, const double *coeffs, size_t N_z);
+void field_radial_derivs(const double *point, double *field, const double *z, const double *coeffs,
+                         size_t N_z);
+
+/* Field callbacks of the tracer, tracing.c:125-174 (field_fun type,
+ * traceon/backend/__init__.py:89).  field_radial_traceable evaluates the BEM
+ * sums on the GPU; field_radial_derivs_traceable is a host table lookup. */
+void field_radial_traceable(const double *position, const double *velocity, void *args, double *elec_out,
+                            double *mag_out);
+void field_radial_derivs_traceable(const double *position, const double *velocity, void *args,
+                                   double *elec_out, double *mag_out);
+
+/* GPU: replaces tracing.c:60-123 trace_particle.  `field` must be one of
+ * this library's field_radial_traceable / field_radial_derivs_traceable
+ * (with the matching args struct, radial.c:175-180 / three_d.c:26-31); the
+ * whole trajectory is then integrated on the GPU.  Any other callback sets
+ * TB_UNSUPPORTED and returns 1 (only the start row).  Writes at most
+ * TRACING_BLOCK_SIZE rows and returns the row count, like the reference. */
+size_t trace_particle(double *times, double *positions, double charge_over_mass, void *field,
+                      const double *bounds, double atol, void *args);
+
+/* Replaces tracing.c:184-223 (host: linear crossing on a host trajectory). */
+bool plane_intersection(const double *p0, const double *normal, const double *positions, size_t N_p,
+                        double *result);
+
+/* Reference entry points outside the radial path (3D geometry, the
+ * kronrod_adaptive test helper).  Exported so the reference's import-time
+ * getattr loop (traceon/backend/__init__.py:341-352) succeeds; calling them
+ * sets TB_UNSUPPORTED and leaves outputs untouched. */
+double kronrod_adaptive(void *f, double a, double b, void *args, double abs_tol, double rel_tol);
+void normal_3d(const double *points, double *normal);
+void position_and_jacobian_3d(double alpha, double beta, const double *triangle, double *pos, double *jac);
+void axial_coefficients_3d(const double *charges, const double *jac, const double *pos, double *trig_cos,
+                           double *trig_sin, size_t N, const double *z, double *out, size_t N_z);
+void fill_jacobian_buffer_current_three_d(const double *lines, double *jac, double *pos, double *dirs,
+                                          size_t N);
+double potential_3d_derivs(const double *point, const double *z, const double *coeffs, size_t N_z);
+void field_3d_derivs(const double *point, double *field, const double *z, const double *coeffs, size_t N_z);
+void fill_jacobian_buffer_3d(double *jac, double *pos, const double *vertices, size_t N);
+void triangle_areas(const double *triangles, double *out, size_t N);
+
+/* ======================================================================
+ * 2. Batched device entry points (device pointers, explicit stream)
+ * ====================================================================== */
+
+/* Replaces radial.c:224-246 for N elements on the device. */
+int tb_jacobian_buffer_radial(const double *vertices, double *jac, double *pos, int64_t N, tb_stream_t stream);
+
+/* Collocation data of each element at alpha = 0: target (N,2) = (r, z) and
+ * normal (N,2) (radial.c:266-267, utilities_2d.c:31-48). */
+int tb_element_targets(const double *vertices, double *target, double *normal, int64_t N, tb_stream_t stream);
+
+/* Off-diagonal BEM matrix, replaces radial.c:249-310 for rows [row0, row1)
+ * of an (N, N) matrix with row stride lda.  types uint8 (N), values (N).
+ * accumulate != 0 adds to A (the reference semantics), else overwrites.
+ * gauss_diagonal != 0 also writes the reference's 16-point value on the
+ * diagonal; otherwise the diagonal entry is left untouched. */
+int tb_fill_matrix_radial(double *A, int64_t lda, const double *vertices, const uint8_t *types,
+                          const double *values, const double *jac, const double *pos, int64_t N, int64_t row0,
+                          int64_t row1, int accumulate, int gauss_diagonal, tb_stream_t stream);
+
+/* Singular self terms: diag[i] = integral over alpha in [-1, 1] of the
+ * self integrand of element i (self_potential_radial, radial.c:182-196, for
+ * voltage rows; self_field_dot_normal_radial - 1, radial.c:203-222 and
+ * solver.py:239-244, for dielectric / magnetizable rows), computed by
+ * composite 16-point Gauss-Legendre on intervals graded geometrically toward
+ * the log singularity at alpha = 0 (FP64, ~1e-15 relative).  If A != NULL the
+ * values are also stored on the diagonal of A (stride lda). */
+int tb_self_integrals(const double *vertices, const uint8_t *types, const double *values, double *diag,
+                      double *A, int64_t lda, int64_t N, tb_stream_t stream);
+
+/* Right-hand side of solver.py:118-150 for voltage / dielectric rows: F = V
+ * for types 1, 2, 5; 0 for type 3.  (Magnetizable rows need the
+ * pre-existing field and are filled by the caller.) */
+int tb_rhs_radial(const uint8_t *types, const double *values, double *F, int64_t N, tb_stream_t stream);
+
+/* Dense LU with partial pivoting in FP64, in place on A (N x N, row stride
+ * lda): P A = L U.  ipiv (N) int32 receives the pivot row of each step
+ * (LAPACK convention, 0-based); perm (N) int32, if not NULL, the resulting
+ * row permutation (row i of P A is row perm[i] of A).  Replaces the
+ * factorisation inside numpy.linalg.solve (solver.py:173, LAPACK dgesv).
+ * A zero pivot yields non-finite factors (checked by the caller, as
+ * solver.py:175 checks the charges). */
+int tb_lu_factor(double *A, int64_t lda, int32_t *ipiv, int64_t N, tb_stream_t stream);
+int tb_lu_factor_perm(double *A, int64_t lda, int32_t *ipiv, int32_t *perm, int64_t N, tb_stream_t stream);
+
+/* Solves A x = f for nrhs right-hand sides stored as rows of F (nrhs, N)
+ * (row stride ldf) into the rows of X (nrhs, N) (row stride ldx, X != F),
+ * given the factors and permutation of tb_lu_factor_perm. */
+int tb_lu_solve_perm(const double *LU, int64_t lda, const int32_t *perm, int64_t N, const double *F, int64_t ldf,
+                     double *X, int64_t ldx, int64_t nrhs, tb_stream_t stream);
+
+/* Packs charges (N), jac (N,16), pos (N,16,2) into sources (3, 16 N):
+ * r, z and w = charge * jac. */
+int tb_pack_sources(const double *charges, const double *jac, const double *pos, double *sources, int64_t N,
+                    tb_stream_t stream);
+
+/* Packs current rings: currents (N), jac (N,12), pos (N,12,3) (y == 0) into
+ * sources (3, 12 N): r, z and w = current * jac. */
+int tb_pack_current_sources(const double *currents, const double *jac, const double *pos, double *sources,
+                            int64_t N, tb_stream_t stream);
+
+/* Magnetic field H at M points from Nc packed current rings, the batched
+ * form of current_field_radial (radial.c:55-83). */
+int tb_current_field_points(const double *points, int64_t M, const double *sources, int64_t Nc, double *field,
+                            tb_stream_t stream);
+
+/* Axial derivatives of the current scalar potential at N_z points,
+ * radial.c:85-103 (overwrites derivs (N_z, 9)).  Column 0 is the on-axis
+ * potential, current_potential_axial (radial.c:38-53). */
+int tb_current_axial_derivatives(const double *z, int64_t Nz, const double *sources, int64_t Nc, double *derivs,
+                                 tb_stream_t stream);
+
+/* Potential and field at M points (M,3) from Nq packed sources: the batched
+ * form of potential_radial / field_radial (radial.c:105-173).  pot (M) and/or
+ * field (M,3) may be NULL. */
+int tb_field_radial_points(const double *points, int64_t M, const double *sources, int64_t Nq, double *pot,
+                           double *field, tb_stream_t stream);
+
+/* Axial derivatives at N_z points, radial.c:18-36 (overwrites derivs
+ * (N_z, 9)). */
+int tb_axial_derivatives_radial(const double *z, int64_t Nz, const double *sources, int64_t Nq,
+                                double *derivs, tb_stream_t stream);
+
+/* Interpolation coefficients (N_z - 1, 9, 6) from derivs (N_z, 9) on an
+ * equally spaced z grid with spacing dz, replaces field.py:914-937: quintic
+ * Hermite through (d_i, d_i+1, d_i+2) for i <= 6, not-a-knot cubic spline
+ * for i = 7, 8.  N_z <= 12288. */
+int tb_axial_coefficients(const double *derivs, int64_t Nz, double dz, double *coeffs, tb_stream_t stream);
+
+/* Potential / field at M points from axial coefficients, the batched form
+ * of radial.c:312-384.  pot and/or field may be NULL. */
+int tb_axial_field_points(const double *points, int64_t M, const double *z, int64_t Nz, const double *coeffs,
+                          double *pot, double *field, tb_stream_t stream);
+
+/* Field sources of the tracer. */
+typedef struct {
+  const double *elec_sources;   /* (3, n_elec) packed rings or NULL */
+  int64_t n_elec;
+  const double *mag_sources;    /* (3, n_mag) packed rings or NULL */
+  int64_t n_mag;
+  const double *cur_sources;    /* (3, n_cur) packed current rings or NULL */
+  int64_t n_cur;
+  const double *field_bounds;   /* (3,2) strict field bounds or NULL (tracing.c:136-138) */
+  const double *axial_z;        /* axial interpolation: z (N_z) or NULL */
+  const double *axial_elec;     /* (N_z-1, 9, 6) */
+  const double *axial_mag;      /* (N_z-1, 9, 6) or NULL */
+  int64_t axial_nz;
+} tb_field_t;
+
+/* Tracing options. */
+typedef struct {
+  double bounds[6];       /* (xmin, xmax, ymin, ymax, zmin, zmax), inclusive (tracing.c:79-81) */
+  double atol;            /* absolute tolerance (tracing.c:106-108) */
+  double plane_z;         /* record the last crossing of z = plane_z ... */
+  int record_plane;       /* ... when nonzero (cubic Hermite on the bracketing states) */
+  int64_t max_attempts;   /* step-attempt cap per particle (> 0) */
+  int64_t max_rows;       /* rows per particle in `rows` (>= 2) or 0 for none */
+  int team_warps;         /* warps cooperating on one particle's BEM sums: 1, 2, 4 or 8; 0 = auto */
+} tb_trace_opts_t;
+
+/* Adaptive RKF45 tracing of n particles (tracing.c:60-123 per particle).
+ *   start (n, 6)   x, y, z, vx, vy, vz (SI)
+ *   t0 (n) or NULL start times; qm (n) charge/mass per particle
+ *   rows (n, max_rows, 7) t, x, y, z, vx, vy, vz (row 0 = start) or NULL
+ *   nrows (n) int64 rows written (or NULL), status (n) int32 (TB_TRACE_*)
+ *   final (n, 7) last accepted state (t, x..vz) or NULL
+ *   plane (n, 7) last crossing of z = plane_z (t, x..vz) or NULL; NaN if none
+ *   counters (n, 2) int64 accepted steps / attempts, or NULL
+ *   work (1) int32 device scratch, zeroed by the call: the work-queue head.
+ * Persistent kernel: teams of warps pull particles from the queue. */
+int tb_trace_rk45(const double *start, const double *t0, const double *qm, int64_t n, const tb_field_t *field,
+                  const tb_trace_opts_t *opts, double *rows, int64_t *nrows, int32_t *status, double *final_state,
+                  double *plane, int64_t *counters, int32_t *work, tb_stream_t stream);
+
+/* Number of SMs of the current device (grid sizing helper). */
+int tb_num_sms(void);
+
+/* Measurement helper, no reference counterpart: `blocks` x 256 threads each
+ * run `iters` x 8 dependent-free FP64 FMAs (16 flops per thread-iteration).
+ * Used to measure the FP64 pipe peak that the FP64-bound kernels are
+ * compared against. */
+int tb_probe_fp64_fma(int blocks, int64_t iters, double *out, tb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TRACEON_B200_H */

@@ -1,0 +1,69 @@
+// tb_internal.cuh -- small device and host helpers shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "tb_common.cuh"
+
+namespace tb {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Status of the last kernel launch on this thread.
+inline int launch_status() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? OK : CUDA_ERR;
+}
+
+// Number of SMs of the current device (cached per device).
+inline int num_sms() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cache[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
+
+// Axial series (radial.c:312-384): locate the interval of z on the equally
+// spaced grid zi and evaluate the 9 derivative polynomials.  Returns false
+// outside [zi[0], zi[Nz-1]].
+__host__ __device__ inline bool axial_eval(double z, const double* zi, const double* coeff, int64_t Nz,
+                                           double* d) {
+  double z0 = zi[0], zl = zi[Nz - 1];
+  if (!(z0 <= z && z <= zl)) return false;
+  double dz = zi[1] - zi[0];
+  int64_t idx = (int64_t)((z - z0) / dz);
+  if (idx < 0) idx = 0;
+  if (idx > Nz - 2) idx = Nz - 2;
+  double x = z - zi[idx];
+  const double* C = coeff + idx * NDERIV * 6;
+  for (int i = 0; i < NDERIV; i++) {
+    const double* c = C + i * 6;
+    d[i] = ((((c[0] * x + c[1]) * x + c[2]) * x + c[3]) * x + c[4]) * x + c[5];
+  }
+  return true;
+}
+
+// potential_radial_derivs, radial.c:340-343
+__host__ __device__ inline double axial_potential(const double* d, double r2) {
+  return d[0] - r2 / 4 * d[2] + r2 * r2 / 64. * d[4] - r2 * r2 * r2 / 2304. * d[6] +
+         r2 * r2 * r2 * r2 / 147456. * d[8];
+}
+
+// field_radial_derivs, radial.c:376-383
+__host__ __device__ inline void axial_field(const double* d, const double* p, double r2, double* f) {
+  double fr = 0.5 * (d[2] - r2 / 8 * d[4] + r2 * r2 / 192 * d[6] - r2 * r2 * r2 / 9216 * d[8]);
+  double fz = -d[1] + r2 / 4 * d[3] - r2 * r2 / 64 * d[5] + r2 * r2 * r2 / 2304 * d[7];
+  f[0] = p[0] * fr;
+  f[1] = p[1] * fr;
+  f[2] = fz;
+}
+
+}  // namespace tb

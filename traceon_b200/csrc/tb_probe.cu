@@ -1,0 +1,32 @@
+// tb_probe.cu -- FP64 pipe throughput probe used as the roofline denominator
+// of the FP64-bound kernels (the field sums of the tracer, fill and field
+// kernels).  Each thread runs 8 independent FMA chains; the result is
+// written so the work cannot be removed.
+#include "tb_common.cuh"
+#include "tb_internal.cuh"
+#include "../../include/traceon_b200.h"
+
+namespace tb {
+
+__global__ void __launch_bounds__(256) k_fp64_fma(int64_t iters, double seed, double* out) {
+  double a[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) a[i] = seed + i + threadIdx.x;
+  const double m = 0.9999999, c = 1e-7;
+  for (int64_t k = 0; k < iters; k++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) a[i] = fma(a[i], m, c);
+  }
+  double s = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s += a[i];
+  if (s == 12345.678) out[0] = s;  // practically never taken
+}
+
+}  // namespace tb
+
+extern "C" int tb_probe_fp64_fma(int blocks, int64_t iters, double* out, tb_stream_t stream) {
+  if (blocks <= 0 || iters <= 0 || !out) return tb::BAD_ARG;
+  tb::k_fp64_fma<<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, 1.0, out);
+  return tb::launch_status();
+}

@@ -1,0 +1,454 @@
+// tb_trace.cu -- persistent adaptive RKF45 tracer (tracing.c:60-123) for many
+// particles at once.
+//
+// Particles are pulled from a device work queue by teams.  For BEM fields a
+// team is 1-8 warps that split the ring sums of every field evaluation
+// (field_radial_traceable, tracing.c:125-165) and reduce them with shuffles
+// (and a named barrier across warps); every lane of a team then holds the
+// same field bits, so the step control runs redundantly and uniformly in all
+// lanes.  For axial-interpolated fields (field_radial_derivs_traceable,
+// tracing.c:168-174) a team is one thread.
+//
+// Step control is the reference's: Fehlberg 4(5) tableau, error = max|pos
+// err| + h max|vel err|, accept if error <= atol, h <- min(0.9 h
+// (atol/error)^(1/5), hmax) after every attempt, hmax = 0.01 / |v0|, stop
+// when the state leaves the inclusive bounds.  Unlike the reference, every
+// particle has a cap on step attempts and a non-finite check, so a trapped or
+// broken particle ends with a status instead of looping forever.
+#include "tb_common.cuh"
+#include "tb_internal.cuh"
+#include "../../include/traceon_b200.h"
+
+namespace tb {
+
+struct TraceParams {
+  const double* esrc;
+  int64_t ne;
+  const double* msrc;
+  int64_t nm;
+  const double* csrc;
+  int64_t nc;
+  const double* fb;
+  const double* az;
+  const double* aec;
+  const double* amc;
+  int64_t anz;
+  double bounds[6];
+  double atol;
+  double plane_z;
+  int record_plane;
+  int64_t max_attempts;
+  int64_t max_rows;
+  const double* start;
+  const double* t0;
+  const double* qm;
+  int64_t n;
+  double* rows;
+  int64_t* nrows;
+  int32_t* status;
+  double* final_state;
+  double* plane;
+  int64_t* counters;
+  int32_t* work;
+};
+
+// Fehlberg 4(5) tableau, tracing.c:9-16
+__constant__ double RK_B[6][5] = {{0, 0, 0, 0, 0},
+                                  {2. / 9., 0, 0, 0, 0},
+                                  {1. / 12., 1. / 4., 0, 0, 0},
+                                  {69. / 128., -243. / 128., 135. / 64., 0, 0},
+                                  {-17. / 12., 27. / 4., -27. / 5., 16. / 15., 0},
+                                  {65. / 432., -5. / 16., 13. / 16., 4. / 27., 5. / 144.}};
+__constant__ double RK_CH[6] = {47. / 450., 0., 12. / 25., 32. / 225., 1. / 30., 6. / 25.};
+__constant__ double RK_CT[6] = {-1. / 150., 0., 3. / 100., -16. / 75., -1. / 20., 6. / 25.};
+
+__device__ __forceinline__ bool in_bounds(const double* b, const double* y) {
+  return b[0] <= y[0] && y[0] <= b[1] && b[2] <= y[1] && y[1] <= b[3] && b[4] <= y[2] && y[2] <= b[5];
+}
+
+// Cubic Hermite crossing of z = zp between accepted states s0 (time t0) and
+// s1 (time t0 + h): Newton iteration safeguarded by bisection from the
+// linear estimate.  Position from the Hermite cubic, velocity linear.
+__device__ void hermite_crossing(double h, const double* s0, const double* s1, double zp, double t0, double* out) {
+  auto pos = [&](double u, int c) {
+    double u2 = u * u, u3 = u2 * u;
+    return (2 * u3 - 3 * u2 + 1) * s0[c] + (u3 - 2 * u2 + u) * h * s0[3 + c] + (-2 * u3 + 3 * u2) * s1[c] +
+           (u3 - u2) * h * s1[3 + c];
+  };
+  auto dpos = [&](double u, int c) {
+    double u2 = u * u;
+    return (6 * u2 - 6 * u) * s0[c] + (3 * u2 - 4 * u + 1) * h * s0[3 + c] + (-6 * u2 + 6 * u) * s1[c] +
+           (3 * u2 - 2 * u) * h * s1[3 + c];
+  };
+  double u = (zp - s0[2]) / (s1[2] - s0[2]);
+  double lo = 0.0, hi = 1.0;
+  bool s0_above = s0[2] - zp > 0;
+  for (int it = 0; it < 60; it++) {
+    double f = pos(u, 2) - zp;
+    if ((f > 0) == s0_above)
+      lo = u;
+    else
+      hi = u;
+    double d = dpos(u, 2);
+    double un = d != 0 ? u - f / d : 0.5 * (lo + hi);
+    if (!(lo < un && un < hi)) un = 0.5 * (lo + hi);
+    if (fabs(un - u) < 1e-16) {
+      u = un;
+      break;
+    }
+    u = un;
+  }
+  out[0] = t0 + u * h;
+  out[1] = pos(u, 0);
+  out[2] = pos(u, 1);
+  out[3] = zp;
+  for (int c = 0; c < 3; c++) out[4 + c] = (1 - u) * s0[3 + c] + u * s1[3 + c];
+}
+
+// The integrator.  `field(p, E, H)` must return identical bits in every
+// thread that shares a particle; `ks` is per-team scratch for the 6 stages.
+template <class FieldFn>
+__device__ void rk45_particle(const TraceParams& P, int64_t idx, FieldFn& field, double (*ks)[6], bool writer) {
+  double y[6];
+  for (int c = 0; c < 6; c++) y[c] = P.start[idx * 6 + c];
+  const double qm = P.qm[idx];
+  double t = P.t0 ? P.t0[idx] : 0.0;
+  const double V = sqrt(y[3] * y[3] + y[4] * y[4] + y[5] * y[5]);
+  const double hmax = STEP_MAX / V;
+  double h = hmax;
+  int64_t nrow = 1, accepted = 0, attempts = 0;
+  int status = TRACE_EXITED;
+  const double atol = P.atol;
+  if (writer && P.rows) {
+    double* r = P.rows + idx * P.max_rows * 7;
+    r[0] = t;
+    for (int c = 0; c < 6; c++) r[1 + c] = y[c];
+  }
+  if (writer && P.plane)
+    for (int c = 0; c < 7; c++) P.plane[idx * 7 + c] = __longlong_as_double(0x7ff8000000000000LL);
+
+  while (in_bounds(P.bounds, y)) {
+    if (attempts >= P.max_attempts) {
+      status = TRACE_MAX_ATTEMPTS;
+      break;
+    }
+    attempts++;
+#pragma unroll 1
+    for (int s = 0; s < 6; s++) {
+      double ys[6];
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        double v = y[c];
+        for (int j = 0; j < s; j++) v += RK_B[s][j] * ks[j][c];
+        ys[c] = v;
+      }
+      double E[3], H[3];
+      field(ys, E, H);
+      double cx = ys[4] * H[2] - ys[5] * H[1];
+      double cy = ys[5] * H[0] - ys[3] * H[2];
+      double cz = ys[3] * H[1] - ys[4] * H[0];
+      double k0 = h * ys[3], k1 = h * ys[4], k2 = h * ys[5];
+      double k3 = h * qm * (E[0] + MU0 * cx);
+      double k4 = h * qm * (E[1] + MU0 * cy);
+      double k5 = h * qm * (E[2] + MU0 * cz);
+      ks[s][0] = k0;
+      ks[s][1] = k1;
+      ks[s][2] = k2;
+      ks[s][3] = k3;
+      ks[s][4] = k4;
+      ks[s][5] = k5;
+    }
+    double ep = 0.0, ev = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double a = 0.0, b = 0.0;
+      for (int j = 0; j < 6; j++) {
+        a += RK_CT[j] * ks[j][c];
+        b += RK_CT[j] * ks[j][c + 3];
+      }
+      ep = fmax(ep, fabs(a));
+      ev = fmax(ev, fabs(b));
+    }
+    double err = ep + h * ev;
+    if (!(err == err)) {
+      status = TRACE_NONFINITE;
+      break;
+    }
+    if (err <= atol) {
+      double yn[6];
+#pragma unroll
+      for (int c = 0; c < 6; c++)
+        yn[c] = y[c] + (RK_CH[0] * ks[0][c] + RK_CH[1] * ks[1][c] + RK_CH[2] * ks[2][c] + RK_CH[3] * ks[3][c] +
+                        RK_CH[4] * ks[4][c] + RK_CH[5] * ks[5][c]);
+      double tn = t + h;
+      if (P.record_plane && ((y[2] - P.plane_z > 0) != (yn[2] - P.plane_z > 0))) {
+        double cr[7];
+        hermite_crossing(h, y, yn, P.plane_z, t, cr);
+        if (writer && P.plane)
+          for (int c = 0; c < 7; c++) P.plane[idx * 7 + c] = cr[c];
+      }
+#pragma unroll
+      for (int c = 0; c < 6; c++) y[c] = yn[c];
+      t = tn;
+      accepted++;
+      bool finite = true;
+      for (int c = 0; c < 6; c++) finite = finite && isfinite(y[c]);
+      if (P.rows) {
+        if (writer) {
+          double* r = P.rows + (idx * P.max_rows + nrow) * 7;
+          r[0] = t;
+          for (int c = 0; c < 6; c++) r[1 + c] = y[c];
+        }
+        nrow++;
+      }
+      if (!finite) {
+        status = TRACE_NONFINITE;
+        break;
+      }
+      if (P.rows && nrow >= P.max_rows) {
+        status = TRACE_ROWS_FULL;
+        break;
+      }
+    }
+    h = fmin(0.9 * h * pow(atol / err, 0.2), hmax);
+  }
+  if (writer) {
+    if (P.nrows) P.nrows[idx] = P.rows ? nrow : 1;
+    if (P.status) P.status[idx] = status;
+    if (P.final_state) {
+      P.final_state[idx * 7] = t;
+      for (int c = 0; c < 6; c++) P.final_state[idx * 7 + 1 + c] = y[c];
+    }
+    if (P.counters) {
+      P.counters[idx * 2] = accepted;
+      P.counters[idx * 2 + 1] = attempts;
+    }
+  }
+}
+
+__device__ __forceinline__ void team_barrier(int team, int nthreads) {
+  if (nthreads <= 32)
+    __syncwarp();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(team + 1), "r"(nthreads) : "memory");
+}
+
+// BEM field of a team: the elec and mag ring sums split over the team's
+// threads, then a butterfly reduction (identical bits in every lane) and,
+// for teams of several warps, a fixed-order sum of the warp partials.
+template <int TW>
+struct BemTeamField {
+  const TraceParams& P;
+  int team, lt;
+  double (*red)[6];  // [TW][6] per team
+
+  __device__ void operator()(const double* p, double* E, double* H) {
+    constexpr int T = 32 * TW;
+    const double* fb = P.fb;
+    bool inside = fb == nullptr || (fb[0] < p[0] && p[0] < fb[1] && fb[2] < p[1] && p[1] < fb[3] &&
+                                    fb[4] < p[2] && p[2] < fb[5]);
+    double r0 = sqrt(p[0] * p[0] + p[1] * p[1]), z0 = p[2];
+    // s: elec (Sr, Sz), mag (Sr, Sz), currents (Br, Bz)
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    double dummy = 0;
+    if (inside) {
+      const double* er = P.esrc;
+      for (int64_t j = lt; j < P.ne; j += T)
+        ring_field_acc<false>(r0, z0, er[j], er[P.ne + j], er[2 * P.ne + j], s[0], s[1], dummy);
+      const double* mr = P.msrc;
+      for (int64_t j = lt; j < P.nm; j += T)
+        ring_field_acc<false>(r0, z0, mr[j], mr[P.nm + j], mr[2 * P.nm + j], s[2], s[3], dummy);
+      const double* cr = P.csrc;
+      for (int64_t j = lt; j < P.nc; j += T) {
+        double hr, hz;
+        current_field_ring(r0, z0, cr[j], cr[P.nc + j], hr, hz);
+        s[4] = fma(cr[2 * P.nc + j], hr, s[4]);
+        s[5] = fma(cr[2 * P.nc + j], hz, s[5]);
+      }
+    }
+    const int nsum = P.nc > 0 ? 6 : 4;
+    for (int c = 0; c < nsum; c++) s[c] = warp_sum(s[c]);
+    if (TW > 1) {
+      int w = lt / 32;
+      if ((lt & 31) == 0)
+        for (int c = 0; c < nsum; c++) red[w][c] = s[c];
+      team_barrier(team, T);
+      for (int c = 0; c < nsum; c++) {
+        double a = 0;
+        for (int k = 0; k < TW; k++) a += red[k][c];
+        s[c] = a;
+      }
+      team_barrier(team, T);
+    }
+    if (!inside) {
+      for (int c = 0; c < 3; c++) E[c] = H[c] = 0.0;
+      return;
+    }
+    if (r0 >= MIN_AXIS) {
+      double er = s[0] / (2 * PI * r0), mr = s[2] / (2 * PI * r0);
+      E[0] = p[0] / r0 * er;
+      E[1] = p[1] / r0 * er;
+      H[0] = p[0] / r0 * mr;
+      H[1] = p[1] / r0 * mr;
+    } else {
+      E[0] = E[1] = H[0] = H[1] = 0.0;
+    }
+    E[2] = -s[1] * INV_PI;
+    H[2] = -s[3] * INV_PI;
+    if (P.nc > 0) {
+      if (r0 >= MIN_AXIS) {
+        H[0] += p[0] / r0 * s[4];
+        H[1] += p[1] / r0 * s[4];
+      }
+      H[2] += s[5];
+    }
+  }
+};
+
+constexpr int TRACE_THREADS = 256;
+
+template <int TW>
+__global__ void __launch_bounds__(TRACE_THREADS) k_trace_bem(TraceParams P) {
+  constexpr int T = 32 * TW;
+  constexpr int TEAMS = TRACE_THREADS / T;
+  __shared__ double s_k[TEAMS][6][6];
+  __shared__ double s_red[TEAMS][TW][6];
+  __shared__ int64_t s_idx[TEAMS];
+  const int team = threadIdx.x / T, lt = threadIdx.x % T;
+  BemTeamField<TW> field{P, team, lt, s_red[team]};
+  for (;;) {
+    int64_t idx;
+    if (TW == 1) {
+      int v = 0;
+      if (lt == 0) v = atomicAdd(P.work, 1);
+      idx = __shfl_sync(0xffffffffu, v, 0);
+    } else {
+      if (lt == 0) s_idx[team] = atomicAdd(P.work, 1);
+      team_barrier(team, T);
+      idx = s_idx[team];
+      team_barrier(team, T);
+    }
+    if (idx >= P.n) break;
+    rk45_particle(P, idx, field, s_k[team], lt == 0);
+  }
+}
+
+// Axial-interpolated field (field_radial_derivs_traceable): per thread.
+struct AxialField {
+  const TraceParams& P;
+  __device__ void operator()(const double* p, double* E, double* H) {
+    double d[NDERIV];
+    double r2 = p[0] * p[0] + p[1] * p[1];
+    if (axial_eval(p[2], P.az, P.aec, P.anz, d))
+      axial_field(d, p, r2, E);
+    else
+      E[0] = E[1] = E[2] = 0.0;
+    if (P.amc && axial_eval(p[2], P.az, P.amc, P.anz, d))
+      axial_field(d, p, r2, H);
+    else
+      H[0] = H[1] = H[2] = 0.0;
+  }
+};
+
+__global__ void __launch_bounds__(128) k_trace_axial(TraceParams P) {
+  AxialField field{P};
+  double ks[6][6];
+  for (;;) {
+    int64_t idx = atomicAdd(P.work, 1);
+    if (idx >= P.n) break;
+    rk45_particle(P, idx, field, ks, true);
+  }
+}
+
+template <int TW>
+static int launch_bem(const TraceParams& P, cudaStream_t s) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_bem<TW>, TRACE_THREADS, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  int64_t teams_needed = P.n;
+  int64_t blocks = (int64_t)num_sms() * per_sm;
+  int64_t by_work = (teams_needed + (TRACE_THREADS / (32 * TW)) - 1) / (TRACE_THREADS / (32 * TW));
+  if (blocks > by_work) blocks = by_work;
+  if (blocks < 1) blocks = 1;
+  k_trace_bem<TW><<<unsigned(blocks), TRACE_THREADS, 0, s>>>(P);
+  return launch_status();
+}
+
+}  // namespace tb
+
+using namespace tb;
+
+extern "C" int tb_trace_rk45(const double* start, const double* t0, const double* qm, int64_t n,
+                             const tb_field_t* field, const tb_trace_opts_t* opts, double* rows, int64_t* nrows,
+                             int32_t* status, double* final_state, double* plane, int64_t* counters, int32_t* work,
+                             tb_stream_t stream) {
+  if (!field || !opts || n < 0 || !work) return BAD_ARG;
+  if (n == 0) return OK;
+  if (n > 0x7fffffff || !start || !qm) return BAD_ARG;
+  if (opts->max_attempts <= 0 || !(opts->atol > 0)) return BAD_ARG;
+  if (rows && opts->max_rows < 2) return BAD_ARG;
+  bool axial = field->axial_z != nullptr;
+  if (axial && (field->axial_nz < 2 || !field->axial_elec)) return BAD_ARG;
+  if (!axial && ((field->n_elec > 0 && !field->elec_sources) || (field->n_mag > 0 && !field->mag_sources)))
+    return BAD_ARG;
+  if (field->n_elec < 0 || field->n_mag < 0 || field->n_cur < 0) return BAD_ARG;
+  if (!axial && field->n_cur > 0 && !field->cur_sources) return BAD_ARG;
+  TraceParams P;
+  P.esrc = field->elec_sources;
+  P.ne = field->n_elec;
+  P.msrc = field->mag_sources;
+  P.nm = field->n_mag;
+  P.csrc = field->cur_sources;
+  P.nc = field->n_cur;
+  P.fb = field->field_bounds;
+  P.az = field->axial_z;
+  P.aec = field->axial_elec;
+  P.amc = field->axial_mag;
+  P.anz = field->axial_nz;
+  for (int i = 0; i < 6; i++) P.bounds[i] = opts->bounds[i];
+  P.atol = opts->atol;
+  P.plane_z = opts->plane_z;
+  P.record_plane = opts->record_plane;
+  P.max_attempts = opts->max_attempts;
+  P.max_rows = rows ? opts->max_rows : 0;
+  P.start = start;
+  P.t0 = t0;
+  P.qm = qm;
+  P.n = n;
+  P.rows = rows;
+  P.nrows = nrows;
+  P.status = status;
+  P.final_state = final_state;
+  P.plane = plane;
+  P.counters = counters;
+  P.work = work;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemsetAsync(work, 0, sizeof(int32_t), s) != cudaSuccess) return CUDA_ERR;
+  if (axial) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_axial, 128, 0) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    int64_t blocks = (int64_t)num_sms() * per_sm;
+    int64_t by_work = (n + 127) / 128;
+    if (blocks > by_work) blocks = by_work;
+    k_trace_axial<<<unsigned(blocks), 128, 0, s>>>(P);
+    return launch_status();
+  }
+  int tw = opts->team_warps;
+  if (tw == 0) {
+    // Fill the GPU: about 32 resident warps per SM.
+    int64_t want = (int64_t)num_sms() * 32;
+    tw = 1;
+    while (tw < 8 && n * tw * 2 <= want) tw *= 2;
+  }
+  switch (tw) {
+    case 1: return launch_bem<1>(P, s);
+    case 2: return launch_bem<2>(P, s);
+    case 4: return launch_bem<4>(P, s);
+    case 8: return launch_bem<8>(P, s);
+    default: return BAD_ARG;
+  }
+}
+
+extern "C" int tb_num_sms(void) { return num_sms(); }

@@ -1,0 +1,136 @@
+"""Synthetic radially symmetric electrode geometries as line4 (cubic) meshes.
+
+The reference builds meshes with ``traceon.geometry.Path(...).mesh()``, whose
+``discretize_path`` spaces nodes uniformly (traceon/geometry.py:39-70).  The
+lens workloads here are graded toward the corners of every straight segment,
+which the reference mesher cannot do, so the mesh rows are written directly
+in the reference's line4 layout: each element row is
+``[start, end, 1/3-point, 2/3-point]`` (traceon/mesher.py:188-227 and the
+vertex ordering of traceon/geometry.py:851-857).  All lengths are metres.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+MM = 1e-3
+
+
+def graded_nodes(n: int) -> np.ndarray:
+    """n+1 Chebyshev-Lobatto nodes on [0, 1]: dense toward both ends."""
+    k = np.arange(n + 1)
+    s = 0.5 * (1.0 - np.cos(np.pi * k / n))
+    s[0], s[-1] = 0.0, 1.0
+    return s
+
+
+def polyline_elements(points_rz, counts) -> np.ndarray:
+    """Cubic line elements along a polyline of (r, z) corners.  ``counts[i]``
+    elements on segment i, graded toward both ends.  Returns (N, 4, 3) rows
+    (r, 0, z) in line4 order [start, end, 1/3, 2/3]."""
+    pts = np.asarray(points_rz, dtype=np.float64)
+    rows = []
+    for (p0, p1), n in zip(zip(pts[:-1], pts[1:]), counts):
+        s = graded_nodes(int(n))
+        for a, b in zip(s[:-1], s[1:]):
+            q = [p0 + (p1 - p0) * t for t in (a, b, a + (b - a) / 3, a + 2 * (b - a) / 3)]
+            rows.append([[x[0], 0.0, x[1]] for x in q])
+    return snap(np.array(rows, dtype=np.float64))
+
+
+def snap(a: np.ndarray) -> np.ndarray:
+    """Zero the low 16 mantissa bits of every coordinate.  The reference
+    Mesh merges points after the same truncation (traceon/mesher.py:262-290),
+    so snapped vertices pass through a reference Mesh unchanged."""
+    a = np.array(a, dtype=np.float64)
+    a.view(np.uint64)[...] &= np.uint64(0xFFFFFFFFFFFF0000)
+    return a
+
+
+def split_counts(total: int, lengths) -> list[int]:
+    """Split ``total`` elements over segments proportionally to length (each
+    segment gets at least 2)."""
+    lengths = np.asarray(lengths, dtype=np.float64)
+    raw = total * lengths / lengths.sum()
+    c = np.maximum(2, np.floor(raw).astype(int))
+    while c.sum() < total:
+        c[np.argmax(raw - c)] += 1
+    while c.sum() > total:
+        i = np.argmax(c - raw)
+        c[i] -= 1
+    return [int(x) for x in c]
+
+
+def aperture_tube(r_in: float, r_out: float, z0: float, z1: float, n: int) -> np.ndarray:
+    """One einzel-lens electrode: a tube of radius r_in over [z0, z1] with
+    annular end caps out to r_out, i.e. the polyline
+    (r_out, z0) -> (r_in, z0) -> (r_in, z1) -> (r_out, z1)."""
+    corners = [(r_out, z0), (r_in, z0), (r_in, z1), (r_out, z1)]
+    lengths = [r_out - r_in, z1 - z0, r_out - r_in]
+    return polyline_elements(corners, split_counts(n, lengths))
+
+
+class LensGeometry:
+    """A meshed electrode stack: vertices (N,4,3), per-element electrode index
+    and the electrode names, in the element order used for the BEM matrix."""
+
+    def __init__(self, vertices, electrode_index, names):
+        self.vertices = np.ascontiguousarray(vertices, dtype=np.float64)
+        self.electrode_index = np.asarray(electrode_index, dtype=np.int64)
+        self.names = list(names)
+
+    def __len__(self):
+        return len(self.vertices)
+
+    def voltages_to_values(self, voltages) -> np.ndarray:
+        v = np.asarray(voltages, dtype=np.float64)
+        return v[self.electrode_index]
+
+    def unit_rhs(self) -> np.ndarray:
+        """One right-hand side per electrode at 1 V (the superposition basis of
+        traceon/solver.py:364-400)."""
+        F = np.zeros((len(self.names), len(self)))
+        for e in range(len(self.names)):
+            F[e, self.electrode_index == e] = 1.0
+        return F
+
+
+def einzel_lens(n_elements: int = 1000, r_tube: float = 1.0 * MM, r_cap: float = 2.0 * MM,
+                spans=((-5 * MM, -1 * MM), (-0.5 * MM, 0.5 * MM), (1 * MM, 5 * MM))) -> LensGeometry:
+    """Three coaxial tubes at r = 1 mm spanning z in [-5,-1], [-0.5,0.5],
+    [1,5] mm with annular end caps to r = 2 mm; ``n_elements`` cubic elements
+    split evenly across the electrodes and graded toward the tube edges."""
+    k = len(spans)
+    per = [n_elements // k + (1 if i < n_elements % k else 0) for i in range(k)]
+    verts, idx = [], []
+    for e, ((z0, z1), n) in enumerate(zip(spans, per)):
+        v = aperture_tube(r_tube, r_cap, z0, z1, n)
+        verts.append(v)
+        idx.append(np.full(len(v), e))
+    names = ['ground_in', 'lens', 'ground_out'][:k] if k == 3 else [f'electrode{i}' for i in range(k)]
+    return LensGeometry(np.concatenate(verts), np.concatenate(idx), names)
+
+
+def einzel_lens_voltages(seed: int) -> np.ndarray:
+    """(0, V_mid, 0) with V_mid uniform in [500, 2000] V from the seed."""
+    rng = np.random.default_rng(seed)
+    return np.array([0.0, rng.uniform(500.0, 2000.0), 0.0])
+
+
+def electron_beam(n: int, seed: int, energy_ev: float = 1000.0, z0: float = -9.5 * MM,
+                  r_max: float = 0.2 * MM, angle_max: float = 5e-3):
+    """Start states of the lens workload: electrons at ``energy_ev`` starting at
+    x = r ~ U[0, r_max], y = 0, z = z0, heading +z at an angle ~ U[-a, a] in
+    the xz-plane.  Returns (positions (n,3), velocities (n,3)) in SI units;
+    the speed follows traceon.tracing.velocity_vec (traceon/tracing.py:24-56)."""
+    from scipy.constants import e, m_e
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(0.0, r_max, n)
+    ang = rng.uniform(-angle_max, angle_max, n)
+    speed = np.sqrt(2 * energy_ev * e / m_e)
+    pos = np.stack([r, np.zeros(n), np.full(n, z0)], axis=1)
+    vel = speed * np.stack([np.sin(ang), np.zeros(n), np.cos(ang)], axis=1)
+    return pos, vel
+
+
+LENS_BOUNDS = np.array([[-2 * MM, 2 * MM], [-2 * MM, 2 * MM], [-10 * MM, 10 * MM]])
+LENS_EXIT_Z = 9.5 * MM
