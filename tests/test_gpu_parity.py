@@ -22,6 +22,25 @@ def rel(a, b, floor=0.0):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
 
 
+def poly_values(c, h):
+    """Values of every (interval, derivative) polynomial of an axial
+    coefficient table (N_z-1, 9, 6) at x = 0, h/3, 2h/3, h."""
+    x = np.array([0.0, h / 3, 2 * h / 3, h])
+    return sum(c[:, :, k, None] * x ** (5 - k) for k in range(6))
+
+
+def assert_same_polynomials(c, c_ref, h, tol):
+    """Coefficient tables agree where it matters: the evaluated pieces, per
+    derivative column, relative to that column's largest value.  (The
+    highest-order coefficients themselves carry cancellation error in any
+    FP64 construction: SciPy's Bernstein route and the closed form here
+    differ there by ~1e-6 relative while the pieces agree to ~1e-14.)"""
+    a, b = poly_values(c, h), poly_values(c_ref, h)
+    for l in range(c.shape[1]):
+        s = np.abs(b[:, l]).max()
+        assert np.max(np.abs(a[:, l] - b[:, l])) / s < tol, l
+
+
 def lens(n=96):
     from traceon_b200.geometry import einzel_lens
     return einzel_lens(n)
@@ -219,9 +238,7 @@ def test_axial(cuda, port, g96):
         s = np.abs(g96['derivs'][:, l]).max()
         assert np.max(np.abs(dn[:, l] - g96['derivs'][:, l])) / s < 1e-11, l
     c = cuda.dev_axial_coefficients(cuda.to_dev(g96['derivs'], torch.float64), z[1] - z[0]).cpu().numpy()
-    for l in range(9):
-        s = np.abs(g96['coeffs'][:, l]).max()
-        assert np.max(np.abs(c[:, l] - g96['coeffs'][:, l])) / s < 1e-10, l
+    assert_same_polynomials(c, g96['coeffs'], z[1] - z[0], 1e-12)
     # compat accumulate semantics
     dd = cuda.axial_derivatives_radial(z, q, jac, pos)
     assert np.max(np.abs(dd - g96['derivs'])) <= 1e-11 * np.abs(g96['derivs']).max(axis=0).max()
@@ -243,9 +260,7 @@ def test_axial_spline_sizes(cuda, nz):
     d = rng.normal(size=(nz, 9)) * 10.0 ** np.arange(9)
     c = cuda.dev_axial_coefficients(cuda.to_dev(d, torch.float64), z[1] - z[0]).cpu().numpy()
     c_or = axial_coefficients(z, d)
-    for l in range(9):
-        s = np.abs(c_or[:, l]).max()
-        assert np.max(np.abs(c[:, l] - c_or[:, l])) / s < 1e-9, (nz, l)
+    assert_same_polynomials(c, c_or, z[1] - z[0], 1e-11)
 
 
 def _geometry_field(cuda, port, n=300, volts=(0.0, 1200.0, 0.0)):
@@ -311,9 +326,8 @@ def test_trace_axial(cuda, g96):
     from traceon_b200.field import EffectivePointCharges, FieldRadialBEM, FieldRadialAxial
     field = FieldRadialBEM(EffectivePointCharges(g96['charges'], g96['jac'], g96['pos']))
     ax = FieldRadialAxial(field, g96['z_axial'][0], g96['z_axial'][-1], N=len(g96['z_axial']))
-    for l in range(9):
-        s = np.abs(g96['coeffs'][:, l]).max()
-        assert np.max(np.abs(ax.electrostatic_coeffs[:, l] - g96['coeffs'][:, l])) / s < 1e-10
+    z = g96['z_axial']
+    assert_same_polynomials(ax.electrostatic_coeffs, g96['coeffs'], z[1] - z[0], 1e-11)
     res = ax.get_tracer(g96['bounds']).trace_multiple(g96['p0'], g96['v0'], atol=1e-10)
     from traceon_b200.tracing import xy_plane_intersection
     for i, (t, s) in enumerate(res):

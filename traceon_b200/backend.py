@@ -589,11 +589,11 @@ def dev_lu_factor(A):
 def dev_lu_solve(LU, perm, F):
     """Solves A x = f for each row f of F (nrhs, N)."""
     torch = _torch()
-    F = F.contiguous()
-    X = torch.empty_like(F)
     N = LU.shape[0]
-    _call('tb_lu_solve_perm', _ptr(LU), LU.stride(0), _ptr(perm), N, _ptr(F), F.stride(0), _ptr(X), X.stride(0),
-          F.shape[0], _stream())
+    F = F.reshape(-1, N).clone(memory_format=torch.contiguous_format)
+    X = torch.empty((F.shape[0], N), dtype=torch.float64, device=F.device)
+    # a (1, N) tensor may report stride 0 for its size-1 dimension
+    _call('tb_lu_solve_perm', _ptr(LU), LU.stride(0), _ptr(perm), N, _ptr(F), N, _ptr(X), N, F.shape[0], _stream())
     return X
 
 

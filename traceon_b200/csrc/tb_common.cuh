@@ -51,25 +51,64 @@ __host__ __device__ inline double gauss_w(int k) {
 // Cody (1965) log-polynomial forms K(1-p) = A(p) + log(1/p) B(p) and
 // E(1-p) = C(p) + log(1/p) D(p), degree 7 (elliptic.c:9-35, :43-69),
 // evaluated here by Horner's rule.
+// The device forms read the coefficients from constant memory, which FP64
+// FMA instructions take as a direct operand; literal 64-bit constants would
+// have to be materialised into registers inside the hot loops.
+__constant__ double C_KA[8] = {1.3862943611198906, 9.65736020516771e-2, 3.08909633861795e-2,
+                               1.52618320622534e-2, 1.25565693543211e-2, 1.68695685967517e-2,
+                               1.09423810688623e-2, 1.40704915496101e-3};
+__constant__ double C_KB[8] = {0.5, 1.24999998585309e-1, 7.03114105853296e-2, 4.87379510945218e-2,
+                               3.57218443007327e-2, 2.09857677336790e-2, 5.81807961871996e-3,
+                               3.42805719229748e-4};
+__constant__ double C_EA[8] = {1.0, 4.43147193467733e-1, 5.68115681053803e-2, 2.21862206993846e-2,
+                               1.56847700239786e-2, 1.92284389022977e-2, 1.21819481486695e-2,
+                               1.55618744745296e-3};
+__constant__ double C_EB[8] = {0.0, 2.49999998448655e-1, 9.37488062098189e-2, 5.84950297066166e-2,
+                               4.09074821593164e-2, 2.35091602564984e-2, 6.45682247315060e-3,
+                               3.78886487349367e-4};
+
+__device__ __forceinline__ double horner_c(const double* c, double p) {
+  double s = c[7];
+#pragma unroll
+  for (int i = 6; i >= 0; i--) s = fma(s, p, c[i]);
+  return s;
+}
+
 TB_HD double poly_ka(double p) {
+#ifdef __CUDA_ARCH__
+  return horner_c(C_KA, p);
+#else
   return ((((((1.40704915496101e-3 * p + 1.09423810688623e-2) * p + 1.68695685967517e-2) * p +
              1.25565693543211e-2) * p + 1.52618320622534e-2) * p + 3.08909633861795e-2) * p +
           9.65736020516771e-2) * p + 1.3862943611198906;
+#endif
 }
 TB_HD double poly_kb(double p) {
+#ifdef __CUDA_ARCH__
+  return horner_c(C_KB, p);
+#else
   return ((((((3.42805719229748e-4 * p + 5.81807961871996e-3) * p + 2.09857677336790e-2) * p +
              3.57218443007327e-2) * p + 4.87379510945218e-2) * p + 7.03114105853296e-2) * p +
           1.24999998585309e-1) * p + 0.5;
+#endif
 }
 TB_HD double poly_ea(double p) {
+#ifdef __CUDA_ARCH__
+  return horner_c(C_EA, p);
+#else
   return ((((((1.55618744745296e-3 * p + 1.21819481486695e-2) * p + 1.92284389022977e-2) * p +
              1.56847700239786e-2) * p + 2.21862206993846e-2) * p + 5.68115681053803e-2) * p +
           4.43147193467733e-1) * p + 1.0;
+#endif
 }
 TB_HD double poly_eb(double p) {
+#ifdef __CUDA_ARCH__
+  return horner_c(C_EB, p);
+#else
   return ((((((3.78886487349367e-4 * p + 6.45682247315060e-3) * p + 2.35091602564984e-2) * p +
              4.09074821593164e-2) * p + 5.84950297066166e-2) * p + 9.37488062098189e-2) * p +
           2.49999998448655e-1) * p;
+#endif
 }
 
 TB_HD double ellipkm1(double p) { return poly_ka(p) + log(1.0 / p) * poly_kb(p); }

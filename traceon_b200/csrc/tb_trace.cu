@@ -253,6 +253,7 @@ struct BemTeamField {
     double dummy = 0;
     if (inside) {
       const double* er = P.esrc;
+#pragma unroll 2
       for (int64_t j = lt; j < P.ne; j += T)
         ring_field_acc<false>(r0, z0, er[j], er[P.ne + j], er[2 * P.ne + j], s[0], s[1], dummy);
       const double* mr = P.msrc;
@@ -308,7 +309,7 @@ struct BemTeamField {
 constexpr int TRACE_THREADS = 256;
 
 template <int TW>
-__global__ void __launch_bounds__(TRACE_THREADS) k_trace_bem(TraceParams P) {
+__global__ void __launch_bounds__(TRACE_THREADS, 3) k_trace_bem(TraceParams P) {
   constexpr int T = 32 * TW;
   constexpr int TEAMS = TRACE_THREADS / T;
   __shared__ double s_k[TEAMS][6][6];

@@ -19,7 +19,7 @@ from scipy.constants import m_e, e
 
 from . import backend as B
 
-DEFAULT_MAX_ATTEMPTS = 1_000_000
+DEFAULT_MAX_ATTEMPTS = 100_000
 DEFAULT_ROWS = 4096
 
 
