@@ -390,7 +390,7 @@ def main():
     ap.add_argument('--ref-seconds', type=float, default=20.0)
     # executed FP64 flops per ring-pair evaluation of the tracer's field sum
     # (dadd + dmul + 2 dfma per pair, from the ncu instruction counts)
-    ap.add_argument('--flop-per-pair', type=float, default=130.0)
+    ap.add_argument('--flop-per-pair', type=float, default=162.0)
     ap.add_argument('--traffic', type=float, default=None)
     args = ap.parse_args()
     if args.impl == 'reference':
