@@ -238,6 +238,22 @@ int tb_lu_solve_perm(const double *LU, int64_t lda, const int32_t *perm, int64_t
 int tb_pack_sources(const double *charges, const double *jac, const double *pos, double *sources, int64_t N,
                     tb_stream_t stream);
 
+/* Dense solve that allocates nothing: LU-factorises A in place (as
+ * tb_lu_factor_perm) and solves for the nrhs rows of F into the rows of X (as
+ * tb_lu_solve_perm), keeping the pivots and permutation in a static device
+ * array of the library instead of caller memory.  No counterpart in the
+ * reference.  It exists for callers that cannot allocate device memory (a
+ * plug-in in a host application that owns the GPU memory pool, a control
+ * loop that may not allocate after start-up).  Limit: N <= 32768 (larger N
+ * returns TB_BAD_ARG); the array (256 KiB) is held by every GPU that loads
+ * the library until the process exits.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (different streams, or other threads) race and must be
+ * serialised by the caller.  Calls no cudaMalloc or cudaFree. */
+int tb_lu_solve_noalloc(double *A, int64_t lda, int64_t N, const double *F, int64_t ldf, double *X, int64_t ldx,
+                        int64_t nrhs, tb_stream_t stream);
+
 /* Packs current rings: currents (N), jac (N,12), pos (N,12,3) (y == 0) into
  * sources (3, 12 N): r, z and w = current * jac. */
 int tb_pack_current_sources(const double *currents, const double *jac, const double *pos, double *sources,

@@ -293,3 +293,51 @@ extern "C" int tb_lu_solve_perm(const double* LU, int64_t lda, const int32_t* pe
   }
   return launch_status();
 }
+
+// ============================================================================
+// Dense solve that allocates nothing.
+//
+// For callers that cannot allocate device memory: a plug-in inside a host
+// application that owns the GPU's memory pool, or a control loop that must
+// not allocate after start-up (e.g. re-solving lens charges whenever the
+// electrode voltages change).  The pivot steps and the row permutation of
+// the factorisation live in this file-scope device array instead of caller
+// or library allocations: every GPU that loads the library holds it
+// (256 KiB) until the process exits, and it bounds N to NOALLOC_MAX_N.
+// ============================================================================
+#include <mutex>
+
+namespace tb {
+constexpr int64_t NOALLOC_MAX_N = 32768;
+static __device__ __align__(256) int32_t g_lu_noalloc_scratch[2 * NOALLOC_MAX_N];
+
+static std::mutex g_noalloc_mutex;
+static int32_t* g_noalloc_addr[64] = {nullptr};
+}  // namespace tb
+
+extern "C" int tb_lu_solve_noalloc(double* A, int64_t lda, int64_t N, const double* F, int64_t ldf, double* X,
+                                   int64_t ldx, int64_t nrhs, tb_stream_t stream) {
+  if (N < 0 || N > tb::NOALLOC_MAX_N) return tb::BAD_ARG;
+  if (nrhs < 0 || lda < N || ldf < N || ldx < N) return tb::BAD_ARG;
+  if (N == 0 || nrhs == 0) return tb::OK;
+  if (!A || !F || !X || F == X) return tb::BAD_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return tb::CUDA_ERR;
+  int32_t* scratch = nullptr;
+  {
+    // Once per device, with that device current: the host-side name of the
+    // array is not a device address, so look the address up.
+    std::lock_guard<std::mutex> lock(tb::g_noalloc_mutex);
+    if (!tb::g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, tb::g_lu_noalloc_scratch) != cudaSuccess || !p) return tb::CUDA_ERR;
+      tb::g_noalloc_addr[dev] = static_cast<int32_t*>(p);
+    }
+    scratch = tb::g_noalloc_addr[dev];
+  }
+  int32_t* ipiv = scratch;
+  int32_t* perm = scratch + tb::NOALLOC_MAX_N;  // reset to the identity by every factorisation
+  int st = tb_lu_factor_perm(A, lda, ipiv, perm, N, stream);
+  if (st != tb::OK) return st;
+  return tb_lu_solve_perm(A, lda, perm, N, F, ldf, X, ldx, nrhs, stream);
+}
