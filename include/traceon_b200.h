@@ -341,6 +341,11 @@ int tb_num_sms(void);
  * compared against. */
 int tb_probe_fp64_fma(int blocks, int64_t iters, double *out, tb_stream_t stream);
 
+/* Test helper, no reference counterpart: out[i] = f(x[i]) on the device for
+ * the branch-free functions of the ring-pair loops (fn 0: 1/x, 1: 1/sqrt(x),
+ * 2: log x) and, for comparison, the CUDA library forms (fn 10, 11, 12). */
+int tb_probe_math(const double *x, int64_t n, int fn, double *out, tb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

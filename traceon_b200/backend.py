@@ -211,6 +211,7 @@ _DEV = {
     'tb_trace_rk45': (vp, vp, vp, i64, C.POINTER(TbField), C.POINTER(TbTraceOpts), vp, vp, vp, vp, vp, vp, vp, vp),
     'tb_num_sms': (),
     'tb_probe_fp64_fma': (C.c_int, i64, vp, vp),
+    'tb_probe_math': (vp, i64, C.c_int, vp, vp),
 }
 for _name, _args in _DEV.items():
     _f = getattr(backend_lib, _name)

@@ -9,6 +9,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "tb_fastmath.cuh"
+
 #define TB_HD __host__ __device__ __forceinline__
 
 namespace tb {
@@ -186,16 +188,28 @@ struct Cubic {
 // (the reference's denominators (-2 dr^2 r + dz^2 (2dr - 2r) + 2 dr^3) and
 // 4 r^2 - 4 dr r + rho2 reduce to -2 r0 rho2 and D).
 
-// Potential of a unit ring, without the 1/pi factor.
+// Degree-7 polynomial by Estrin's scheme (depth 3 instead of Horner's 7),
+// given t, t^2 and t^4 shared by the four Cody polynomials.
+__device__ __forceinline__ double estrin8(const double* c, double t, double t2, double t4) {
+  double a = fma(c[1], t, c[0]);
+  double b = fma(c[3], t, c[2]);
+  double d = fma(c[5], t, c[4]);
+  double e = fma(c[7], t, c[6]);
+  return fma(t4, fma(t2, e, d), fma(t2, b, a));
+}
+
+// Potential of a unit ring, without the 1/pi factor: K(1-t) rs / sqrt(D).
 __device__ __forceinline__ double ring_pot_nopi(double r0, double z0, double rs, double zs) {
   double dr = rs - r0, dz = zs - z0;
-  double rho2 = fma(dr, dr, dz * dz);
+  double dz2 = dz * dz;
+  double rho2 = fma(dr, dr, dz2);
   double s = rs + r0;
-  double D = fma(s, s, dz * dz);
-  double invD = 1.0 / D;
-  double t = rho2 * invD;
-  double K = poly_ka(t) - log(t) * poly_kb(t);
-  return K * rs * sqrt(D) * invD;
+  double D = fma(s, s, dz2);
+  double rD = rsqrt_nr(D);
+  double t = rho2 * rD * rD;
+  double t2 = t * t, t4 = t2 * t2;
+  double K = fma(-log_bf(t), estrin8(C_KB, t, t2, t4), estrin8(C_KA, t, t2, t4));
+  return K * rs * rD;
 }
 
 // Accumulates one weighted ring into the partial field sums.  After the
@@ -209,13 +223,14 @@ __device__ __forceinline__ void ring_field_acc(double r0, double z0, double rs, 
   double rho2 = fma(dr, dr, dz2);
   double s = rs + r0;
   double D = fma(s, s, dz2);
-  double q = 1.0 / (rho2 * D);     // 1 / (rho2 D)
-  double sq = sqrt(D);
-  double t = rho2 * rho2 * q;      // rho2 / D
-  double L = -log(t);
-  double K = fma(L, poly_kb(t), poly_ka(t));
-  double E = fma(L, poly_eb(t), poly_ea(t));
-  double c = w * rs * sq * q;      // w rs / (rho2 sqrt(D))
+  double ir = rcp_nr(rho2);        // 1 / rho2
+  double rD = rsqrt_nr(D);         // 1 / sqrt(D)
+  double t = rho2 * rD * rD;       // rho2 / D
+  double t2 = t * t, t4 = t2 * t2;
+  double L = -log_bf(t);
+  double K = fma(L, estrin8(C_KB, t, t2, t4), estrin8(C_KA, t, t2, t4));
+  double E = fma(L, estrin8(C_EB, t, t2, t4), estrin8(C_EA, t, t2, t4));
+  double c = w * rs * rD * ir;     // w rs / (rho2 sqrt(D))
   double m = fma(dr, dr - 2.0 * rs, -dz2);   // dr^2 - 2 dr rs - dz^2
   Sr = fma(c, fma(rho2, K, m * E), Sr);
   Sz = fma(c * dz, E, Sz);

@@ -4,6 +4,7 @@
 // written so the work cannot be removed.
 #include "tb_common.cuh"
 #include "tb_internal.cuh"
+#include "tb_fastmath.cuh"
 #include "../../include/traceon_b200.h"
 
 namespace tb {
@@ -23,7 +24,29 @@ __global__ void __launch_bounds__(256) k_fp64_fma(int64_t iters, double seed, do
   if (s == 12345.678) out[0] = s;  // practically never taken
 }
 
+__global__ void k_probe_math(const double* __restrict__ x, int64_t n, int fn, double* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = x[i], r;
+  switch (fn) {
+    case 0: r = rcp_nr(v); break;
+    case 1: r = rsqrt_nr(v); break;
+    case 2: r = log_bf(v); break;
+    case 10: r = 1.0 / v; break;
+    case 11: r = 1.0 / sqrt(v); break;
+    default: r = log(v); break;
+  }
+  out[i] = r;
+}
+
 }  // namespace tb
+
+extern "C" int tb_probe_math(const double* x, int64_t n, int fn, double* out, tb_stream_t stream) {
+  if (n < 0 || (n > 0 && (!x || !out))) return tb::BAD_ARG;
+  if (n == 0) return tb::OK;
+  tb::k_probe_math<<<unsigned((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(x, n, fn, out);
+  return tb::launch_status();
+}
 
 extern "C" int tb_probe_fp64_fma(int blocks, int64_t iters, double* out, tb_stream_t stream) {
   if (blocks <= 0 || iters <= 0 || !out) return tb::BAD_ARG;

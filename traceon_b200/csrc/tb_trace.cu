@@ -308,11 +308,165 @@ struct BemTeamField {
 
 constexpr int TRACE_THREADS = 256;
 
+// Integrator state of one warp, kept in shared memory rather than registers
+// so that the only values live across a field evaluation are the evaluation
+// point and the loop's own (every lane would otherwise hold its own copy of
+// the whole state).  Each warp of a team keeps its own copy: all lanes of a
+// warp store identical values in the same instruction, while warps of a team
+// only meet at the barriers of the field reduction, so a warp never reads a
+// value that another warp has already advanced.
+struct TeamState {
+  double y[6];
+  double k[6][6];
+  double t, h, hmax, qm;
+  int64_t nrow, accepted, attempts;
+  int status;
+};
+
+// rk45_particle (above) with its state in shared memory, for the BEM teams.
 template <int TW>
-__global__ void __launch_bounds__(TRACE_THREADS, 3) k_trace_bem(TraceParams P) {
+__device__ void rk45_team(const TraceParams& P, int64_t idx, BemTeamField<TW>& field, volatile TeamState* S,
+                          bool writer) {
+  for (int c = 0; c < 6; c++) S->y[c] = P.start[idx * 6 + c];
+  S->qm = P.qm[idx];
+  S->t = P.t0 ? P.t0[idx] : 0.0;
+  {
+    const double V = sqrt(S->y[3] * S->y[3] + S->y[4] * S->y[4] + S->y[5] * S->y[5]);
+    S->hmax = STEP_MAX / V;
+    S->h = S->hmax;
+  }
+  S->nrow = 1;
+  S->accepted = 0;
+  S->attempts = 0;
+  S->status = TRACE_EXITED;
+  if (writer && P.rows) {
+    double* r = P.rows + idx * P.max_rows * 7;
+    r[0] = S->t;
+    for (int c = 0; c < 6; c++) r[1 + c] = S->y[c];
+  }
+  if (writer && P.plane)
+    for (int c = 0; c < 7; c++) P.plane[idx * 7 + c] = __longlong_as_double(0x7ff8000000000000LL);
+  const double atol = P.atol;
+
+  for (;;) {
+    {
+      double y[6];
+      for (int c = 0; c < 6; c++) y[c] = S->y[c];
+      if (!in_bounds(P.bounds, y)) break;
+    }
+    if (S->attempts >= P.max_attempts) {
+      S->status = TRACE_MAX_ATTEMPTS;
+      break;
+    }
+    S->attempts = S->attempts + 1;
+#pragma unroll 1
+    for (int s = 0; s < 6; s++) {
+      double p[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        double v = S->y[c];
+        for (int j = 0; j < s; j++) v += RK_B[s][j] * S->k[j][c];
+        p[c] = v;
+      }
+      double E[3], H[3];
+      field(p, E, H);
+      double u[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        double v = S->y[3 + c];
+        for (int j = 0; j < s; j++) v += RK_B[s][j] * S->k[j][3 + c];
+        u[c] = v;
+      }
+      const double h = S->h, qm = S->qm;
+      double cx = u[1] * H[2] - u[2] * H[1];
+      double cy = u[2] * H[0] - u[0] * H[2];
+      double cz = u[0] * H[1] - u[1] * H[0];
+      S->k[s][0] = h * u[0];
+      S->k[s][1] = h * u[1];
+      S->k[s][2] = h * u[2];
+      S->k[s][3] = h * qm * (E[0] + MU0 * cx);
+      S->k[s][4] = h * qm * (E[1] + MU0 * cy);
+      S->k[s][5] = h * qm * (E[2] + MU0 * cz);
+    }
+    const double h = S->h;
+    double ep = 0.0, ev = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double a = 0.0, b = 0.0;
+      for (int j = 0; j < 6; j++) {
+        a += RK_CT[j] * S->k[j][c];
+        b += RK_CT[j] * S->k[j][c + 3];
+      }
+      ep = fmax(ep, fabs(a));
+      ev = fmax(ev, fabs(b));
+    }
+    const double err = ep + h * ev;
+    if (!(err == err)) {
+      S->status = TRACE_NONFINITE;
+      break;
+    }
+    if (err <= atol) {
+      double y[6], yn[6];
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        y[c] = S->y[c];
+        yn[c] = y[c] + (RK_CH[0] * S->k[0][c] + RK_CH[1] * S->k[1][c] + RK_CH[2] * S->k[2][c] +
+                        RK_CH[3] * S->k[3][c] + RK_CH[4] * S->k[4][c] + RK_CH[5] * S->k[5][c]);
+      }
+      const double t = S->t;
+      if (P.record_plane && ((y[2] - P.plane_z > 0) != (yn[2] - P.plane_z > 0))) {
+        double cr[7];
+        hermite_crossing(h, y, yn, P.plane_z, t, cr);
+        if (writer && P.plane)
+          for (int c = 0; c < 7; c++) P.plane[idx * 7 + c] = cr[c];
+      }
+      bool finite = true;
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        S->y[c] = yn[c];
+        finite = finite && isfinite(yn[c]);
+      }
+      S->t = t + h;
+      S->accepted = S->accepted + 1;
+      if (P.rows) {
+        const int64_t nrow = S->nrow;
+        if (writer) {
+          double* r = P.rows + (idx * P.max_rows + nrow) * 7;
+          r[0] = t + h;
+          for (int c = 0; c < 6; c++) r[1 + c] = yn[c];
+        }
+        S->nrow = nrow + 1;
+      }
+      if (!finite) {
+        S->status = TRACE_NONFINITE;
+        break;
+      }
+      if (P.rows && S->nrow >= P.max_rows) {
+        S->status = TRACE_ROWS_FULL;
+        break;
+      }
+    }
+    S->h = fmin(0.9 * h * pow(atol / err, 0.2), S->hmax);
+  }
+  if (writer) {
+    if (P.nrows) P.nrows[idx] = P.rows ? S->nrow : 1;
+    if (P.status) P.status[idx] = S->status;
+    if (P.final_state) {
+      P.final_state[idx * 7] = S->t;
+      for (int c = 0; c < 6; c++) P.final_state[idx * 7 + 1 + c] = S->y[c];
+    }
+    if (P.counters) {
+      P.counters[idx * 2] = S->accepted;
+      P.counters[idx * 2 + 1] = S->attempts;
+    }
+  }
+}
+
+template <int TW>
+__global__ void __launch_bounds__(TRACE_THREADS, 2) k_trace_bem(TraceParams P) {
   constexpr int T = 32 * TW;
   constexpr int TEAMS = TRACE_THREADS / T;
-  __shared__ double s_k[TEAMS][6][6];
+  __shared__ TeamState s_state[TEAMS][TW];
   __shared__ double s_red[TEAMS][TW][6];
   __shared__ int64_t s_idx[TEAMS];
   const int team = threadIdx.x / T, lt = threadIdx.x % T;
@@ -330,7 +484,8 @@ __global__ void __launch_bounds__(TRACE_THREADS, 3) k_trace_bem(TraceParams P) {
       team_barrier(team, T);
     }
     if (idx >= P.n) break;
-    rk45_particle(P, idx, field, s_k[team], lt == 0);
+    rk45_team(P, idx, field, &s_state[team][lt / 32], lt == 0);
+    __syncwarp();
   }
 }
 
