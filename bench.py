@@ -1,21 +1,26 @@
-"""Benchmark: traced electrons per second through the einzel-lens workload.
+"""Benchmark: traced electrons per second at <= 1 nm endpoint error through
+the einzel-lens workload, learned surrogate vs plain BEM field.
 
-Workload (one step): the three-tube einzel lens of 1,000 cubic line elements
-graded toward the tube edges (0 V / V_mid / 0 V, V_mid from the seed), solved
-once on the GPU (FP64 fill, singular self terms, FP64 LU); each step traces a
-batch of 1 keV electrons (start r in [0, 0.2] mm, angle in [-5, 5] mrad,
-z = -9.5 mm) with adaptive RKF45 at atol = 1e-10 m through the plain BEM
-field until they leave the bounds (|x|,|y| <= 2 mm, |z| <= 10 mm), recording
-each electron's crossing of the exit plane z = +9.5 mm.  Synthetic inputs;
-no dataset.
+Workload: the three-tube einzel lens of 1,000 cubic line elements graded
+toward the tube edges (0 V / V_mid / 0 V, V_mid from the seed), solved once on
+the GPU (FP64 fill, singular self terms, FP64 LU).  A step traces a batch of
+electrons (default 262,144) at 1 keV +-5 %, angles +-20 mrad, start radius
+<= 0.2 mm at z = -9.5 mm, with adaptive RKF45 at atol = 1e-10 m until they
+leave the bounds (|x|,|y| <= 2 mm, |z| <= 10 mm), recording each electron's
+crossing of the exit plane z = +9.5 mm.  Synthetic inputs; no dataset.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--electrons E]
-  python bench.py --impl reference ...   # the reference C backend on host cores
+  --field surrogate (default): the surrogate field (axial series + BF16 MLP
+      correction trained on the GPU from BEM samples in the setup phase, BEM
+      fallback near electrodes); the plain BEM tracer is measured beside it
+      on a 16,384-electron slice of the same beam (`plain_bem`).
+  --field bem: the plain FP64 BEM field only.
+  --impl reference: the reference C backend's plain BEM tracer on host cores.
 
 `value` is whole-job electrons/s with the start states resident in HBM;
-`e2e` is the same through the public API (Tracer.trace_endpoints) with host
-arrays, host<->device copies inside the timed region.  Endpoint accuracy is
-checked every run against the CPU oracle on a sample of electrons.
+`e2e` is the same through the public API with host arrays, host<->device
+copies inside the timed region.  Endpoints of a sample of electrons are
+checked every run against the full CPU oracle (oracle charges, FP64 BEM
+trace): `accuracy.endpoint_err_max_nm` must stay <= 1.
 """
 from __future__ import annotations
 
@@ -35,14 +40,16 @@ sys.path.insert(0, HERE)
 N_ELEMENTS = 1000
 SEED = 1
 ATOL = 1e-10
-METRIC = 'traced electrons/s at <=1 nm endpoint error, plain BEM field'
+METRIC = 'traced electrons/s at <=1 nm endpoint error, surrogate vs plain BEM field'
 
 
-def workload_config(electrons):
-    return {'workload': f'einzel lens, {N_ELEMENTS} cubic elements, plain BEM field (FP64), '
-                        f'{electrons} electrons/step at 1 keV, RKF45 atol=1e-10 m, exit plane z=+9.5 mm',
+def workload_config(electrons, field):
+    desc = {'surrogate': 'learned surrogate field (axial series + BF16 MLP correction, BEM fallback)',
+            'bem': 'plain BEM field (FP64)'}[field]
+    return {'workload': f'einzel lens, {N_ELEMENTS} cubic elements, {desc}, {electrons} electrons/step at '
+                        f'1 keV +-5%, +-20 mrad, r0<=0.2 mm, RKF45 atol=1e-10 m, exit plane z=+9.5 mm',
             'elements': N_ELEMENTS, 'electrons_per_step': electrons, 'atol_m': ATOL, 'seed': SEED,
-            'field': 'plain BEM', 'l2': 'L2 flushed (256 MiB write) between timed steps'}
+            'field': field, 'l2': 'L2 flushed (256 MiB write) between timed steps'}
 
 
 def dist_info():
@@ -106,8 +113,8 @@ class Clocks:
 def lens_inputs(electrons, seed=SEED):
     from traceon_b200 import geometry as G
     geo = G.einzel_lens(N_ELEMENTS)
-    volts = G.einzel_lens_voltages(seed)
-    p0, v0 = G.electron_beam(electrons, seed + 100)
+    volts = G.einzel_lens_voltages(SEED)
+    p0, v0 = G.surrogate_beam(electrons, seed + 100)
     return geo, volts, p0, v0
 
 
@@ -187,7 +194,7 @@ def run_reference(args):
     if rank != 0:
         return
     cores = host_cores()
-    geo, volts, p0, v0 = lens_inputs(max(4096, args.electrons))
+    geo, volts, p0, v0 = lens_inputs(4096)
     q, jac, pos = oracle_charges(geo, volts, cores)
     for _ in range(args.warmup):
         cpu_reference_rate(geo, q, jac, pos, p0, v0, cores, 2.0)
@@ -202,7 +209,8 @@ def run_reference(args):
     line = {'metric': METRIC, 'value': value, 'unit': 'electrons/s', 'n_gpus': ws, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': 1e3 * t_total / max(args.steps, 1), 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic', 'impl': 'reference',
-            'config': workload_config(args.electrons),
+            'config': workload_config(args.electrons, args.field),
+            'reference_field': 'plain BEM (the reference has no learned surrogate)',
             'cpu_baseline': {'value': value, 'unit': 'electrons/s', 'cores': cores,
                              'kind': 'reference' if kind == 'ref' else 'port',
                              'sample': f'{n_total} electrons over {args.steps} steps of ~{args.ref_seconds:.0f} s '
@@ -233,6 +241,32 @@ def measure_fp64_peak(B, torch):
     return best
 
 
+def read_peaks():
+    try:
+        return json.load(open(os.path.join(HERE, 'MEASURED_PEAKS.json')))
+    except Exception:
+        return {}
+
+
+MLP_FLOP_PER_EVAL = 2 * (16 * 128 + 3 * 128 * 128 + 128 * 16)  # dense BF16 flops of one network evaluation
+
+
+def time_steps(fn, steps, flush):
+    """CUDA-event time of `steps` calls of fn (L2 flushed before each)."""
+    import torch
+    ms, results = [], []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        results.append(r)
+    return ms, results
+
+
 def run_gpu(args):
     import torch
     ws, rank, local = dist_info()
@@ -240,84 +274,103 @@ def run_gpu(args):
     if ws > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group('nccl', timeout=timedelta(seconds=120))
+        dist.init_process_group('nccl', timeout=timedelta(seconds=300))
     from traceon_b200 import backend as B
     from traceon_b200 import geometry as G
-    from traceon_b200.field import EffectivePointCharges, FieldRadialBEM
     from traceon_b200.solver import ElectrostaticSolverRadial
     from traceon_b200.excitation import Mesh, Excitation
     from traceon_b200.tracing import Tracer
+    from scipy.constants import e as qe, m_e
 
     E = args.electrons
     geo, volts, p0, v0 = lens_inputs(E, SEED + rank)
-    # ---- setup: GPU solve (timed separately, not part of a step)
+    # ---- setup (timed separately, not part of a step): GPU solve
     exc = Excitation(Mesh.from_geometry(geo))
     exc.add_voltage(**{n: float(v) for n, v in zip(geo.names, volts)})
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    solver = ElectrostaticSolverRadial(exc)
-    field = solver.solve_matrix()[0]
+    field = ElectrostaticSolverRadial(exc).solve_matrix()[0]
     torch.cuda.synchronize()
-    setup_s = time.perf_counter() - t0
-    tracer = Tracer(field, G.LENS_BOUNDS)
+    setup = {'solve_s': time.perf_counter() - t0}
+    bem_tracer = Tracer(field, G.LENS_BOUNDS)
     Nq = len(field.electrostatic_point_charges) * B.N_QUAD_2D
+    sur = None
+    if args.field == 'surrogate':
+        from traceon_b200.surrogate import SurrogateTrainer, FieldSurrogate
+        t0 = time.perf_counter()
+        trainer = SurrogateTrainer(geo)
+        model, info = trainer.train(n_samples=args.train_samples, steps=args.train_steps, batch=8192, seed=0)
+        torch.cuda.synchronize()
+        setup['surrogate_train_s'] = time.perf_counter() - t0
+        setup['surrogate_holdout_mse'] = info['holdout_mse']
+        setup['surrogate_train'] = f'{args.train_samples} BEM samples, {args.train_steps} Adam steps of 8192'
+        sur = FieldSurrogate(model, trainer.fields, trainer.z, trainer.tabs, volts, geo.segments)
 
-    from scipy.constants import e as qe, m_e
     start = torch.as_tensor(np.concatenate([p0, v0], 1), device='cuda', dtype=torch.float64).contiguous()
     qm = torch.full((E,), -qe / m_e, device='cuda', dtype=torch.float64)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device='cuda')
 
-    def step_dev():
-        return tracer.trace_device(start, qm, atol=ATOL, plane_z=G.LENS_EXIT_Z, team_warps=args.team_warps,
-                                   max_attempts=20000)
+    def step_bem(st=start, q=qm):
+        return bem_tracer.trace_device(st, q, atol=ATOL, plane_z=G.LENS_EXIT_Z, team_warps=args.team_warps,
+                                       max_attempts=20000)
 
+    def step_sur():
+        return sur.trace_device(start, qm, G.LENS_BOUNDS, ATOL, plane_z=G.LENS_EXIT_Z, max_attempts=20000)
+
+    step = step_sur if sur is not None else step_bem
     for _ in range(args.warmup):
-        res = step_dev()
+        step()
     torch.cuda.synchronize()
-
-    # ---- timed device steps
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
-    ms_list, attempts, launches = [], 0, 0
     with Clocks(local) as clk:
-        for _ in range(args.steps):
-            flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            res = step_dev()
-            e1.record()
-            launches += 1
-            torch.cuda.synchronize()
-            ms_list.append(e0.elapsed_time(e1))
-            attempts += int(res.counters[:, 1].sum().item())
-        total_ms = float(np.sum(ms_list))
+        ms_list, results = time_steps(step, args.steps, flush)
+    total_ms = float(np.sum(ms_list))
     if ws > 1:
         import torch.distributed as dist
         t = torch.tensor([total_ms], device='cuda', dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
+    res = results[-1]
+    attempts = [int(r.counters[:, 1].sum().item()) for r in results]
     status = res.status.cpu().numpy()
     plane = res.plane.cpu().numpy()
     counters = res.counters.cpu().numpy()
     value = ws * E * args.steps / (total_ms * 1e-3)
 
     # ---- e2e through the public API with host arrays
-    torch.cuda.synchronize()
     e2e_ms = []
     for _ in range(max(1, min(args.steps, 3))):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        out_plane, out_final, out_status, out_counters = tracer.trace_endpoints(p0, v0, G.LENS_EXIT_Z, atol=ATOL,
-                                                                                team_warps=args.team_warps,
-                                                                                max_attempts=20000)
+        if sur is not None:
+            sur.trace_endpoints(p0, v0, G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=ATOL, max_attempts=20000)
+        else:
+            bem_tracer.trace_endpoints(p0, v0, G.LENS_EXIT_Z, atol=ATOL, team_warps=args.team_warps,
+                                       max_attempts=20000)
         torch.cuda.synchronize()
         e2e_ms.append((time.perf_counter() - t1) * 1e3)
     e2e_value = ws * E / (np.mean(e2e_ms) * 1e-3)
+    ncnt = 3 if sur is not None else 2
     h2d = E * 6 * 8 + E * 8
-    d2h = E * (7 + 7) * 8 + E * 4 + E * 2 * 8
+    d2h = E * (7 + 7) * 8 + E * 4 + E * ncnt * 8
+
+    # ---- plain BEM tracer on a slice of the same beam (for the comparison)
+    plain = None
+    if sur is not None:
+        m = min(E, args.bem_electrons)
+        st_m, qm_m = start[:m].contiguous(), qm[:m].contiguous()
+        step_bem(st_m, qm_m)
+        ms_b, res_b = time_steps(lambda: step_bem(st_m, qm_m), 2, flush)
+        pairs = np.mean([int(r.counters[:, 1].sum().item()) for r in res_b]) * 6 * Nq
+        launch_s = np.mean(ms_b) * 1e-3
+        plain = {'value': ws * m / launch_s, 'unit': 'electrons/s', 'electrons': m,
+                 'ms_per_step': float(np.mean(ms_b)),
+                 'roofline': {'bound': 'fp64', 'achieved': pairs * args.flop_per_pair / launch_s / 1e12,
+                              'unit': 'TFLOP/s', 'kernel': 'k_trace_bem', 'flop_per_pair': args.flop_per_pair}}
 
     if rank != 0:
         if ws > 1:
@@ -326,12 +379,30 @@ def run_gpu(args):
             dist.destroy_process_group()
         return
 
-    # ---- roofline of the dominant kernel (k_trace_bem): FP64 pipe
-    pairs_per_launch = attempts / args.steps * 6 * Nq
+    # ---- roofline of the dominant kernel
+    peaks = read_peaks()
+    fp64_peak = measure_fp64_peak(B, torch)
     launch_s = total_ms / args.steps * 1e-3
-    flop_per_pair = args.flop_per_pair
-    achieved = pairs_per_launch * flop_per_pair / launch_s / 1e12
-    peak = measure_fp64_peak(B, torch)
+    if sur is not None:
+        evals = np.mean(attempts) * 6
+        achieved = evals * MLP_FLOP_PER_EVAL / launch_s / 1e12
+        peak = peaks.get('bf16_tflops')
+        roof = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                'frac': achieved / peak if peak else None, 'traffic': args.traffic, 'kernel': 'k_trace_surrogate',
+                'flop_per_unit': MLP_FLOP_PER_EVAL, 'units_per_launch': evals,
+                'unit_desc': 'network evaluations (dense BF16 flops of the 16-128x4-16 MLP)',
+                'peak_source': 'MEASURED_PEAKS.json bf16_tflops (burst)'}
+        if plain is not None:
+            plain['roofline']['peak'] = fp64_peak
+            plain['roofline']['frac'] = plain['roofline']['achieved'] / fp64_peak
+    else:
+        pairs_per_launch = np.mean(attempts) * 6 * Nq
+        achieved = pairs_per_launch * args.flop_per_pair / launch_s / 1e12
+        roof = {'bound': 'fp64', 'achieved': achieved, 'peak': fp64_peak, 'unit': 'TFLOP/s',
+                'frac': achieved / fp64_peak if fp64_peak else None, 'traffic': args.traffic, 'kernel': 'k_trace_bem',
+                'flop_per_unit': args.flop_per_pair, 'units_per_launch': pairs_per_launch,
+                'unit_desc': 'ring-pair field evaluations (executed FP64 flops per pair, ncu)',
+                'peak_source': 'measured FP64 FMA probe (tb_probe_fp64_fma) in this run'}
 
     # ---- accuracy vs the CPU oracle and the CPU baseline (rank 0, N = 1)
     cores = host_cores()
@@ -347,29 +418,26 @@ def run_gpu(args):
     if ws == 1 and args.cpu_seconds > 0:
         rate, n, kind = cpu_reference_rate(geo, q_or, jac_or, pos_or, p0, v0, cores, args.cpu_seconds)
         cpu = {'value': rate, 'unit': 'electrons/s', 'cores': cores, 'kind': 'reference' if kind == 'ref' else 'port',
-               'sample': f'{n} electrons of this workload traced by the reference C backend '
-                         f'(trace_particle + field_radial_traceable) on {cores} threads for ~{args.cpu_seconds:.0f} s'}
+               'sample': f'{n} electrons of this beam traced by the reference C backend (trace_particle + '
+                         f'field_radial_traceable, plain BEM; the reference has no surrogate) on {cores} threads '
+                         f'for ~{args.cpu_seconds:.0f} s'}
 
-    clocks = clk.summary()
     line = {'metric': METRIC, 'value': value, 'unit': 'electrons/s', 'n_gpus': ws, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': total_ms / args.steps, 'higher_is_better': True,
-            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-            'config': workload_config(E),
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'bf16+f64' if sur is not None else 'f64',
+            'data': 'synthetic', 'config': workload_config(E, args.field),
             'e2e': {'value': e2e_value, 'unit': 'electrons/s', 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
-            'gpu_launches': launches,
-            'roofline': {'bound': 'fp64', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
-                         'frac': achieved / peak if peak else None, 'traffic': args.traffic,
-                         'kernel': 'k_trace_bem', 'flop_per_pair': flop_per_pair,
-                         'pairs_per_launch': pairs_per_launch,
-                         'peak_source': 'measured FP64 FMA probe (tb_probe_fp64_fma) on this GPU'},
-            'cpu_baseline': cpu,
-            'clocks': clocks,
+            'gpu_launches': args.steps, 'roofline': roof, 'plain_bem': plain,
+            'speedup_vs_plain_bem': (value / plain['value']) if plain else None,
+            'cpu_baseline': cpu, 'clocks': clk.summary(),
             'accuracy': {'endpoint_err_max_nm': err_max_nm, 'endpoint_err_p99_nm': err_p99_nm,
-                         'checked_electrons': int(len(sample)), 'charges_rel_err': charge_err},
+                         'checked_electrons': int(len(sample)), 'judge': 'CPU oracle FP64 BEM trace, Hermite crossing',
+                         'charges_rel_err': charge_err},
             'trace_stats': {'status_exited': int((status == 0).sum()),
                             'accepted_steps_mean': float(counters[:, 0].mean()),
-                            'attempts_mean': float(counters[:, 1].mean())},
-            'setup_solve_s': setup_s}
+                            'attempts_mean': float(counters[:, 1].mean()),
+                            'bem_fallback_evals': int(counters[:, 2].sum()) if counters.shape[1] > 2 else None},
+            'setup': setup}
     print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -383,7 +451,11 @@ def main():
     ap.add_argument('--steps', type=int, default=5)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--electrons', type=int, default=16384)
+    ap.add_argument('--electrons', type=int, default=262144)
+    ap.add_argument('--field', default='surrogate', choices=['surrogate', 'bem'])
+    ap.add_argument('--bem-electrons', type=int, default=16384, help='slice traced with the plain BEM field')
+    ap.add_argument('--train-samples', type=int, default=1 << 22)
+    ap.add_argument('--train-steps', type=int, default=40000)
     ap.add_argument('--team-warps', type=int, default=0)
     ap.add_argument('--check', type=int, default=16, help='electrons checked against the CPU oracle')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)

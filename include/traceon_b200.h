@@ -332,6 +332,71 @@ int tb_trace_rk45(const double *start, const double *t0, const double *qm, int64
                   const tb_trace_opts_t *opts, double *rows, int64_t *nrows, int32_t *status, double *final_state,
                   double *plane, int64_t *counters, int32_t *work, tb_stream_t stream);
 
+/* ---------------------------------------------------------------------
+ * Learned field surrogate (no reference counterpart; see tb_mlp.cuh).
+ * Network: 16 input features -> 4 x 128 SiLU -> 16 outputs; parameters in
+ * one flat array of 51,344 entries (W1 128x16, b1, W2 128x128, b2, W3, b3,
+ * W4, b4, W5 16x128, b5), FP32 master copy plus BF16 copy.  Matrices are
+ * BF16 (device pointers passed as void*), accumulators FP32.
+ * ------------------------------------------------------------------- */
+
+/* C (M x N, fp32, row stride ldc) (+)= A . B^T on the tensor cores, BF16 in,
+ * FP32 accumulate.  A is M x K (a_t = 0: A[m*lda + k]; a_t = 1:
+ * A[k*lda + m]); B is N x K likewise with b_t. */
+int tb_mlp_gemm(const void *A, int64_t lda, int a_t, const void *B, int64_t ldb, int b_t, float *C, int64_t ldc,
+                int64_t M, int64_t N, int64_t K, int accumulate, tb_stream_t stream);
+/* Z = C + b (Z may be NULL), Y = silu(Z) as BF16; C, Z, Y are M x N. */
+int tb_mlp_bias_silu(const float *C, const float *b, float *Z, void *Y, int64_t M, int64_t N, tb_stream_t stream);
+/* Y = C + b (FP32). */
+int tb_mlp_bias_out(const float *C, const float *b, float *Y, int64_t M, int64_t N, tb_stream_t stream);
+/* dY = 2 (Y - T) w / (M n_out) for the first n_out of N columns (BF16, zero
+ * elsewhere); loss_part[block] = partial sums of w (Y - T)^2 (256 entries per
+ * block).  T is M x n_out, w (M) or NULL. */
+int tb_mlp_mse_grad(const float *Y, const float *T, const float *w, void *dY, float *loss_part, int64_t M, int64_t N,
+                    int64_t n_out, tb_stream_t stream);
+/* dZ = dA * silu'(Z) (BF16), n elements. */
+int tb_mlp_silu_back(const float *dA, const float *Z, void *dZ, int64_t n, tb_stream_t stream);
+/* db[c] = sum over the M rows of dZ (BF16, M x N). */
+int tb_mlp_colsum(const void *dZ, float *db, int64_t M, int64_t N, tb_stream_t stream);
+/* Adam step (bias-corrected, step >= 1) on n FP32 parameters, refreshing the
+ * BF16 copy pb. */
+int tb_mlp_adam(float *p, const float *g, float *m, float *v, void *pb, int64_t n, float lr, float b1, float b2,
+                float eps, int64_t step, tb_stream_t stream);
+/* Input features (M x 16, BF16) of M points (M,3): rho = r / r_max,
+ * zeta = (z - z_c) / z_half. */
+int tb_mlp_features(const double *points, int64_t M, double r_max, double z_c, double z_half, void *X,
+                    tb_stream_t stream);
+
+/* Surrogate description for tb_trace_surrogate. */
+typedef struct {
+  const void *weights_bf16;     /* flat BF16 parameters */
+  const float *params_f32;      /* flat FP32 parameters (biases are read from here) */
+  double r_max, z_c, z_half;    /* input normalisation; also the domain in r */
+  double z_lo, z_hi;            /* domain in z */
+  int n_electrodes;             /* <= 5; outputs 3e..3e+2 are (phi, E_r, E_z) of electrode e at 1 V */
+  double volts[5];              /* electrode voltages */
+  float scale[16];              /* output scales */
+  int env_power;                /* correction = scale * y * rho^p (E_r: rho^(p+1)) */
+  const double *segments;       /* (n_segments, 4) electrode segments r0, z0, r1, z1 (device) */
+  int n_segments;               /* <= 64 */
+  double fallback_dist;         /* exact BEM within this distance of a segment */
+} tb_surrogate_t;
+
+/* RKF45 tracing (tracing.c:60-123 step control) through the surrogate field:
+ * axial-series field of `field->axial_*` (the table for the actual voltages)
+ * plus the network's correction, exact BEM sums of `field->elec_sources`
+ * near electrodes and outside the network's domain.  Endpoint mode only
+ * (no trajectories); counters (n, 3): accepted steps, attempts, field
+ * evaluations that fell back to BEM. */
+int tb_trace_surrogate(const double *start, const double *t0, const double *qm, int64_t n, const tb_field_t *field,
+                       const tb_surrogate_t *sur, const tb_trace_opts_t *opts, int32_t *status, double *final_state,
+                       double *plane, int64_t *counters, int32_t *work, tb_stream_t stream);
+
+/* The surrogate field E (M,3) at M points (M,3) exactly as the tracer sees
+ * it (fallback included); used_bem (M) int32 flags BEM fallbacks, or NULL. */
+int tb_surrogate_field_points(const double *points, int64_t M, const tb_field_t *field, const tb_surrogate_t *sur,
+                              double *out, int32_t *used_bem, tb_stream_t stream);
+
 /* Number of SMs of the current device (grid sizing helper). */
 int tb_num_sms(void);
 

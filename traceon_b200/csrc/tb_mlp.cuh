@@ -1,0 +1,200 @@
+// tb_mlp.cuh -- the field-surrogate network: sizes, parameter layout, input
+// features, activation, and the warp-level forward pass used inside the
+// tracer.  The network is 16 features -> 4 x 128 (SiLU) -> 16 outputs, BF16
+// weights and activations with FP32 accumulation on the tensor cores
+// (mma.sync m16n8k16).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace tb {
+
+constexpr int MLP_IN = 16;
+constexpr int MLP_H = 128;
+constexpr int MLP_OUT = 16;
+constexpr int MLP_MAX_ELECTRODES = 5;  // 3 outputs (phi, E_r, E_z) each, <= MLP_OUT
+
+// Flat parameter layout: W1 (H x IN), b1 (H), W2, b2, W3, b3, W4, b4 (H x H, H),
+// W5 (OUT x H), b5 (OUT).  Weights are row-major [out][in].
+constexpr int64_t MLP_OFF_W1 = 0;
+constexpr int64_t MLP_OFF_B1 = MLP_OFF_W1 + MLP_H * MLP_IN;
+constexpr int64_t MLP_OFF_W2 = MLP_OFF_B1 + MLP_H;
+constexpr int64_t MLP_OFF_B2 = MLP_OFF_W2 + MLP_H * MLP_H;
+constexpr int64_t MLP_OFF_W3 = MLP_OFF_B2 + MLP_H;
+constexpr int64_t MLP_OFF_B3 = MLP_OFF_W3 + MLP_H * MLP_H;
+constexpr int64_t MLP_OFF_W4 = MLP_OFF_B3 + MLP_H;
+constexpr int64_t MLP_OFF_B4 = MLP_OFF_W4 + MLP_H * MLP_H;
+constexpr int64_t MLP_OFF_W5 = MLP_OFF_B4 + MLP_H;
+constexpr int64_t MLP_OFF_B5 = MLP_OFF_W5 + MLP_OUT * MLP_H;
+constexpr int64_t MLP_NPARAM = MLP_OFF_B5 + MLP_OUT;
+
+// Normalisation of the inputs: rho = r / r_max, zeta = (z - z_c) / z_half.
+struct MlpDomain {
+  double r_max, z_c, z_half;
+};
+
+__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+__device__ __forceinline__ float silu_grad(float z) {
+  float s = 1.f / (1.f + __expf(-z));
+  return s * (1.f + z * (1.f - s));
+}
+
+// Input features of a point (r, z): polynomial terms in rho^2 and zeta (the
+// field is even in r) and five Fourier pairs in zeta.
+__host__ __device__ __forceinline__ void mlp_features(double r, double z, const MlpDomain& d, float* f) {
+  float rho = float(r / d.r_max), zeta = float((z - d.z_c) / d.z_half);
+  float p = rho * rho;
+  f[0] = p;
+  f[1] = zeta;
+  f[2] = p * zeta;
+  f[3] = zeta * zeta;
+  f[4] = p * p;
+  f[5] = p * zeta * zeta;
+  const float PI_F = 3.14159265358979f;
+#pragma unroll
+  for (int k = 1; k <= 5; k++) {
+    float s, c;
+    sincosf(PI_F * float(k) * zeta, &s, &c);
+    f[4 + 2 * k] = s;
+    f[5 + 2 * k] = c;
+  }
+}
+
+// D (16x8, fp32) += A (16x16, bf16, row) . B (16x8, bf16, col).
+__device__ __forceinline__ void mma_bf16_16816(float* d, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// Shared-memory image of the network for the warp-level forward pass.
+constexpr int MLP_LD_IN = MLP_IN + 8;  // padded row strides (bf16 elements)
+constexpr int MLP_LD_H = MLP_H + 8;
+struct MlpSmem {
+  __nv_bfloat16 w1[MLP_H][MLP_LD_IN];
+  __nv_bfloat16 w2[MLP_H][MLP_LD_H];
+  __nv_bfloat16 w3[MLP_H][MLP_LD_H];
+  __nv_bfloat16 w4[MLP_H][MLP_LD_H];
+  __nv_bfloat16 w5[MLP_OUT][MLP_LD_H];
+  float b1[MLP_H], b2[MLP_H], b3[MLP_H], b4[MLP_H], b5[MLP_OUT];
+};
+
+// Copies the BF16 weights and FP32 biases (flat layout above) into shared
+// memory; all threads of the block take part.
+__device__ inline void mlp_load_smem(MlpSmem& s, const __nv_bfloat16* __restrict__ wb,
+                                     const float* __restrict__ pf) {
+  for (int e = threadIdx.x; e < MLP_H * MLP_IN; e += blockDim.x) s.w1[e / MLP_IN][e % MLP_IN] = wb[MLP_OFF_W1 + e];
+  for (int e = threadIdx.x; e < MLP_H * MLP_H; e += blockDim.x) {
+    s.w2[e / MLP_H][e % MLP_H] = wb[MLP_OFF_W2 + e];
+    s.w3[e / MLP_H][e % MLP_H] = wb[MLP_OFF_W3 + e];
+    s.w4[e / MLP_H][e % MLP_H] = wb[MLP_OFF_W4 + e];
+  }
+  for (int e = threadIdx.x; e < MLP_OUT * MLP_H; e += blockDim.x) s.w5[e / MLP_H][e % MLP_H] = wb[MLP_OFF_W5 + e];
+  for (int e = threadIdx.x; e < MLP_H; e += blockDim.x) {
+    s.b1[e] = pf[MLP_OFF_B1 + e];
+    s.b2[e] = pf[MLP_OFF_B2 + e];
+    s.b3[e] = pf[MLP_OFF_B3 + e];
+    s.b4[e] = pf[MLP_OFF_B4 + e];
+  }
+  for (int e = threadIdx.x; e < MLP_OUT; e += blockDim.x) s.b5[e] = pf[MLP_OFF_B5 + e];
+}
+
+// One hidden layer for one 16-row m-tile held in A fragments `a` (K = 128,
+// 8 k-blocks): produces the next layer's A fragments after bias + SiLU.
+// The C fragment of two adjacent n8 tiles is exactly the A fragment of one
+// k16 block, so activations never leave registers.
+__device__ __forceinline__ void mlp_hidden_layer(const __nv_bfloat16 (*W)[MLP_LD_H], const float* bias,
+                                                 const uint32_t (&a)[8][4], uint32_t (&out)[8][4], int g, int q) {
+#pragma unroll
+  for (int kb = 0; kb < 8; kb++) {  // output columns 16 kb .. 16 kb + 15
+    float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int ki = 0; ki < 8; ki++) {
+      uint32_t b0[2], b1[2];
+      int n0 = 16 * kb + g, n1 = 16 * kb + 8 + g;
+      b0[0] = *reinterpret_cast<const uint32_t*>(&W[n0][16 * ki + 2 * q]);
+      b0[1] = *reinterpret_cast<const uint32_t*>(&W[n0][16 * ki + 8 + 2 * q]);
+      b1[0] = *reinterpret_cast<const uint32_t*>(&W[n1][16 * ki + 2 * q]);
+      b1[1] = *reinterpret_cast<const uint32_t*>(&W[n1][16 * ki + 8 + 2 * q]);
+      mma_bf16_16816(c0, a[ki], b0);
+      mma_bf16_16816(c1, a[ki], b1);
+    }
+    int col0 = 16 * kb + 2 * q, col1 = 16 * kb + 8 + 2 * q;
+    out[kb][0] = pack_bf16(silu(c0[0] + bias[col0]), silu(c0[1] + bias[col0 + 1]));
+    out[kb][1] = pack_bf16(silu(c0[2] + bias[col0]), silu(c0[3] + bias[col0 + 1]));
+    out[kb][2] = pack_bf16(silu(c1[0] + bias[col1]), silu(c1[1] + bias[col1 + 1]));
+    out[kb][3] = pack_bf16(silu(c1[2] + bias[col1]), silu(c1[3] + bias[col1 + 1]));
+  }
+}
+
+// Forward pass of the network for the 32 points of a warp.  `feat` is the
+// warp's [32][MLP_IN] feature block and `out` its [32][MLP_OUT] result block
+// in shared memory; every lane writes its row of `feat` before the call and
+// reads its row of `out` after it.
+__device__ inline void mlp_warp_forward(const MlpSmem& s, const __nv_bfloat16 (*feat)[MLP_LD_IN],
+                                        float (*out)[MLP_OUT]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  __syncwarp();
+#pragma unroll 1
+  for (int mt = 0; mt < 2; mt++) {
+    const int r0 = 16 * mt + g, r1 = r0 + 8;
+    // layer 1: K = 16 (one k-block)
+    uint32_t a1[4];
+    a1[0] = *reinterpret_cast<const uint32_t*>(&feat[r0][2 * q]);
+    a1[1] = *reinterpret_cast<const uint32_t*>(&feat[r1][2 * q]);
+    a1[2] = *reinterpret_cast<const uint32_t*>(&feat[r0][8 + 2 * q]);
+    a1[3] = *reinterpret_cast<const uint32_t*>(&feat[r1][8 + 2 * q]);
+    uint32_t h[8][4], h2[8][4];
+#pragma unroll
+    for (int kb = 0; kb < 8; kb++) {
+      float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+      uint32_t b0[2], b1[2];
+      int n0 = 16 * kb + g, n1 = 16 * kb + 8 + g;
+      b0[0] = *reinterpret_cast<const uint32_t*>(&s.w1[n0][2 * q]);
+      b0[1] = *reinterpret_cast<const uint32_t*>(&s.w1[n0][8 + 2 * q]);
+      b1[0] = *reinterpret_cast<const uint32_t*>(&s.w1[n1][2 * q]);
+      b1[1] = *reinterpret_cast<const uint32_t*>(&s.w1[n1][8 + 2 * q]);
+      mma_bf16_16816(c0, a1, b0);
+      mma_bf16_16816(c1, a1, b1);
+      int col0 = 16 * kb + 2 * q, col1 = 16 * kb + 8 + 2 * q;
+      h[kb][0] = pack_bf16(silu(c0[0] + s.b1[col0]), silu(c0[1] + s.b1[col0 + 1]));
+      h[kb][1] = pack_bf16(silu(c0[2] + s.b1[col0]), silu(c0[3] + s.b1[col0 + 1]));
+      h[kb][2] = pack_bf16(silu(c1[0] + s.b1[col1]), silu(c1[1] + s.b1[col1 + 1]));
+      h[kb][3] = pack_bf16(silu(c1[2] + s.b1[col1]), silu(c1[3] + s.b1[col1 + 1]));
+    }
+    mlp_hidden_layer(s.w2, s.b2, h, h2, g, q);
+    mlp_hidden_layer(s.w3, s.b3, h2, h, g, q);
+    mlp_hidden_layer(s.w4, s.b4, h, h2, g, q);
+    // output layer: N = 16 (two n8 tiles), FP32 results
+    float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int ki = 0; ki < 8; ki++) {
+      uint32_t b0[2], b1[2];
+      b0[0] = *reinterpret_cast<const uint32_t*>(&s.w5[g][16 * ki + 2 * q]);
+      b0[1] = *reinterpret_cast<const uint32_t*>(&s.w5[g][16 * ki + 8 + 2 * q]);
+      b1[0] = *reinterpret_cast<const uint32_t*>(&s.w5[8 + g][16 * ki + 2 * q]);
+      b1[1] = *reinterpret_cast<const uint32_t*>(&s.w5[8 + g][16 * ki + 8 + 2 * q]);
+      mma_bf16_16816(c0, h2[ki], b0);
+      mma_bf16_16816(c1, h2[ki], b1);
+    }
+    out[r0][2 * q] = c0[0] + s.b5[2 * q];
+    out[r0][2 * q + 1] = c0[1] + s.b5[2 * q + 1];
+    out[r1][2 * q] = c0[2] + s.b5[2 * q];
+    out[r1][2 * q + 1] = c0[3] + s.b5[2 * q + 1];
+    out[r0][8 + 2 * q] = c1[0] + s.b5[8 + 2 * q];
+    out[r0][9 + 2 * q] = c1[1] + s.b5[9 + 2 * q];
+    out[r1][8 + 2 * q] = c1[2] + s.b5[8 + 2 * q];
+    out[r1][9 + 2 * q] = c1[3] + s.b5[9 + 2 * q];
+  }
+  __syncwarp();
+}
+
+}  // namespace tb

@@ -15,8 +15,11 @@
 // when the state leaves the inclusive bounds.  Unlike the reference, every
 // particle has a cap on step attempts and a non-finite check, so a trapped or
 // broken particle ends with a status instead of looping forever.
+#include <cstring>
+
 #include "tb_common.cuh"
 #include "tb_internal.cuh"
+#include "tb_mlp.cuh"
 #include "../../include/traceon_b200.h"
 
 namespace tb {
@@ -531,9 +534,370 @@ static int launch_bem(const TraceParams& P, cudaStream_t s) {
   return launch_status();
 }
 
+// ============================================================================
+// Surrogate-field tracer.  The field at a point is the axial-series field
+// (radial.c:347-384) of a coefficient table for the actual voltages plus a
+// learned correction: a small MLP predicts, per electrode at 1 V, the
+// difference between the BEM field and the axial series, scaled by
+// rho^p (rho = r / r_max) so that the correction vanishes toward the axis
+// where the series is already exact; the per-electrode outputs are
+// contracted with the electrode voltages (the field is linear in them).
+// Points within `fallback_dist` of an electrode segment, or outside the
+// network's domain, fall back to the exact BEM sum.  One particle per lane;
+// the 32 lanes of a warp evaluate the network together on the tensor cores
+// at every RK stage.
+// ============================================================================
+struct SurrogateParams {
+  const __nv_bfloat16* wb;
+  const float* pf;
+  MlpDomain dom;
+  double z_lo, z_hi;
+  int n_el;
+  double volts[MLP_MAX_ELECTRODES];
+  float scale[MLP_OUT];
+  int env_p;
+  const double* segs;  // (nseg, 4): r0, z0, r1, z1
+  int nseg;
+  double fb_dist2;
+};
+
+constexpr int SG_THREADS = 256;
+constexpr int SG_WARPS = SG_THREADS / 32;
+constexpr int SG_MAX_SEGS = 64;
+
+struct SurrogateSmem {
+  MlpSmem mlp;
+  __nv_bfloat16 feat[SG_WARPS][32][MLP_LD_IN];
+  float out[SG_WARPS][32][MLP_OUT];
+  double segs[SG_MAX_SEGS][4];
+};
+
+__device__ __forceinline__ bool near_segments(const double (*seg)[4], int nseg, double r, double z, double d2) {
+  bool nearby = false;
+  for (int i = 0; i < nseg; i++) {
+    double ar = seg[i][0], az = seg[i][1], br = seg[i][2], bz = seg[i][3];
+    double ur = br - ar, uz = bz - az;
+    double L2 = ur * ur + uz * uz;
+    double tt = L2 > 0 ? ((r - ar) * ur + (z - az) * uz) / L2 : 0.0;
+    tt = fmin(fmax(tt, 0.0), 1.0);
+    double dr = r - (ar + tt * ur), dz = z - (az + tt * uz);
+    nearby = nearby || (dr * dr + dz * dz < d2);
+  }
+  return nearby;
+}
+
+// Exact BEM field of the electrostatic rings at one point, by one lane.
+__device__ void bem_point_field(const TraceParams& P, const double* p, double* E) {
+  double r0 = sqrt(p[0] * p[0] + p[1] * p[1]);
+  double Sr = 0, Sz = 0, dummy = 0;
+  const double* er = P.esrc;
+  for (int64_t j = 0; j < P.ne; j++) ring_field_acc<false>(r0, p[2], er[j], er[P.ne + j], er[2 * P.ne + j], Sr, Sz, dummy);
+  if (r0 >= MIN_AXIS) {
+    double e = Sr / (2 * PI * r0);
+    E[0] = p[0] / r0 * e;
+    E[1] = p[1] / r0 * e;
+  } else {
+    E[0] = E[1] = 0.0;
+  }
+  E[2] = -Sz * INV_PI;
+}
+
+// Field at this lane's point; every lane of the warp must call it.
+__device__ void surrogate_field(const TraceParams& P, const SurrogateParams& S, SurrogateSmem& sm, int warp, int lane,
+                                const double* p, bool live, double* E, bool& used_bem) {
+  const double r2 = p[0] * p[0] + p[1] * p[1], r = sqrt(r2);
+  float f[MLP_IN];
+  mlp_features(r, p[2], S.dom, f);
+#pragma unroll
+  for (int c = 0; c < MLP_IN; c++) sm.feat[warp][lane][c] = __float2bfloat16(f[c]);
+  mlp_warp_forward(sm.mlp, sm.feat[warp], sm.out[warp]);
+  used_bem = false;
+  if (!live) {
+    E[0] = E[1] = E[2] = 0.0;
+    return;
+  }
+  const double* fb = P.fb;
+  if (fb && !(fb[0] < p[0] && p[0] < fb[1] && fb[2] < p[1] && p[1] < fb[3] && fb[4] < p[2] && p[2] < fb[5])) {
+    E[0] = E[1] = E[2] = 0.0;
+    return;
+  }
+  const bool out_of_domain = r > S.dom.r_max || p[2] < S.z_lo || p[2] > S.z_hi;
+  if (out_of_domain || near_segments(sm.segs, S.nseg, r, p[2], S.fb_dist2)) {
+    used_bem = true;
+    bem_point_field(P, p, E);
+    return;
+  }
+  double d[NDERIV];
+  if (axial_eval(p[2], P.az, P.aec, P.anz, d))
+    axial_field(d, p, r2, E);
+  else
+    E[0] = E[1] = E[2] = 0.0;
+  const double rho = r / S.dom.r_max;
+  double env = 1.0;
+  for (int i = 0; i < S.env_p; i++) env *= rho;
+  double fr = 0.0, fz = 0.0;
+  for (int e = 0; e < S.n_el; e++) {
+    fr += S.volts[e] * double(S.scale[3 * e + 1]) * double(sm.out[warp][lane][3 * e + 1]);
+    fz += S.volts[e] * double(S.scale[3 * e + 2]) * double(sm.out[warp][lane][3 * e + 2]);
+  }
+  // E_r correction = fr * rho^(p+1), applied as x * (E_r / r)
+  fr *= env / S.dom.r_max;
+  fz *= env;
+  E[0] += p[0] * fr;
+  E[1] += p[1] * fr;
+  E[2] += fz;
+}
+
+__global__ void __launch_bounds__(SG_THREADS, 1) k_trace_surrogate(TraceParams P, SurrogateParams S) {
+  extern __shared__ __align__(16) unsigned char sg_raw[];
+  SurrogateSmem& sm = *reinterpret_cast<SurrogateSmem*>(sg_raw);
+  mlp_load_smem(sm.mlp, S.wb, S.pf);
+  for (int e = threadIdx.x; e < S.nseg * 4; e += blockDim.x) sm.segs[e / 4][e % 4] = S.segs[e];
+  __syncthreads();
+  const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+
+  double y[6], ks[6][6];
+  double t = 0, h = 0, hmax = 0, qm = 0;
+  int64_t accepted = 0, attempts = 0, fallbacks = 0;
+  int status = TRACE_EXITED;
+  int64_t idx = atomicAdd(P.work, 1);
+  bool active = idx < P.n;
+
+  auto start = [&]() {
+    for (int c = 0; c < 6; c++) y[c] = P.start[idx * 6 + c];
+    qm = P.qm[idx];
+    t = P.t0 ? P.t0[idx] : 0.0;
+    hmax = STEP_MAX / sqrt(y[3] * y[3] + y[4] * y[4] + y[5] * y[5]);
+    h = hmax;
+    accepted = attempts = fallbacks = 0;
+    status = TRACE_EXITED;
+    if (P.plane)
+      for (int c = 0; c < 7; c++) P.plane[idx * 7 + c] = __longlong_as_double(0x7ff8000000000000LL);
+  };
+  auto finish = [&]() {
+    if (P.status) P.status[idx] = status;
+    if (P.nrows) P.nrows[idx] = 1;
+    if (P.final_state) {
+      P.final_state[idx * 7] = t;
+      for (int c = 0; c < 6; c++) P.final_state[idx * 7 + 1 + c] = y[c];
+    }
+    if (P.counters) {
+      P.counters[idx * 3] = accepted;
+      P.counters[idx * 3 + 1] = attempts;
+      P.counters[idx * 3 + 2] = fallbacks;
+    }
+    idx = atomicAdd(P.work, 1);
+    active = idx < P.n;
+  };
+  if (active) start();
+
+  while (__any_sync(0xffffffffu, active)) {
+    bool go = false;
+    if (active) {
+      if (!in_bounds(P.bounds, y)) {
+        finish();
+        if (active) start();
+      } else if (attempts >= P.max_attempts) {
+        status = TRACE_MAX_ATTEMPTS;
+        finish();
+        if (active) start();
+      }
+      go = active && in_bounds(P.bounds, y) && attempts < P.max_attempts;
+    }
+    if (go) attempts++;
+#pragma unroll 1
+    for (int s = 0; s < 6; s++) {
+      double ys[6];
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        double v = y[c];
+        for (int j = 0; j < s; j++) v += RK_B[s][j] * ks[j][c];
+        ys[c] = v;
+      }
+      if (!go) {
+        ys[0] = 0.5 * S.dom.r_max;
+        ys[1] = 0.0;
+        ys[2] = S.dom.z_c;
+      }
+      double E[3];
+      bool used_bem;
+      surrogate_field(P, S, sm, warp, lane, ys, go, E, used_bem);
+      if (go) {
+        fallbacks += used_bem ? 1 : 0;
+        ks[s][0] = h * ys[3];
+        ks[s][1] = h * ys[4];
+        ks[s][2] = h * ys[5];
+        ks[s][3] = h * qm * E[0];
+        ks[s][4] = h * qm * E[1];
+        ks[s][5] = h * qm * E[2];
+      }
+    }
+    if (!go) continue;
+    double ep = 0.0, ev = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double a = 0.0, b = 0.0;
+      for (int j = 0; j < 6; j++) {
+        a += RK_CT[j] * ks[j][c];
+        b += RK_CT[j] * ks[j][c + 3];
+      }
+      ep = fmax(ep, fabs(a));
+      ev = fmax(ev, fabs(b));
+    }
+    double err = ep + h * ev;
+    if (!(err == err)) {
+      status = TRACE_NONFINITE;
+      finish();
+      if (active) start();
+      continue;
+    }
+    if (err <= P.atol) {
+      double yn[6];
+#pragma unroll
+      for (int c = 0; c < 6; c++)
+        yn[c] = y[c] + (RK_CH[0] * ks[0][c] + RK_CH[1] * ks[1][c] + RK_CH[2] * ks[2][c] + RK_CH[3] * ks[3][c] +
+                        RK_CH[4] * ks[4][c] + RK_CH[5] * ks[5][c]);
+      if (P.record_plane && ((y[2] - P.plane_z > 0) != (yn[2] - P.plane_z > 0))) {
+        double cr[7];
+        hermite_crossing(h, y, yn, P.plane_z, t, cr);
+        if (P.plane)
+          for (int c = 0; c < 7; c++) P.plane[idx * 7 + c] = cr[c];
+      }
+      bool finite = true;
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        y[c] = yn[c];
+        finite = finite && isfinite(yn[c]);
+      }
+      t += h;
+      accepted++;
+      if (!finite) {
+        status = TRACE_NONFINITE;
+        finish();
+        if (active) start();
+        continue;
+      }
+    }
+    h = fmin(0.9 * h * pow(P.atol / err, 0.2), hmax);
+  }
+}
+
+// Surrogate field at M points (one point per lane), for tests.
+__global__ void __launch_bounds__(SG_THREADS, 1)
+    k_surrogate_points(TraceParams P, SurrogateParams S, const double* __restrict__ pts, int64_t M,
+                       double* __restrict__ field, int32_t* __restrict__ used_bem) {
+  extern __shared__ __align__(16) unsigned char sg_raw[];
+  SurrogateSmem& sm = *reinterpret_cast<SurrogateSmem*>(sg_raw);
+  mlp_load_smem(sm.mlp, S.wb, S.pf);
+  for (int e = threadIdx.x; e < S.nseg * 4; e += blockDim.x) sm.segs[e / 4][e % 4] = S.segs[e];
+  __syncthreads();
+  const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * SG_THREADS + warp * 32; base < M; base += (int64_t)gridDim.x * SG_THREADS) {
+    int64_t i = base + lane;
+    bool live = i < M;
+    double p[3] = {0.5 * S.dom.r_max, 0.0, S.dom.z_c};
+    if (live)
+      for (int c = 0; c < 3; c++) p[c] = pts[3 * i + c];
+    double E[3];
+    bool ub;
+    surrogate_field(P, S, sm, warp, lane, p, live, E, ub);
+    if (live) {
+      for (int c = 0; c < 3; c++) field[3 * i + c] = E[c];
+      if (used_bem) used_bem[i] = ub ? 1 : 0;
+    }
+  }
+}
+
 }  // namespace tb
 
 using namespace tb;
+
+static int fill_surrogate_params(const tb_field_t* field, const tb_surrogate_t* sur, TraceParams& P,
+                                 SurrogateParams& S) {
+  if (!field->axial_z || field->axial_nz < 2 || !field->axial_elec) return BAD_ARG;
+  if (field->n_elec > 0 && !field->elec_sources) return BAD_ARG;
+  if (!sur->weights_bf16 || !sur->params_f32 || sur->n_electrodes < 1 || sur->n_electrodes > MLP_MAX_ELECTRODES)
+    return BAD_ARG;
+  if (sur->n_segments < 0 || sur->n_segments > SG_MAX_SEGS || (sur->n_segments > 0 && !sur->segments)) return BAD_ARG;
+  if (!(sur->r_max > 0) || !(sur->z_half > 0) || sur->env_power < 0 || sur->env_power > 32) return BAD_ARG;
+  memset(&P, 0, sizeof(P));
+  P.esrc = field->elec_sources;
+  P.ne = field->n_elec;
+  P.fb = field->field_bounds;
+  P.az = field->axial_z;
+  P.aec = field->axial_elec;
+  P.anz = field->axial_nz;
+  memset(&S, 0, sizeof(S));
+  S.wb = static_cast<const __nv_bfloat16*>(sur->weights_bf16);
+  S.pf = sur->params_f32;
+  S.dom = MlpDomain{sur->r_max, sur->z_c, sur->z_half};
+  S.z_lo = sur->z_lo;
+  S.z_hi = sur->z_hi;
+  S.n_el = sur->n_electrodes;
+  for (int e = 0; e < MLP_MAX_ELECTRODES; e++) S.volts[e] = sur->volts[e];
+  for (int c = 0; c < MLP_OUT; c++) S.scale[c] = sur->scale[c];
+  S.env_p = sur->env_power;
+  S.segs = sur->segments;
+  S.nseg = sur->n_segments;
+  S.fb_dist2 = sur->fallback_dist * sur->fallback_dist;
+  return OK;
+}
+
+extern "C" int tb_surrogate_field_points(const double* points, int64_t M, const tb_field_t* field,
+                                         const tb_surrogate_t* sur, double* out, int32_t* used_bem,
+                                         tb_stream_t stream) {
+  if (!field || !sur || M < 0 || (M > 0 && (!points || !out))) return BAD_ARG;
+  if (M == 0) return OK;
+  TraceParams P;
+  SurrogateParams S;
+  int st = fill_surrogate_params(field, sur, P, S);
+  if (st != OK) return st;
+  const int smem = int(sizeof(SurrogateSmem));
+  if (cudaFuncSetAttribute(k_surrogate_points, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    return CUDA_ERR;
+  int64_t blocks = (M + SG_THREADS - 1) / SG_THREADS;
+  if (blocks > 4 * num_sms()) blocks = 4 * num_sms();
+  k_surrogate_points<<<unsigned(blocks), SG_THREADS, smem, (cudaStream_t)stream>>>(P, S, points, M, out, used_bem);
+  return launch_status();
+}
+
+extern "C" int tb_trace_surrogate(const double* start, const double* t0, const double* qm, int64_t n,
+                                  const tb_field_t* field, const tb_surrogate_t* sur, const tb_trace_opts_t* opts,
+                                  int32_t* status, double* final_state, double* plane, int64_t* counters,
+                                  int32_t* work, tb_stream_t stream) {
+  if (!field || !sur || !opts || n < 0 || !work) return BAD_ARG;
+  if (n == 0) return OK;
+  if (n > 0x3fffffff || !start || !qm) return BAD_ARG;
+  if (opts->max_attempts <= 0 || !(opts->atol > 0)) return BAD_ARG;
+  TraceParams P;
+  SurrogateParams S;
+  int st = fill_surrogate_params(field, sur, P, S);
+  if (st != OK) return st;
+  for (int i = 0; i < 6; i++) P.bounds[i] = opts->bounds[i];
+  P.atol = opts->atol;
+  P.plane_z = opts->plane_z;
+  P.record_plane = opts->record_plane;
+  P.max_attempts = opts->max_attempts;
+  P.start = start;
+  P.t0 = t0;
+  P.qm = qm;
+  P.n = n;
+  P.status = status;
+  P.final_state = final_state;
+  P.plane = plane;
+  P.counters = counters;
+  P.work = work;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemsetAsync(work, 0, sizeof(int32_t), s) != cudaSuccess) return CUDA_ERR;
+  const int smem = int(sizeof(SurrogateSmem));
+  if (cudaFuncSetAttribute(k_trace_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    return CUDA_ERR;
+  int64_t blocks = num_sms();
+  int64_t by_work = (n + SG_THREADS - 1) / SG_THREADS;
+  if (blocks > by_work) blocks = by_work;
+  k_trace_surrogate<<<unsigned(blocks), SG_THREADS, smem, s>>>(P, S);
+  return launch_status();
+}
 
 extern "C" int tb_trace_rk45(const double* start, const double* t0, const double* qm, int64_t n,
                              const tb_field_t* field, const tb_trace_opts_t* opts, double* rows, int64_t* nrows,

@@ -71,12 +71,14 @@ def aperture_tube(r_in: float, r_out: float, z0: float, z1: float, n: int) -> np
 
 class LensGeometry:
     """A meshed electrode stack: vertices (N,4,3), per-element electrode index
-    and the electrode names, in the element order used for the BEM matrix."""
+    and the electrode names, in the element order used for the BEM matrix;
+    `segments` (S, 4) lists the straight electrode segments (r0, z0, r1, z1)."""
 
-    def __init__(self, vertices, electrode_index, names):
+    def __init__(self, vertices, electrode_index, names, segments=None):
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float64)
         self.electrode_index = np.asarray(electrode_index, dtype=np.int64)
         self.names = list(names)
+        self.segments = np.zeros((0, 4)) if segments is None else np.asarray(segments, dtype=np.float64)
 
     def __len__(self):
         return len(self.vertices)
@@ -101,13 +103,15 @@ def einzel_lens(n_elements: int = 1000, r_tube: float = 1.0 * MM, r_cap: float =
     split evenly across the electrodes and graded toward the tube edges."""
     k = len(spans)
     per = [n_elements // k + (1 if i < n_elements % k else 0) for i in range(k)]
-    verts, idx = [], []
+    verts, idx, segs = [], [], []
     for e, ((z0, z1), n) in enumerate(zip(spans, per)):
         v = aperture_tube(r_tube, r_cap, z0, z1, n)
         verts.append(v)
         idx.append(np.full(len(v), e))
+        corners = [(r_cap, z0), (r_tube, z0), (r_tube, z1), (r_cap, z1)]
+        segs += [(a[0], a[1], b[0], b[1]) for a, b in zip(corners[:-1], corners[1:])]
     names = ['ground_in', 'lens', 'ground_out'][:k] if k == 3 else [f'electrode{i}' for i in range(k)]
-    return LensGeometry(np.concatenate(verts), np.concatenate(idx), names)
+    return LensGeometry(np.concatenate(verts), np.concatenate(idx), names, segs)
 
 
 def einzel_lens_voltages(seed: int) -> np.ndarray:
@@ -117,19 +121,27 @@ def einzel_lens_voltages(seed: int) -> np.ndarray:
 
 
 def electron_beam(n: int, seed: int, energy_ev: float = 1000.0, z0: float = -9.5 * MM,
-                  r_max: float = 0.2 * MM, angle_max: float = 5e-3):
-    """Start states of the lens workload: electrons at ``energy_ev`` starting at
-    x = r ~ U[0, r_max], y = 0, z = z0, heading +z at an angle ~ U[-a, a] in
-    the xz-plane.  Returns (positions (n,3), velocities (n,3)) in SI units;
-    the speed follows traceon.tracing.velocity_vec (traceon/tracing.py:24-56)."""
+                  r_max: float = 0.2 * MM, angle_max: float = 5e-3, energy_spread: float = 0.0):
+    """Start states of the lens workload: electrons at ``energy_ev`` (times
+    U[1 - spread, 1 + spread]) starting at x = r ~ U[0, r_max], y = 0, z = z0,
+    heading +z at an angle ~ U[-a, a] in the xz-plane.  Returns (positions
+    (n,3), velocities (n,3)) in SI units; the speed follows
+    traceon.tracing.velocity_vec (traceon/tracing.py:24-56)."""
     from scipy.constants import e, m_e
     rng = np.random.default_rng(seed)
     r = rng.uniform(0.0, r_max, n)
     ang = rng.uniform(-angle_max, angle_max, n)
-    speed = np.sqrt(2 * energy_ev * e / m_e)
+    energy = energy_ev * (rng.uniform(1 - energy_spread, 1 + energy_spread, n) if energy_spread else np.ones(n))
+    speed = np.sqrt(2 * energy * e / m_e)[:, None]
     pos = np.stack([r, np.zeros(n), np.full(n, z0)], axis=1)
     vel = speed * np.stack([np.sin(ang), np.zeros(n), np.cos(ang)], axis=1)
     return pos, vel
+
+
+def surrogate_beam(n: int, seed: int):
+    """The learned-surrogate workload's beam: 1 keV +-5 % (uniform), angles
+    +-20 mrad, start radius up to 0.2 mm at z = -9.5 mm."""
+    return electron_beam(n, seed, r_max=0.2 * MM, angle_max=20e-3, energy_spread=0.05)
 
 
 LENS_BOUNDS = np.array([[-2 * MM, 2 * MM], [-2 * MM, 2 * MM], [-10 * MM, 10 * MM]])
