@@ -110,10 +110,12 @@ def test_network_gain_on_field(cuda, trained):
     err_sur = np.abs(E_sur - E_bem)[ok].max()
     err_ax = np.abs(E_ax - E_bem)[ok].max()
     assert err_sur < err_ax / 20
-    # the kernel's field matches the batched host evaluation of the same model
-    # (the two differ only in the FP32 accumulation order of the network)
+    # The kernel's field matches the batched host evaluation of the same model.
+    # They differ in the FP32 accumulation order inside the network, which can
+    # flip BF16 roundings of hidden activations: compare against the size of
+    # the learned correction itself.
     E_host = fs.field_at_points(pts)
-    assert np.abs(E_host - E_sur)[ok].max() < 1e-8 * np.abs(E_bem).max()
+    assert np.abs(E_host - E_sur)[ok].max() < 0.05 * np.abs(E_sur - E_ax)[ok].max()
 
 
 def _endpoint_errors(port, field, p0, v0):

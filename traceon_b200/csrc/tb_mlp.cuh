@@ -115,7 +115,10 @@ __device__ __forceinline__ void mlp_hidden_layer(const __nv_bfloat16 (*W)[MLP_LD
                                                  const uint32_t (&a)[8][4], uint32_t (&out)[8][4], int g, int q) {
 #pragma unroll
   for (int kb = 0; kb < 8; kb++) {  // output columns 16 kb .. 16 kb + 15
+    // two partial sums per n8 tile (even / odd k-blocks): four independent
+    // accumulation chains instead of two
     float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+    float d0[4] = {0.f, 0.f, 0.f, 0.f}, d1[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int ki = 0; ki < 8; ki++) {
       uint32_t b0[2], b1[2];
@@ -124,8 +127,18 @@ __device__ __forceinline__ void mlp_hidden_layer(const __nv_bfloat16 (*W)[MLP_LD
       b0[1] = *reinterpret_cast<const uint32_t*>(&W[n0][16 * ki + 8 + 2 * q]);
       b1[0] = *reinterpret_cast<const uint32_t*>(&W[n1][16 * ki + 2 * q]);
       b1[1] = *reinterpret_cast<const uint32_t*>(&W[n1][16 * ki + 8 + 2 * q]);
-      mma_bf16_16816(c0, a[ki], b0);
-      mma_bf16_16816(c1, a[ki], b1);
+      if (ki & 1) {
+        mma_bf16_16816(d0, a[ki], b0);
+        mma_bf16_16816(d1, a[ki], b1);
+      } else {
+        mma_bf16_16816(c0, a[ki], b0);
+        mma_bf16_16816(c1, a[ki], b1);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      c0[c] += d0[c];
+      c1[c] += d1[c];
     }
     int col0 = 16 * kb + 2 * q, col1 = 16 * kb + 8 + 2 * q;
     out[kb][0] = pack_bf16(silu(c0[0] + bias[col0]), silu(c0[1] + bias[col0 + 1]));

@@ -561,7 +561,7 @@ struct SurrogateParams {
   double fb_dist2;
 };
 
-constexpr int SG_THREADS = 256;
+constexpr int SG_THREADS = 512;
 constexpr int SG_WARPS = SG_THREADS / 32;
 constexpr int SG_MAX_SEGS = 64;
 
@@ -892,8 +892,9 @@ extern "C" int tb_trace_surrogate(const double* start, const double* t0, const d
   const int smem = int(sizeof(SurrogateSmem));
   if (cudaFuncSetAttribute(k_trace_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
     return CUDA_ERR;
+  // one block per SM; fewer only when there is not a warp of particles per SM
   int64_t blocks = num_sms();
-  int64_t by_work = (n + SG_THREADS - 1) / SG_THREADS;
+  int64_t by_work = (n + 31) / 32;
   if (blocks > by_work) blocks = by_work;
   k_trace_surrogate<<<unsigned(blocks), SG_THREADS, smem, s>>>(P, S);
   return launch_status();
