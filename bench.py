@@ -329,10 +329,8 @@ def run_gpu(args):
         ms_list, results = time_steps(step, args.steps, flush)
     total_ms = float(np.sum(ms_list))
     if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([total_ms], device='cuda', dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        from traceon_b200.parallel import max_over_ranks
+        total_ms = max_over_ranks(total_ms, device='cuda')
     res = results[-1]
     attempts = [int(r.counters[:, 1].sum().item()) for r in results]
     status = res.status.cpu().numpy()

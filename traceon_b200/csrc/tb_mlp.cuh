@@ -34,9 +34,13 @@ struct MlpDomain {
   double r_max, z_c, z_half;
 };
 
-__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+// SiLU with the fast approximate division (a few ulp in FP32, far below the
+// BF16 rounding that follows); the same function serves training and the
+// tracer.  For z < -87, 1 + exp(-z) overflows and the quotient is 0, the
+// limit of silu.
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
-  float s = 1.f / (1.f + __expf(-z));
+  float s = __fdividef(1.f, 1.f + __expf(-z));
   return s * (1.f + z * (1.f - s));
 }
 
