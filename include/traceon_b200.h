@@ -238,6 +238,27 @@ int tb_lu_solve_perm(const double *LU, int64_t lda, const int32_t *perm, int64_t
 int tb_pack_sources(const double *charges, const double *jac, const double *pos, double *sources, int64_t N,
                     tb_stream_t stream);
 
+/* Blocked LU without pivoting, in place (A = L U, L unit lower), FP64 or
+ * FP32.  The radial BEM matrices need no pivoting (growth factor < 1 on the
+ * lens meshes); no reference counterpart beyond the factorisation inside
+ * numpy.linalg.solve (solver.py:173). */
+int tb_lu_nopiv_f64(double *A, int64_t lda, int64_t N, tb_stream_t stream);
+int tb_lu_nopiv_f32(float *A, int64_t lda, int64_t N, tb_stream_t stream);
+
+/* Mixed-precision solve of A x = f for the nrhs (<= 16) rows of F (nrhs, N)
+ * into X (nrhs, N): FP32 LU without pivoting of A diag(c), c_j = 1 / max_i
+ * |A_ij|, then FP64 iterative refinement with the FP64 matrix until, for
+ * every right-hand side, max |correction| / max |x| <= tol (at most max_iter
+ * rounds; corrections that stall within 100 tol count as converged).  `work`
+ * is device scratch of tb_solve_mixed_workspace(N, nrhs) bytes.  Returns
+ * TB_SINGULAR when refinement does not converge (the caller then solves with
+ * tb_lu_factor_perm / tb_lu_solve_perm).  Replaces numpy.linalg.solve
+ * (solver.py:173) with the same FP64 answer. */
+int64_t tb_solve_mixed_workspace(int64_t N, int64_t nrhs);
+int tb_solve_mixed(const double *A, int64_t lda, int64_t N, const double *F, double *X, int64_t nrhs, void *work,
+                   int64_t work_bytes, int max_iter, double tol, int *iters_out, double *last_rel_out,
+                   tb_stream_t stream);
+
 /* Dense solve that allocates nothing: LU-factorises A in place (as
  * tb_lu_factor_perm) and solves for the nrhs rows of F into the rows of X (as
  * tb_lu_solve_perm), keeping the pivots and permutation in a static device

@@ -212,6 +212,9 @@ _DEV = {
     'tb_num_sms': (),
     'tb_probe_fp64_fma': (C.c_int, i64, vp, vp),
     'tb_probe_math': (vp, i64, C.c_int, vp, vp),
+    'tb_lu_nopiv_f64': (vp, i64, i64, vp),
+    'tb_lu_nopiv_f32': (vp, i64, i64, vp),
+    'tb_solve_mixed': (vp, i64, i64, vp, vp, i64, vp, i64, C.c_int, dbl, C.POINTER(C.c_int), C.POINTER(dbl), vp),
 }
 for _name, _args in _DEV.items():
     _f = getattr(backend_lib, _name)
@@ -596,6 +599,39 @@ def dev_lu_solve(LU, perm, F):
     # a (1, N) tensor may report stride 0 for its size-1 dimension
     _call('tb_lu_solve_perm', _ptr(LU), LU.stride(0), _ptr(perm), N, _ptr(F), N, _ptr(X), N, F.shape[0], _stream())
     return X
+
+
+backend_lib.tb_solve_mixed_workspace.restype = i64
+backend_lib.tb_solve_mixed_workspace.argtypes = [i64, i64]
+
+
+def dev_lu_nopiv(A):
+    """In-place LU without pivoting of a square FP64 or FP32 device matrix."""
+    torch = _torch()
+    name = 'tb_lu_nopiv_f64' if A.dtype == torch.float64 else 'tb_lu_nopiv_f32'
+    _call(name, _ptr(A), A.stride(0), A.shape[0], _stream())
+
+
+def dev_solve_mixed(A, F, max_iter=12, tol=1e-12):
+    """Mixed-precision solve (FP32 factors, FP64 refinement) of A x = f for
+    each row f of F (nrhs <= 16).  Returns (X, iterations, last relative
+    correction); raises BackendError(status) when refinement fails."""
+    torch = _torch()
+    N = A.shape[0]
+    F = F.reshape(-1, N).contiguous()
+    nrhs = F.shape[0]
+    X = torch.empty((nrhs, N), dtype=torch.float64, device=A.device)
+    nbytes = backend_lib.tb_solve_mixed_workspace(N, nrhs)
+    work = torch.empty(nbytes, dtype=torch.uint8, device=A.device)
+    it = C.c_int(0)
+    rel = dbl(0.0)
+    r = backend_lib.tb_solve_mixed(_ptr(A), A.stride(0), N, _ptr(F), _ptr(X), nrhs, _ptr(work), nbytes, max_iter, tol,
+                                   C.byref(it), C.byref(rel), _stream())
+    if r != TB_OK:
+        err = BackendError(f'tb_solve_mixed failed with status {r}')
+        err.status = r
+        raise err
+    return X, it.value, rel.value
 
 
 def dev_pack_sources(charges_t, jac_t, pos_t):

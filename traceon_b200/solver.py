@@ -111,25 +111,39 @@ class SolverRadial:
         assert np.all(np.isfinite(A)), "Matrix contains non-finite values."
         return A
 
-    def solve_charges_device(self, F):
-        """Charges (nrhs, N) device tensor for right-hand sides F (nrhs, N)."""
+    def solve_charges_device(self, F, method='mixed'):
+        """Charges (nrhs, N) device tensor for right-hand sides F (nrhs, N).
+
+        method 'mixed': FP32 factors of the equilibrated matrix refined in
+        FP64 against the FP64 matrix (tb_solve_mixed); falls back to 'lu' if
+        refinement does not converge.  method 'lu': FP64 LU with partial
+        pivoting, the factorisation of numpy.linalg.solve (solver.py:173)."""
         torch = B._torch()
         A = self.get_matrix_device()
         if not bool(torch.isfinite(A).all()):
             raise ValueError('Matrix contains non-finite values.')
-        ipiv, perm = B.dev_lu_factor(A)
         Ft = B.to_dev(np.atleast_2d(F), torch.float64)
+        self.solve_info = {'method': method}
+        if method == 'mixed' and Ft.shape[0] <= 16:
+            try:
+                X, iters, rel = B.dev_solve_mixed(A, Ft)
+                self.solve_info.update(iterations=iters, last_correction=rel)
+                return X
+            except B.BackendError as e:
+                self.solve_info.update(fallback=f'mixed refinement failed (status {getattr(e, "status", "?")})')
+        ipiv, perm = B.dev_lu_factor(A)
         X = B.dev_lu_solve(A, perm, Ft)
+        self.solve_info['method'] = 'lu'
         return X
 
-    def solve_matrix(self, right_hand_side=None):
+    def solve_matrix(self, right_hand_side=None, method='mixed'):
         """traceon/solver.py:160-180"""
         F = np.array([self.get_right_hand_side()]) if right_hand_side is None else np.atleast_2d(right_hand_side)
         N = self.get_number_of_matrix_elements()
         if N == 0:
             return [self.charges_to_field(EffectivePointCharges.empty_2d()) for _ in range(len(F))]
         assert all(f.shape == (N,) for f in F)
-        charges = self.solve_charges_device(F).cpu().numpy()
+        charges = self.solve_charges_device(F, method).cpu().numpy()
         assert np.all(np.isfinite(charges)) and charges.shape == F.shape, 'non-finite charges (singular matrix?)'
         jac, pos = self.jacobians_and_positions()
         return [self.charges_to_field(EffectivePointCharges(c, jac, pos)) for c in charges]
