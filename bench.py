@@ -255,6 +255,7 @@ def time_steps(fn, steps, flush):
     """CUDA-event time of `steps` calls of fn (L2 flushed before each)."""
     import torch
     ms, results = [], []
+    torch.cuda.nvtx.range_push('timed_steps')  # lets a profiler select the timed launches
     for _ in range(steps):
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -264,6 +265,7 @@ def time_steps(fn, steps, flush):
         torch.cuda.synchronize()
         ms.append(e0.elapsed_time(e1))
         results.append(r)
+    torch.cuda.nvtx.range_pop()
     return ms, results
 
 
@@ -304,7 +306,7 @@ def run_gpu(args):
         setup['surrogate_train_s'] = time.perf_counter() - t0
         setup['surrogate_holdout_mse'] = info['holdout_mse']
         setup['surrogate_train'] = f'{args.train_samples} BEM samples, {args.train_steps} Adam steps of 8192'
-        sur = FieldSurrogate(model, trainer.fields, trainer.z, trainer.tabs, volts, geo.segments)
+        sur = FieldSurrogate(model, trainer.fields, trainer.z, trainer.tabs, volts, geo.segments, engine=args.engine)
 
     start = torch.as_tensor(np.concatenate([p0, v0], 1), device='cuda', dtype=torch.float64).contiguous()
     qm = torch.full((E,), -qe / m_e, device='cuda', dtype=torch.float64)
@@ -455,6 +457,8 @@ def main():
     ap.add_argument('--train-samples', type=int, default=1 << 22)
     ap.add_argument('--train-steps', type=int, default=40000)
     ap.add_argument('--team-warps', type=int, default=0)
+    ap.add_argument('--engine', default='warp', choices=['tc', 'warp'],
+                    help='surrogate network engine: tcgen05 (tc) or warp-level mma.sync (warp)')
     ap.add_argument('--check', type=int, default=16, help='electrons checked against the CPU oracle')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
     ap.add_argument('--ref-seconds', type=float, default=20.0)

@@ -55,6 +55,7 @@ typedef struct CUstream_st *tb_stream_t;
 #define TB_TRACE_MAX_ATTEMPTS 1
 #define TB_TRACE_ROWS_FULL 2
 #define TB_TRACE_NONFINITE 3
+#define TB_TRACE_ENGINE_TIMEOUT 4  /* tensor-core engine: bounded MMA wait ran out */
 
 /* ======================================================================
  * 1. Reference-compatible entry points (host pointers)
@@ -401,6 +402,8 @@ typedef struct {
   const double *segments;       /* (n_segments, 4) electrode segments r0, z0, r1, z1 (device) */
   int n_segments;               /* <= 64 */
   double fallback_dist;         /* exact BEM within this distance of a segment */
+  int engine;                   /* network engine: 0 = tcgen05 (groups of 128 particles, accumulators in
+                                   tensor memory), 1 = warp-level mma.sync (32 particles per warp) */
 } tb_surrogate_t;
 
 /* RKF45 tracing (tracing.c:60-123 step control) through the surrogate field:

@@ -82,10 +82,10 @@ def trained():
     return geo, tr, model, info
 
 
-def _fields(trained, volts):
+def _fields(trained, volts, engine='warp'):
     from traceon_b200.surrogate import FieldSurrogate, SurrogateModel
     geo, tr, model, info = trained
-    fs = FieldSurrogate(model, tr.fields, tr.z, tr.tabs, volts, geo.segments)
+    fs = FieldSurrogate(model, tr.fields, tr.z, tr.tabs, volts, geo.segments, engine=engine)
     axial_only = FieldSurrogate(model, tr.fields, tr.z, tr.tabs, volts, geo.segments)
     axial_only.model = SurrogateModel(model.n_el, model.r_max, model.z_lo, model.z_hi, model.scale * 0,
                                       model.env_power, params=model.mlp.p.cpu().numpy())
@@ -165,3 +165,51 @@ def test_surrogate_fallback_near_electrodes(cuda, trained):
     _, E_bem = B.dev_field_points(B.to_dev(pts, torch.float64), fs.sources)
     E_bem = E_bem.cpu().numpy()
     assert np.all(np.linalg.norm(E - E_bem, axis=1) < 1e-12 * np.linalg.norm(E_bem, axis=1))
+
+
+def test_tc_engine_matches_warp_engine(cuda, trained):
+    """The tcgen05 engine (128-particle groups, accumulators in tensor
+    memory) evaluates the same network as the warp-level mma.sync engine:
+    the same fallback decisions, and fields that differ only by FP32
+    accumulation order (which can flip BF16 roundings of hidden activations),
+    far below the learned correction itself.  1,000 points: not a multiple of
+    the 128-row tile."""
+    volts = np.array([0.0, 1500.0, 0.0])
+    fs_w, axial_only = _fields(trained, volts, 'warp')
+    fs_t, _ = _fields(trained, volts, 'tc')
+    rng = np.random.default_rng(5)
+    n = 1000
+    pts = np.stack([rng.uniform(0.0, 0.9e-3, n), rng.uniform(-0.1e-3, 0.1e-3, n), rng.uniform(-9.5e-3, 9.5e-3, n)], 1)
+    pts[:10, 0] = 0.985e-3  # near the tube wall: exact BEM fallback
+    E_w, used_w = fs_w.kernel_field_at_points(pts)
+    E_t, used_t = fs_t.kernel_field_at_points(pts)
+    E_ax, _ = axial_only.kernel_field_at_points(pts)
+    assert (used_t >= 0).all()  # no engine timeout
+    assert (used_t == used_w).all() and used_t[:10].all()
+    ok = used_w == 0
+    corr = np.abs(E_w - E_ax)[ok].max()
+    assert corr > 0
+    assert np.abs(E_t - E_w)[ok].max() < 0.02 * corr
+    assert np.array_equal(E_t[~ok], E_w[~ok])
+
+
+def test_tc_engine_traces_vs_bem_oracle(cuda, port, trained):
+    """Tracing through the tcgen05 engine: 300 electrons (2 full groups and a
+    partial one), all exit, sampled endpoints within 1 nm of the exact FP64
+    BEM trace of the oracle and within 0.1 nm of the warp engine's."""
+    import torch
+    from traceon_b200 import geometry as G
+    from oracle.oracle import EM
+    volts = np.array([0.0, 1500.0, 0.0])
+    fs_t, _ = _fields(trained, volts, 'tc')
+    fs_w, _ = _fields(trained, volts, 'warp')
+    p0, v0 = G.surrogate_beam(300, 23)
+    start = torch.as_tensor(np.concatenate([p0, v0], 1), device='cuda')
+    qm = torch.full((300,), EM, device='cuda', dtype=torch.float64)
+    r_t = fs_t.trace_device(start, qm, G.LENS_BOUNDS, 1e-10, plane_z=G.LENS_EXIT_Z)
+    r_w = fs_w.trace_device(start, qm, G.LENS_BOUNDS, 1e-10, plane_z=G.LENS_EXIT_Z)
+    assert (r_t.status.cpu().numpy() == 0).all()
+    d = np.abs(r_t.plane.cpu().numpy()[:, 1:3] - r_w.plane.cpu().numpy()[:, 1:3]).max()
+    assert d < 1e-10
+    err, _ = _endpoint_errors(port, fs_t, p0[:12], v0[:12])
+    assert err.max() < 1e-9

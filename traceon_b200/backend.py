@@ -47,7 +47,7 @@ NU_MAX = C.c_int.in_dll(backend_lib, 'NU_MAX_SYM').value
 M_MAX = C.c_int.in_dll(backend_lib, 'M_MAX_SYM').value
 
 TB_OK, TB_BAD_ARG, TB_CUDA_ERR, TB_NONFINITE, TB_UNSUPPORTED, TB_SINGULAR = range(6)
-TRACE_EXITED, TRACE_MAX_ATTEMPTS, TRACE_ROWS_FULL, TRACE_NONFINITE = range(4)
+TRACE_EXITED, TRACE_MAX_ATTEMPTS, TRACE_ROWS_FULL, TRACE_NONFINITE, TRACE_ENGINE_TIMEOUT = range(5)
 
 dbl = C.c_double
 dbl_p = C.POINTER(dbl)

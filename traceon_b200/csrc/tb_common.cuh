@@ -369,6 +369,7 @@ enum TraceStatus : int {
   TRACE_MAX_ATTEMPTS = 1,  // step-attempt cap reached
   TRACE_ROWS_FULL = 2,     // trajectory buffer full; resume from the last row
   TRACE_NONFINITE = 3,     // state became non-finite
+  TRACE_ENGINE_TIMEOUT = 4,  // the tensor-core engine's bounded MMA wait ran out; particle abandoned
 };
 
 }  // namespace tb

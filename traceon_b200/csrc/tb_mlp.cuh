@@ -34,19 +34,29 @@ struct MlpDomain {
   double r_max, z_c, z_half;
 };
 
-// SiLU with the fast approximate division (a few ulp in FP32, far below the
-// BF16 rounding that follows); the same function serves training and the
-// tracer.  For z < -87, 1 + exp(-z) overflows and the quotient is 0, the
-// limit of silu.
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.f + __expf(-z)); }
+// SiLU through a single hardware tanh: silu(z) = z sigmoid(z) = h + h tanh(h)
+// with h = z / 2.  tanh.approx.f32 (one MUFU operation instead of the exp and
+// reciprocal of z / (1 + exp(-z))) has a maximum relative error of about
+// 2^-11, below the BF16 rounding of the activations that follows; training
+// and the tracer use the same function.
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float silu(float z) {
+  const float h = 0.5f * z;
+  return fmaf(h, tanh_fast(h), h);
+}
 __device__ __forceinline__ float silu_grad(float z) {
-  float s = __fdividef(1.f, 1.f + __expf(-z));
-  return s * (1.f + z * (1.f - s));
+  const float s = fmaf(0.5f, tanh_fast(0.5f * z), 0.5f);  // sigmoid(z)
+  return s * fmaf(z, 1.f - s, 1.f);
 }
 
 // Input features of a point (r, z): polynomial terms in rho^2 and zeta (the
-// field is even in r) and five Fourier pairs in zeta.
-__host__ __device__ __forceinline__ void mlp_features(double r, double z, const MlpDomain& d, float* f) {
+// field is even in r) and five Fourier pairs in zeta, sin/cos(k pi zeta) for
+// k = 1..5, the higher harmonics by the angle-addition recurrence.
+__device__ __forceinline__ void mlp_features(double r, double z, const MlpDomain& d, float* f) {
   float rho = float(r / d.r_max), zeta = float((z - d.z_c) / d.z_half);
   float p = rho * rho;
   f[0] = p;
@@ -55,13 +65,16 @@ __host__ __device__ __forceinline__ void mlp_features(double r, double z, const 
   f[3] = zeta * zeta;
   f[4] = p * p;
   f[5] = p * zeta * zeta;
-  const float PI_F = 3.14159265358979f;
+  float s1, c1;
+  sincospif(zeta, &s1, &c1);
+  float s = s1, c = c1;
 #pragma unroll
   for (int k = 1; k <= 5; k++) {
-    float s, c;
-    sincosf(PI_F * float(k) * zeta, &s, &c);
     f[4 + 2 * k] = s;
     f[5 + 2 * k] = c;
+    const float sn = fmaf(s, c1, c * s1);
+    c = fmaf(c, c1, -s * s1);
+    s = sn;
   }
 }
 
@@ -84,11 +97,9 @@ constexpr int MLP_LD_IN = MLP_IN + 8;  // padded row strides (bf16 elements)
 constexpr int MLP_LD_H = MLP_H + 8;
 struct MlpSmem {
   __nv_bfloat16 w1[MLP_H][MLP_LD_IN];
-  __nv_bfloat16 w2[MLP_H][MLP_LD_H];
-  __nv_bfloat16 w3[MLP_H][MLP_LD_H];
-  __nv_bfloat16 w4[MLP_H][MLP_LD_H];
+  __nv_bfloat16 wh[3][MLP_H][MLP_LD_H];  // W2, W3, W4
   __nv_bfloat16 w5[MLP_OUT][MLP_LD_H];
-  float b1[MLP_H], b2[MLP_H], b3[MLP_H], b4[MLP_H], b5[MLP_OUT];
+  float b1[MLP_H], bh[3][MLP_H], b5[MLP_OUT];
 };
 
 // Copies the BF16 weights and FP32 biases (flat layout above) into shared
@@ -97,16 +108,16 @@ __device__ inline void mlp_load_smem(MlpSmem& s, const __nv_bfloat16* __restrict
                                      const float* __restrict__ pf) {
   for (int e = threadIdx.x; e < MLP_H * MLP_IN; e += blockDim.x) s.w1[e / MLP_IN][e % MLP_IN] = wb[MLP_OFF_W1 + e];
   for (int e = threadIdx.x; e < MLP_H * MLP_H; e += blockDim.x) {
-    s.w2[e / MLP_H][e % MLP_H] = wb[MLP_OFF_W2 + e];
-    s.w3[e / MLP_H][e % MLP_H] = wb[MLP_OFF_W3 + e];
-    s.w4[e / MLP_H][e % MLP_H] = wb[MLP_OFF_W4 + e];
+    s.wh[0][e / MLP_H][e % MLP_H] = wb[MLP_OFF_W2 + e];
+    s.wh[1][e / MLP_H][e % MLP_H] = wb[MLP_OFF_W3 + e];
+    s.wh[2][e / MLP_H][e % MLP_H] = wb[MLP_OFF_W4 + e];
   }
   for (int e = threadIdx.x; e < MLP_OUT * MLP_H; e += blockDim.x) s.w5[e / MLP_H][e % MLP_H] = wb[MLP_OFF_W5 + e];
   for (int e = threadIdx.x; e < MLP_H; e += blockDim.x) {
     s.b1[e] = pf[MLP_OFF_B1 + e];
-    s.b2[e] = pf[MLP_OFF_B2 + e];
-    s.b3[e] = pf[MLP_OFF_B3 + e];
-    s.b4[e] = pf[MLP_OFF_B4 + e];
+    s.bh[0][e] = pf[MLP_OFF_B2 + e];
+    s.bh[1][e] = pf[MLP_OFF_B3 + e];
+    s.bh[2][e] = pf[MLP_OFF_B4 + e];
   }
   for (int e = threadIdx.x; e < MLP_OUT; e += blockDim.x) s.b5[e] = pf[MLP_OFF_B5 + e];
 }
@@ -187,9 +198,16 @@ __device__ inline void mlp_warp_forward(const MlpSmem& s, const __nv_bfloat16 (*
       h[kb][2] = pack_bf16(silu(c1[0] + s.b1[col1]), silu(c1[1] + s.b1[col1 + 1]));
       h[kb][3] = pack_bf16(silu(c1[2] + s.b1[col1]), silu(c1[3] + s.b1[col1 + 1]));
     }
-    mlp_hidden_layer(s.w2, s.b2, h, h2, g, q);
-    mlp_hidden_layer(s.w3, s.b3, h2, h, g, q);
-    mlp_hidden_layer(s.w4, s.b4, h, h2, g, q);
+    // the three hidden layers share one copy of the code (smaller kernel:
+    // fewer instruction-fetch stalls)
+#pragma unroll 1
+    for (int l = 0; l < 3; l++) {
+      mlp_hidden_layer(s.wh[l], s.bh[l], h, h2, g, q);
+#pragma unroll
+      for (int kb = 0; kb < 8; kb++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) h[kb][c] = h2[kb][c];
+    }
     // output layer: N = 16 (two n8 tiles), FP32 results
     float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll

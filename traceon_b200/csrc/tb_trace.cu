@@ -15,11 +15,13 @@
 // when the state leaves the inclusive bounds.  Unlike the reference, every
 // particle has a cap on step attempts and a non-finite check, so a trapped or
 // broken particle ends with a status instead of looping forever.
+#include <cstddef>
 #include <cstring>
 
 #include "tb_common.cuh"
 #include "tb_internal.cuh"
 #include "tb_mlp.cuh"
+#include "tb_tc.cuh"
 #include "../../include/traceon_b200.h"
 
 namespace tb {
@@ -569,18 +571,31 @@ struct SurrogateSmem {
   MlpSmem mlp;
   __nv_bfloat16 feat[SG_WARPS][32][MLP_LD_IN];
   float out[SG_WARPS][32][MLP_OUT];
-  double segs[SG_MAX_SEGS][4];
+  double segs[SG_MAX_SEGS][5];
 };
 
-__device__ __forceinline__ bool near_segments(const double (*seg)[4], int nseg, double r, double z, double d2) {
+// Electrode segments staged in shared memory as (r0, z0, dr, dz, 1 / |d|^2),
+// so the distance test takes no division.
+__device__ inline void load_segments(double (*seg)[5], const double* __restrict__ segs, int nseg) {
+  for (int i = threadIdx.x; i < nseg; i += blockDim.x) {
+    const double ar = segs[4 * i], az = segs[4 * i + 1];
+    const double ur = segs[4 * i + 2] - ar, uz = segs[4 * i + 3] - az;
+    const double L2 = ur * ur + uz * uz;
+    seg[i][0] = ar;
+    seg[i][1] = az;
+    seg[i][2] = ur;
+    seg[i][3] = uz;
+    seg[i][4] = L2 > 0 ? 1.0 / L2 : 0.0;
+  }
+}
+
+__device__ __forceinline__ bool near_segments(const double (*seg)[5], int nseg, double r, double z, double d2) {
   bool nearby = false;
   for (int i = 0; i < nseg; i++) {
-    double ar = seg[i][0], az = seg[i][1], br = seg[i][2], bz = seg[i][3];
-    double ur = br - ar, uz = bz - az;
-    double L2 = ur * ur + uz * uz;
-    double tt = L2 > 0 ? ((r - ar) * ur + (z - az) * uz) / L2 : 0.0;
+    const double ar = seg[i][0], az = seg[i][1], ur = seg[i][2], uz = seg[i][3];
+    double tt = ((r - ar) * ur + (z - az) * uz) * seg[i][4];
     tt = fmin(fmax(tt, 0.0), 1.0);
-    double dr = r - (ar + tt * ur), dz = z - (az + tt * uz);
+    const double dr = r - (ar + tt * ur), dz = z - (az + tt * uz);
     nearby = nearby || (dr * dr + dz * dz < d2);
   }
   return nearby;
@@ -602,15 +617,12 @@ __device__ void bem_point_field(const TraceParams& P, const double* p, double* E
   E[2] = -Sz * INV_PI;
 }
 
-// Field at this lane's point; every lane of the warp must call it.
-__device__ void surrogate_field(const TraceParams& P, const SurrogateParams& S, SurrogateSmem& sm, int warp, int lane,
-                                const double* p, bool live, double* E, bool& used_bem) {
-  const double r2 = p[0] * p[0] + p[1] * p[1], r = sqrt(r2);
-  float f[MLP_IN];
-  mlp_features(r, p[2], S.dom, f);
-#pragma unroll
-  for (int c = 0; c < MLP_IN; c++) sm.feat[warp][lane][c] = __float2bfloat16(f[c]);
-  mlp_warp_forward(sm.mlp, sm.feat[warp], sm.out[warp]);
+// The field at point p from the network's outputs `y` (16 FP32 values of
+// this point): zero outside the field bounds, exact BEM near electrodes and
+// outside the network's domain, else axial series + learned correction.
+__device__ void surrogate_combine(const TraceParams& P, const SurrogateParams& S, const double (*segs)[5],
+                                  const double* p, double r2, double r, bool live, const float* y, double* E,
+                                  bool& used_bem) {
   used_bem = false;
   if (!live) {
     E[0] = E[1] = E[2] = 0.0;
@@ -622,7 +634,7 @@ __device__ void surrogate_field(const TraceParams& P, const SurrogateParams& S, 
     return;
   }
   const bool out_of_domain = r > S.dom.r_max || p[2] < S.z_lo || p[2] > S.z_hi;
-  if (out_of_domain || near_segments(sm.segs, S.nseg, r, p[2], S.fb_dist2)) {
+  if (out_of_domain || near_segments(segs, S.nseg, r, p[2], S.fb_dist2)) {
     used_bem = true;
     bem_point_field(P, p, E);
     return;
@@ -637,8 +649,8 @@ __device__ void surrogate_field(const TraceParams& P, const SurrogateParams& S, 
   for (int i = 0; i < S.env_p; i++) env *= rho;
   double fr = 0.0, fz = 0.0;
   for (int e = 0; e < S.n_el; e++) {
-    fr += S.volts[e] * double(S.scale[3 * e + 1]) * double(sm.out[warp][lane][3 * e + 1]);
-    fz += S.volts[e] * double(S.scale[3 * e + 2]) * double(sm.out[warp][lane][3 * e + 2]);
+    fr += S.volts[e] * double(S.scale[3 * e + 1]) * double(y[3 * e + 1]);
+    fz += S.volts[e] * double(S.scale[3 * e + 2]) * double(y[3 * e + 2]);
   }
   // E_r correction = fr * rho^(p+1), applied as x * (E_r / r)
   fr *= env / S.dom.r_max;
@@ -648,14 +660,26 @@ __device__ void surrogate_field(const TraceParams& P, const SurrogateParams& S, 
   E[2] += fz;
 }
 
-__global__ void __launch_bounds__(SG_THREADS, 1) k_trace_surrogate(TraceParams P, SurrogateParams S) {
-  extern __shared__ __align__(16) unsigned char sg_raw[];
-  SurrogateSmem& sm = *reinterpret_cast<SurrogateSmem*>(sg_raw);
-  mlp_load_smem(sm.mlp, S.wb, S.pf);
-  for (int e = threadIdx.x; e < S.nseg * 4; e += blockDim.x) sm.segs[e / 4][e % 4] = S.segs[e];
-  __syncthreads();
-  const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+// Field at this lane's point; every lane of the warp must call it.
+__device__ void surrogate_field(const TraceParams& P, const SurrogateParams& S, SurrogateSmem& sm, int warp, int lane,
+                                const double* p, bool live, double* E, bool& used_bem) {
+  const double r2 = p[0] * p[0] + p[1] * p[1], r = sqrt(r2);
+  float f[MLP_IN];
+  mlp_features(r, p[2], S.dom, f);
+#pragma unroll
+  for (int c = 0; c < MLP_IN; c++) sm.feat[warp][lane][c] = __float2bfloat16(f[c]);
+  mlp_warp_forward(sm.mlp, sm.feat[warp], sm.out[warp]);
+  surrogate_combine(P, S, sm.segs, p, r2, r, live, sm.out[warp][lane], E, used_bem);
+}
 
+// The RKF45 particle loop of the surrogate tracer, shared by both network
+// engines.  `eng.any(b)` is true if b holds on any thread that evaluates the
+// network together with this one; `eng.field(p, live, E, used_bem)` is the
+// field at p (all those threads call it together) and returns false if the
+// engine failed (uniformly across them).
+template <class Engine>
+__device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams& S, Engine& eng) {
+  bool engine_failed = false;
   double y[6], ks[6][6];
   double t = 0, h = 0, hmax = 0, qm = 0;
   int64_t accepted = 0, attempts = 0, fallbacks = 0;
@@ -691,7 +715,7 @@ __global__ void __launch_bounds__(SG_THREADS, 1) k_trace_surrogate(TraceParams P
   };
   if (active) start();
 
-  while (__any_sync(0xffffffffu, active)) {
+  while (eng.any(active)) {
     bool go = false;
     if (active) {
       if (!in_bounds(P.bounds, y)) {
@@ -721,7 +745,10 @@ __global__ void __launch_bounds__(SG_THREADS, 1) k_trace_surrogate(TraceParams P
       }
       double E[3];
       bool used_bem;
-      surrogate_field(P, S, sm, warp, lane, ys, go, E, used_bem);
+      if (!eng.field(ys, go, E, used_bem)) {
+        engine_failed = true;
+        break;
+      }
       if (go) {
         fallbacks += used_bem ? 1 : 0;
         ks[s][0] = h * ys[3];
@@ -731,6 +758,24 @@ __global__ void __launch_bounds__(SG_THREADS, 1) k_trace_surrogate(TraceParams P
         ks[s][4] = h * qm * E[1];
         ks[s][5] = h * qm * E[2];
       }
+    }
+    if (engine_failed) {
+      // the tensor-core engine gave up waiting for its MMAs (group-uniform):
+      // the particles in hand end with TRACE_ENGINE_TIMEOUT, no new ones
+      if (active) {
+        status = TRACE_ENGINE_TIMEOUT;
+        if (P.status) P.status[idx] = status;
+        if (P.final_state) {
+          P.final_state[idx * 7] = t;
+          for (int c = 0; c < 6; c++) P.final_state[idx * 7 + 1 + c] = y[c];
+        }
+        if (P.counters) {
+          P.counters[idx * 3] = accepted;
+          P.counters[idx * 3 + 1] = attempts;
+          P.counters[idx * 3 + 2] = fallbacks;
+        }
+      }
+      return;
     }
     if (!go) continue;
     double ep = 0.0, ev = 0.0;
@@ -782,6 +827,33 @@ __global__ void __launch_bounds__(SG_THREADS, 1) k_trace_surrogate(TraceParams P
   }
 }
 
+
+// Network engine of the warp-level kernel: the 32 lanes of a warp evaluate
+// the network together with mma.sync.
+struct WarpEngine {
+  const TraceParams& P;
+  const SurrogateParams& S;
+  SurrogateSmem& sm;
+  int warp, lane;
+  __device__ bool any(bool b) const { return __any_sync(0xffffffffu, b); }
+  __device__ bool field(const double* p, bool live, double* E, bool& used_bem) {
+    surrogate_field(P, S, sm, warp, lane, p, live, E, used_bem);
+    return true;
+  }
+};
+
+__global__ void __launch_bounds__(SG_THREADS, 1) k_trace_surrogate(TraceParams P, SurrogateParams S) {
+  extern __shared__ __align__(16) unsigned char sg_raw[];
+  SurrogateSmem& sm = *reinterpret_cast<SurrogateSmem*>(sg_raw);
+  mlp_load_smem(sm.mlp, S.wb, S.pf);
+  load_segments(sm.segs, S.segs, S.nseg);
+  __syncthreads();
+  const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+
+  WarpEngine eng{P, S, sm, warp, lane};
+  surrogate_trace_loop(P, S, eng);
+}
+
 // Surrogate field at M points (one point per lane), for tests.
 __global__ void __launch_bounds__(SG_THREADS, 1)
     k_surrogate_points(TraceParams P, SurrogateParams S, const double* __restrict__ pts, int64_t M,
@@ -789,7 +861,7 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
   extern __shared__ __align__(16) unsigned char sg_raw[];
   SurrogateSmem& sm = *reinterpret_cast<SurrogateSmem*>(sg_raw);
   mlp_load_smem(sm.mlp, S.wb, S.pf);
-  for (int e = threadIdx.x; e < S.nseg * 4; e += blockDim.x) sm.segs[e / 4][e % 4] = S.segs[e];
+  load_segments(sm.segs, S.segs, S.nseg);
   __syncthreads();
   const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
   for (int64_t base = (int64_t)blockIdx.x * SG_THREADS + warp * 32; base < M; base += (int64_t)gridDim.x * SG_THREADS) {
@@ -806,6 +878,240 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
       if (used_bem) used_bem[i] = ub ? 1 : 0;
     }
   }
+}
+
+// ============================================================================
+// Tensor-memory engine of the surrogate tracer (tcgen05).  The CTA's threads
+// form TC_GROUPS groups of 128 (one warpgroup each); a group's 128 particles
+// are the 128 rows of one MMA tile.  At every RK stage the threads write
+// their input features (BF16) into the group's activation tile in shared
+// memory; one elected thread issues the layer's tcgen05.mma chain (A: the
+// activation tile, B: the layer's weights, both K-major SWIZZLE_128B in
+// shared memory; D: the group's 128 FP32 columns of tensor memory) and
+// commits it to the group's mbarrier; the threads read their own row back
+// (tcgen05.ld: thread row = TMEM lane), add the bias, apply SiLU and write
+// the next layer's BF16 activations into the same tile.  The weights are
+// staged once per CTA; one CTA per SM (shared memory ~218 KB).
+// ============================================================================
+constexpr int TC_GROUPS = 3;
+constexpr int TC_THREADS = 128 * TC_GROUPS;
+constexpr uint32_t TC_TMEM_COLS = 512;              // 3 x 128 used
+constexpr long long TC_WAIT_CYCLES = 2000000000LL;  // ~1 s; an MMA chain takes microseconds
+constexpr uint32_t TC_ATOM = 128 * 128;             // bytes of a 128-row SWIZZLE_128B atom
+
+struct TcSmem {
+  uint8_t w1[TC_ATOM];                    // W1: 128 rows x K = 16 (chunks 0, 1 of each row)
+  uint8_t wh[3][2][TC_ATOM];              // W2..W4: 128 rows x K = 128 (two atoms)
+  uint8_t w5[2][16 * 128];                // W5: 16 rows x K = 128
+  uint8_t act[TC_GROUPS][2][TC_ATOM];     // per group: activations, 128 rows x K <= 128
+  float b1[MLP_H], bh[3][MLP_H], b5[MLP_OUT];
+  double segs[SG_MAX_SEGS][5];
+  uint64_t mbar[TC_GROUPS];
+  uint32_t tmem_base;
+};
+static_assert(offsetof(TcSmem, wh) % 1024 == 0 && offsetof(TcSmem, w5) % 1024 == 0 &&
+                  offsetof(TcSmem, act) % 1024 == 0,
+              "operand tiles must be 1024-byte aligned");
+constexpr int TC_SMEM_BYTES = int(sizeof(TcSmem)) + 1024;  // + alignment slack of the dynamic window
+
+__device__ __forceinline__ void st_bf16(uint8_t* dst, __nv_bfloat16 v) { *reinterpret_cast<__nv_bfloat16*>(dst) = v; }
+
+// Stages the network in the swizzled operand layout (all threads take part).
+__device__ void tc_load_network(TcSmem& s, const __nv_bfloat16* __restrict__ wb, const float* __restrict__ pf) {
+  const int nt = blockDim.x;
+  for (int e = threadIdx.x; e < MLP_H * MLP_IN; e += nt) {
+    const int n = e / MLP_IN, k = e % MLP_IN;
+    st_bf16(s.w1 + tc::sw128(n, k >> 3) + (k & 7) * 2, wb[MLP_OFF_W1 + e]);
+  }
+  const int64_t off[3] = {MLP_OFF_W2, MLP_OFF_W3, MLP_OFF_W4};
+  for (int l = 0; l < 3; l++)
+    for (int e = threadIdx.x; e < MLP_H * MLP_H; e += nt) {
+      const int n = e / MLP_H, k = e % MLP_H;
+      st_bf16(s.wh[l][k >> 6] + tc::sw128(n, (k & 63) >> 3) + (k & 7) * 2, wb[off[l] + e]);
+    }
+  for (int e = threadIdx.x; e < MLP_OUT * MLP_H; e += nt) {
+    const int n = e / MLP_H, k = e % MLP_H;
+    st_bf16(s.w5[k >> 6] + tc::sw128(n, (k & 63) >> 3) + (k & 7) * 2, wb[MLP_OFF_W5 + e]);
+  }
+  for (int e = threadIdx.x; e < MLP_H; e += nt) {
+    s.b1[e] = pf[MLP_OFF_B1 + e];
+    s.bh[0][e] = pf[MLP_OFF_B2 + e];
+    s.bh[1][e] = pf[MLP_OFF_B3 + e];
+    s.bh[2][e] = pf[MLP_OFF_B4 + e];
+  }
+  for (int e = threadIdx.x; e < MLP_OUT; e += nt) s.b5[e] = pf[MLP_OFF_B5 + e];
+}
+
+// Issues layer `layer` (0: K = 16 -> 128, 1-3: 128 -> 128, 4: 128 -> 16) of
+// one group: A = the group's activation tile, D = its TMEM columns.
+__device__ __forceinline__ void tc_issue_layer(const TcSmem& s, uint32_t act, uint32_t dtm, int layer) {
+  constexpr uint32_t ID128 = tc::idesc_bf16_f32(128, 128);
+  constexpr uint32_t ID16 = tc::idesc_bf16_f32(128, 16);
+  if (layer == 0) {
+    tc::mma_bf16(dtm, tc::desc_sw128(act), tc::desc_sw128(tc::smem_u32(s.w1)), ID128, 0u);
+    return;
+  }
+  const uint32_t wbase = layer < 4 ? tc::smem_u32(s.wh[layer - 1][0]) : tc::smem_u32(s.w5[0]);
+  const uint32_t watom = layer < 4 ? TC_ATOM : 16u * 128u;
+  const uint32_t id = layer < 4 ? ID128 : ID16;
+#pragma unroll
+  for (int kk = 0; kk < 8; kk++) {
+    const uint32_t ka = (kk >> 2) * TC_ATOM + (kk & 3) * 32;
+    const uint32_t kb = (kk >> 2) * watom + (kk & 3) * 32;
+    tc::mma_bf16(dtm, tc::desc_sw128(act + ka), tc::desc_sw128(wbase + kb), id, kk > 0 ? 1u : 0u);
+  }
+}
+
+// One group's view of the engine.
+struct TcEngine {
+  const TraceParams& P;
+  const SurrogateParams& S;
+  TcSmem& s;
+  int g;           // group index
+  int row;         // this thread's row of the group's tile = its TMEM lane
+  uint32_t act;    // shared address of the group's activation tile
+  uint32_t dtm;    // TMEM address of the group's accumulator (lane 0)
+  uint32_t tld;    // the same with this warp's lane quarter, for tcgen05.ld
+  uint32_t phase;  // parity of the group's next mbarrier phase
+
+  __device__ bool any(bool b) const { return tc::bar_any(1 + g, 128, b); }
+
+  // Network outputs y (16) for this thread's features; all 128 threads of
+  // the group call it together.  False (group-uniform) if an MMA wait ran out.
+  __device__ bool forward(const float* feat, float* y) {
+    tc::st_shared_v4(act + tc::sw128(row, 0), pack_bf16(feat[0], feat[1]), pack_bf16(feat[2], feat[3]),
+                     pack_bf16(feat[4], feat[5]), pack_bf16(feat[6], feat[7]));
+    tc::st_shared_v4(act + tc::sw128(row, 1), pack_bf16(feat[8], feat[9]), pack_bf16(feat[10], feat[11]),
+                     pack_bf16(feat[12], feat[13]), pack_bf16(feat[14], feat[15]));
+#pragma unroll 1
+    for (int layer = 0; layer < 5; layer++) {
+      // the A tile is complete and every earlier TMEM read of the group done
+      tc::fence_async_smem();
+      tc::fence_before_sync();
+      asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
+      if (row == 0) {
+        tc::fence_after_sync();
+        tc_issue_layer(s, act, dtm, layer);
+        tc::mma_commit(&s.mbar[g]);
+      }
+      const bool ok = tc::mbar_wait_bounded(&s.mbar[g], phase, TC_WAIT_CYCLES);
+      phase ^= 1u;
+      if (tc::bar_any(1 + g, 128, !ok)) return false;
+      tc::fence_after_sync();
+      if (layer < 4) {
+        const float* bias = layer == 0 ? s.b1 : s.bh[layer - 1];
+#pragma unroll 1
+        for (int c = 0; c < 4; c++) {  // columns 32c .. 32c + 31
+          uint32_t v[32];
+          tc::tmem_ld32(tld + 32 * c, v);
+          tc::tmem_wait_ld();
+          uint32_t q[16];
+#pragma unroll
+          for (int j = 0; j < 16; j++)
+            q[j] = pack_bf16(silu(__uint_as_float(v[2 * j]) + bias[32 * c + 2 * j]),
+                             silu(__uint_as_float(v[2 * j + 1]) + bias[32 * c + 2 * j + 1]));
+          // next layer's K = 32c .. 32c + 31: atom c / 2, chunks 4 (c % 2) .. + 3
+          const uint32_t base = act + (c >> 1) * TC_ATOM;
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            tc::st_shared_v4(base + tc::sw128(row, 4 * (c & 1) + j), q[4 * j], q[4 * j + 1], q[4 * j + 2],
+                             q[4 * j + 3]);
+        }
+      } else {
+        uint32_t v[16];
+        tc::tmem_ld16(tld, v);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < MLP_OUT; j++) y[j] = __uint_as_float(v[j]) + s.b5[j];
+      }
+    }
+    return true;
+  }
+
+  __device__ bool field(const double* p, bool live, double* E, bool& used_bem) {
+    const double r2 = p[0] * p[0] + p[1] * p[1], r = sqrt(r2);
+    float f[MLP_IN], y[MLP_OUT];
+    mlp_features(r, p[2], S.dom, f);
+    if (!forward(f, y)) {
+      E[0] = E[1] = E[2] = 0.0;
+      used_bem = false;
+      return false;
+    }
+    surrogate_combine(P, S, s.segs, p, r2, r, live, y, E, used_bem);
+    return true;
+  }
+};
+
+// Shared set-up of the tcgen05 kernels: network and segments staged,
+// mbarriers initialised, TMEM allocated (warp 0).  Returns the aligned
+// shared-memory image.
+__device__ TcSmem& tc_setup(unsigned char* raw, const SurrogateParams& S) {
+  const uint32_t a = tc::smem_u32(raw);
+  TcSmem& s = *reinterpret_cast<TcSmem*>(raw + (((a + 1023u) & ~1023u) - a));
+  tc_load_network(s, S.wb, S.pf);
+  load_segments(s.segs, S.segs, S.nseg);
+  if (threadIdx.x < TC_GROUPS) tc::mbar_init(&s.mbar[threadIdx.x], 1);
+  if (threadIdx.x == 0) tc::fence_mbar_init();
+  if (threadIdx.x / 32 == 0) {
+    tc::tmem_alloc(&s.tmem_base, TC_TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  return s;
+}
+
+__device__ void tc_teardown(TcSmem& s) {
+  tc::fence_before_sync();
+  __syncthreads();
+  if (threadIdx.x / 32 == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(s.tmem_base, TC_TMEM_COLS);
+  }
+}
+
+__device__ __forceinline__ TcEngine tc_engine(const TraceParams& P, const SurrogateParams& S, TcSmem& s) {
+  const int g = threadIdx.x / 128, row = threadIdx.x % 128;
+  const uint32_t dtm = s.tmem_base + uint32_t(128 * g);
+  const uint32_t tld = dtm + (uint32_t((threadIdx.x / 32) % 4 * 32) << 16);
+  return TcEngine{P, S, s, g, row, tc::smem_u32(s.act[g][0]), dtm, tld, 0u};
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) k_trace_surrogate_tc(TraceParams P, SurrogateParams S) {
+  extern __shared__ __align__(1024) unsigned char tc_raw[];
+  TcSmem& s = tc_setup(tc_raw, S);
+  TcEngine eng = tc_engine(P, S, s);
+  surrogate_trace_loop(P, S, eng);
+  tc_teardown(s);
+}
+
+// Surrogate field at M points (one point per thread, 128 per group), for
+// tests; used_bem = -1 marks points whose MMA wait ran out.
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_surrogate_points_tc(TraceParams P, SurrogateParams S, const double* __restrict__ pts, int64_t M,
+                          double* __restrict__ field, int32_t* __restrict__ used_bem) {
+  extern __shared__ __align__(1024) unsigned char tc_raw[];
+  TcSmem& s = tc_setup(tc_raw, S);
+  TcEngine eng = tc_engine(P, S, s);
+  for (int64_t base = ((int64_t)blockIdx.x * TC_GROUPS + eng.g) * 128; base < M;
+       base += (int64_t)gridDim.x * TC_THREADS) {
+    const int64_t i = base + eng.row;
+    const bool live = i < M;
+    double p[3] = {0.5 * S.dom.r_max, 0.0, S.dom.z_c};
+    if (live)
+      for (int c = 0; c < 3; c++) p[c] = pts[3 * i + c];
+    double E[3];
+    bool ub;
+    const bool ok = eng.field(p, live, E, ub);
+    if (live) {
+      for (int c = 0; c < 3; c++) field[3 * i + c] = ok ? E[c] : __longlong_as_double(0x7ff8000000000000LL);
+      if (used_bem) used_bem[i] = ok ? (ub ? 1 : 0) : -1;
+    }
+    if (!ok) break;
+  }
+  tc_teardown(s);
 }
 
 }  // namespace tb
@@ -840,6 +1146,7 @@ static int fill_surrogate_params(const tb_field_t* field, const tb_surrogate_t* 
   S.segs = sur->segments;
   S.nseg = sur->n_segments;
   S.fb_dist2 = sur->fallback_dist * sur->fallback_dist;
+  if (sur->engine != 0 && sur->engine != 1) return BAD_ARG;
   return OK;
 }
 
@@ -852,6 +1159,16 @@ extern "C" int tb_surrogate_field_points(const double* points, int64_t M, const 
   SurrogateParams S;
   int st = fill_surrogate_params(field, sur, P, S);
   if (st != OK) return st;
+  if (sur->engine == 0) {
+    if (cudaFuncSetAttribute(k_surrogate_points_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES) !=
+        cudaSuccess)
+      return CUDA_ERR;
+    int64_t blocks = (M + TC_THREADS - 1) / TC_THREADS;
+    if (blocks > num_sms()) blocks = num_sms();
+    k_surrogate_points_tc<<<unsigned(blocks), TC_THREADS, TC_SMEM_BYTES, (cudaStream_t)stream>>>(P, S, points, M, out,
+                                                                                              used_bem);
+    return launch_status();
+  }
   const int smem = int(sizeof(SurrogateSmem));
   if (cudaFuncSetAttribute(k_surrogate_points, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
     return CUDA_ERR;
@@ -889,6 +1206,18 @@ extern "C" int tb_trace_surrogate(const double* start, const double* t0, const d
   P.work = work;
   cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemsetAsync(work, 0, sizeof(int32_t), s) != cudaSuccess) return CUDA_ERR;
+  if (sur->engine == 0) {
+    // one CTA (3 groups of 128 particles) per SM; fewer only when there are
+    // fewer particles than that
+    if (cudaFuncSetAttribute(k_trace_surrogate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES) !=
+        cudaSuccess)
+      return CUDA_ERR;
+    int64_t blocks = num_sms();
+    const int64_t by_work = (n + TC_THREADS - 1) / TC_THREADS;
+    if (blocks > by_work) blocks = by_work;
+    k_trace_surrogate_tc<<<unsigned(blocks), TC_THREADS, TC_SMEM_BYTES, s>>>(P, S);
+    return launch_status();
+  }
   const int smem = int(sizeof(SurrogateSmem));
   if (cudaFuncSetAttribute(k_trace_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
     return CUDA_ERR;

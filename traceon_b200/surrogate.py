@@ -61,7 +61,7 @@ class TbSurrogate(C.Structure):
     _fields_ = [('weights_bf16', _vp), ('params_f32', _vp), ('r_max', C.c_double), ('z_c', C.c_double),
                 ('z_half', C.c_double), ('z_lo', C.c_double), ('z_hi', C.c_double), ('n_electrodes', C.c_int),
                 ('volts', C.c_double * 5), ('scale', C.c_float * 16), ('env_power', C.c_int), ('segments', _vp),
-                ('n_segments', C.c_int), ('fallback_dist', C.c_double)]
+                ('n_segments', C.c_int), ('fallback_dist', C.c_double), ('engine', C.c_int)]
 
 
 def _call(name, *args):
@@ -337,8 +337,16 @@ class FieldSurrogate:
     series of sum_e V_e (unit table e) plus the network's correction, with the
     exact BEM field of the same charges as fallback."""
 
-    def __init__(self, model, fields, z, tabs, volts, segments, fallback_dist=50e-6):
+    ENGINES = {'tc': 0, 'warp': 1}
+
+    def __init__(self, model, fields, z, tabs, volts, segments, fallback_dist=50e-6, engine='warp'):
+        """engine: 'tc' evaluates the network with tcgen05 MMAs (groups of 128
+        particles, accumulators in tensor memory); 'warp' with warp-level
+        mma.sync (32 particles per warp)."""
         torch = B._torch()
+        if engine not in self.ENGINES:
+            raise ValueError(f'unknown engine {engine!r}; expected one of {sorted(self.ENGINES)}')
+        self.engine = engine
         self.model = model
         self.volts = np.asarray(volts, dtype=np.float64)
         assert len(self.volts) == model.n_el
@@ -369,6 +377,7 @@ class FieldSurrogate:
         s.segments = self.segments.data_ptr()
         s.n_segments = self.segments.shape[0]
         s.fallback_dist = self.fallback_dist
+        s.engine = self.ENGINES[self.engine]
         f = B.TbField(self.sources.data_ptr(), self.sources.shape[1], None, 0, None, 0, None, self.zt.data_ptr(),
                       self.table.data_ptr(), None, len(self.z))
         return f, s
