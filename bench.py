@@ -388,7 +388,8 @@ def run_gpu(args):
         achieved = evals * MLP_FLOP_PER_EVAL / launch_s / 1e12
         peak = peaks.get('bf16_tflops')
         roof = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
-                'frac': achieved / peak if peak else None, 'traffic': args.traffic, 'kernel': 'k_trace_surrogate',
+                'frac': achieved / peak if peak else None, 'traffic': args.traffic,
+                'kernel': 'k_trace_surrogate_tc' if args.engine == 'tc' else 'k_trace_surrogate',
                 'flop_per_unit': MLP_FLOP_PER_EVAL, 'units_per_launch': evals,
                 'unit_desc': 'network evaluations (dense BF16 flops of the 16-128x4-16 MLP)',
                 'peak_source': 'MEASURED_PEAKS.json bf16_tflops (burst)'}
@@ -457,7 +458,7 @@ def main():
     ap.add_argument('--train-samples', type=int, default=1 << 22)
     ap.add_argument('--train-steps', type=int, default=40000)
     ap.add_argument('--team-warps', type=int, default=0)
-    ap.add_argument('--engine', default='warp', choices=['tc', 'warp'],
+    ap.add_argument('--engine', default='tc', choices=['tc', 'warp'],
                     help='surrogate network engine: tcgen05 (tc) or warp-level mma.sync (warp)')
     ap.add_argument('--check', type=int, default=16, help='electrons checked against the CPU oracle')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)

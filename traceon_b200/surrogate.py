@@ -339,7 +339,7 @@ class FieldSurrogate:
 
     ENGINES = {'tc': 0, 'warp': 1}
 
-    def __init__(self, model, fields, z, tabs, volts, segments, fallback_dist=50e-6, engine='warp'):
+    def __init__(self, model, fields, z, tabs, volts, segments, fallback_dist=50e-6, engine='tc'):
         """engine: 'tc' evaluates the network with tcgen05 MMAs (groups of 128
         particles, accumulators in tensor memory); 'warp' with warp-level
         mma.sync (32 particles per warp)."""
