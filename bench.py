@@ -220,6 +220,63 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- precision solve
+def precision_solve(n, nrhs=8, seed=2):
+    """The precision workload's charge solve: the three-electrode lens meshed
+    to n cubic elements, nrhs right-hand sides with every electrode voltage
+    ~U[-3, 3] kV.  GPU FP64 fill (+ singular self terms), then (a) the FP64
+    LU with partial pivoting (numpy.linalg.solve's factorisation) and (b) the
+    mixed solve (FP32 tensor-core LU of the equilibrated matrix, FP64
+    iterative refinement).  CUDA-event times; charges of (b) against (a)."""
+    import torch
+    from traceon_b200 import backend as B
+    from traceon_b200.geometry import einzel_lens
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    geo = einzel_lens(n)
+    v = B.to_dev(geo.vertices, torch.float64)
+    t = B.to_dev(np.ones(n, np.uint8), torch.uint8)
+    val = B.to_dev(np.zeros(n), torch.float64)
+    A = torch.empty((n, n), dtype=torch.float64, device='cuda')
+
+    def fill():
+        jac, pos = B.dev_jacobian_buffer(v)
+        B.dev_fill_matrix(A, v, t, val, jac, pos)
+        B.dev_self_integrals(v, t, val, A)
+
+    fill()  # warm-up
+    fill_ms, _ = timed(fill)
+    rng = np.random.default_rng(seed)
+    F = torch.as_tensor(geo.voltages_to_values(rng.uniform(-3000, 3000, (nrhs, 3)).T).T.copy(), device='cuda')
+
+    def lu64():
+        LU = A.clone()
+        _, perm = B.dev_lu_factor(LU)
+        return B.dev_lu_solve(LU, perm, F)
+
+    lu64()
+    lu_ms, X64 = timed(lu64)
+    B.dev_solve_mixed(A, F)
+    mixed_ms, (Xm, iters, rel) = timed(lambda: B.dev_solve_mixed(A, F))
+    err = float(((Xm - X64).abs().amax(1) / X64.abs().amax(1)).max())
+    out = {'workload': f'einzel lens, {n} cubic elements, {nrhs} right-hand sides (electrode voltages U[-3,3] kV)',
+           'fill_fp64_ms': fill_ms, 'solve_fp64_lu_ms': lu_ms, 'solve_mixed_ms': mixed_ms,
+           'mixed_iterations': iters, 'mixed_last_correction': rel, 'charges_rel_err_vs_fp64': err,
+           'speedup_solve': lu_ms / mixed_ms, 'speedup_fill_plus_solve': (fill_ms + lu_ms) / (fill_ms + mixed_ms),
+           'lu_flop': 2.0 / 3.0 * n ** 3}
+    del A
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm
 def measure_fp64_peak(B, torch):
     out = torch.zeros(1, dtype=torch.float64, device='cuda')
@@ -405,6 +462,8 @@ def run_gpu(args):
                 'unit_desc': 'ring-pair field evaluations (executed FP64 flops per pair, ncu)',
                 'peak_source': 'measured FP64 FMA probe (tb_probe_fp64_fma) in this run'}
 
+    precision = precision_solve(args.precision_n) if args.precision_n > 0 else None
+
     # ---- accuracy vs the CPU oracle and the CPU baseline (rank 0, N = 1)
     cores = host_cores()
     q_or, jac_or, pos_or = oracle_charges(geo, volts, cores)
@@ -438,7 +497,7 @@ def run_gpu(args):
                             'accepted_steps_mean': float(counters[:, 0].mean()),
                             'attempts_mean': float(counters[:, 1].mean()),
                             'bem_fallback_evals': int(counters[:, 2].sum()) if counters.shape[1] > 2 else None},
-            'setup': setup}
+            'setup': setup, 'precision_solve': precision}
     print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -462,6 +521,8 @@ def main():
                     help='surrogate network engine: tcgen05 (tc) or warp-level mma.sync (warp)')
     ap.add_argument('--check', type=int, default=16, help='electrons checked against the CPU oracle')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
+    ap.add_argument('--precision-n', type=int, default=16384,
+                    help='elements of the precision-workload solve measured beside the tracer (0: skip)')
     ap.add_argument('--ref-seconds', type=float, default=20.0)
     # executed FP64 flops per ring-pair evaluation of the tracer's field sum
     # (dadd + dmul + 2 dfma per pair, from the ncu instruction counts)

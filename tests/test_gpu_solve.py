@@ -80,3 +80,46 @@ def test_mixed_solve_reports_failure_and_solver_falls_back(cuda):
     X = s.solve_charges_device(F.cpu().numpy(), method='mixed').cpu().numpy()
     assert s.solve_info['method'] == 'lu' and 'fallback' in s.solve_info
     assert _close(X, np.linalg.solve(A_h, F.cpu().numpy().T).T) < 1e-10
+
+
+@pytest.mark.parametrize('M,N,K', [(128, 256, 32), (300, 500, 256), (1000, 700, 100), (37, 9, 5)])
+def test_gemm_tf32x3_vs_fp64(cuda, M, N, K):
+    """The tensor-core update C -= A B (tcgen05, 3xTF32) against FP64 numpy,
+    on strided sub-matrices with sizes that are not multiples of the 128 x 256
+    tile or the 32-wide K chunk: FP32-level accuracy."""
+    import torch
+    rng = np.random.default_rng(M + N + K)
+    big_a = rng.normal(size=(M + 3, K + 5)).astype(np.float32)
+    big_b = rng.normal(size=(K + 2, N + 7)).astype(np.float32)
+    big_c = rng.normal(size=(M + 1, N + 3)).astype(np.float32)
+    At = torch.as_tensor(big_a, device='cuda')[1:M + 1, 2:K + 2]
+    Bt = torch.as_tensor(big_b, device='cuda')[1:K + 1, 3:N + 3]
+    Ct = torch.as_tensor(big_c, device='cuda')
+    cuda.dev_gemm_sub_tf32x3(Ct[1:M + 1, 1:N + 1], At, Bt)
+    out = Ct.cpu().numpy().astype(np.float64)
+    ref = big_c.astype(np.float64)
+    ref[1:M + 1, 1:N + 1] -= big_a[1:M + 1, 2:K + 2].astype(np.float64) @ big_b[1:K + 1, 3:N + 3].astype(np.float64)
+    scale = np.abs(big_a[1:M + 1, 2:K + 2]).astype(np.float64) @ np.abs(big_b[1:K + 1, 3:N + 3]).astype(np.float64)
+    inner = np.abs(out[1:M + 1, 1:N + 1] - ref[1:M + 1, 1:N + 1]) / (scale + 1.0)
+    assert inner.max() < 1e-5
+    # everything outside the sub-matrix untouched
+    mask = np.ones_like(out, dtype=bool)
+    mask[1:M + 1, 1:N + 1] = False
+    assert np.array_equal(out[mask], ref[mask])
+
+
+def test_lu_nopiv_tc_factors(cuda):
+    """The FP32 LU with tensor-core trailing updates (256-column panels): on a
+    BEM matrix of 700 elements (three panels, the last partial) L U
+    reproduces the column-equilibrated FP32 matrix to FP32 accuracy."""
+    import torch
+    A, F = _matrix(cuda, 700)
+    A_h = A.cpu().numpy()
+    c = 1.0 / np.abs(A_h).max(axis=0)
+    S_h = (A_h * c).astype(np.float32)
+    S = torch.as_tensor(S_h, device='cuda')
+    cuda.dev_lu_nopiv_tc(S)
+    LU = S.cpu().numpy().astype(np.float64)
+    L = np.tril(LU, -1) + np.eye(700)
+    U = np.triu(LU)
+    assert np.abs(L @ U - S_h).max() < 2e-5 * np.abs(S_h).max()

@@ -46,7 +46,7 @@ N_TRIANGLE_QUAD = C.c_int.in_dll(backend_lib, 'N_TRIANGLE_QUAD_SYM').value
 NU_MAX = C.c_int.in_dll(backend_lib, 'NU_MAX_SYM').value
 M_MAX = C.c_int.in_dll(backend_lib, 'M_MAX_SYM').value
 
-TB_OK, TB_BAD_ARG, TB_CUDA_ERR, TB_NONFINITE, TB_UNSUPPORTED, TB_SINGULAR = range(6)
+TB_OK, TB_BAD_ARG, TB_CUDA_ERR, TB_NONFINITE, TB_UNSUPPORTED, TB_SINGULAR, TB_TIMEOUT = range(7)
 TRACE_EXITED, TRACE_MAX_ATTEMPTS, TRACE_ROWS_FULL, TRACE_NONFINITE, TRACE_ENGINE_TIMEOUT = range(5)
 
 dbl = C.c_double
@@ -214,6 +214,8 @@ _DEV = {
     'tb_probe_math': (vp, i64, C.c_int, vp, vp),
     'tb_lu_nopiv_f64': (vp, i64, i64, vp),
     'tb_lu_nopiv_f32': (vp, i64, i64, vp),
+    'tb_lu_nopiv_f32_tc': (vp, i64, i64, vp, vp),
+    'tb_gemm_sub_tf32x3': (vp, i64, vp, i64, vp, i64, i64, i64, i64, vp, vp),
     'tb_solve_mixed': (vp, i64, i64, vp, vp, i64, vp, i64, C.c_int, dbl, C.POINTER(C.c_int), C.POINTER(dbl), vp),
 }
 for _name, _args in _DEV.items():
@@ -610,6 +612,29 @@ def dev_lu_nopiv(A):
     torch = _torch()
     name = 'tb_lu_nopiv_f64' if A.dtype == torch.float64 else 'tb_lu_nopiv_f32'
     _call(name, _ptr(A), A.stride(0), A.shape[0], _stream())
+
+
+def dev_lu_nopiv_tc(A):
+    """In-place FP32 LU without pivoting, trailing updates on the tensor
+    cores (3xTF32)."""
+    torch = _torch()
+    err = torch.zeros(1, dtype=torch.int32, device=A.device)
+    _call('tb_lu_nopiv_f32_tc', _ptr(A), A.stride(0), A.shape[0], _ptr(err), _stream())
+    if int(err.item()):
+        raise BackendError('tb_lu_nopiv_f32_tc: a bounded wait in the tensor-core kernel ran out')
+
+
+def dev_gemm_sub_tf32x3(C, A, B):
+    """C -= A @ B (FP32 device matrices, unit column stride) on the tensor
+    cores with 3xTF32."""
+    torch = _torch()
+    M, K = A.shape
+    N = B.shape[1]
+    err = torch.zeros(1, dtype=torch.int32, device=C.device)
+    _call('tb_gemm_sub_tf32x3', _ptr(C), C.stride(0), _ptr(A), A.stride(0), _ptr(B), B.stride(0), M, N, K, _ptr(err),
+          _stream())
+    if int(err.item()):
+        raise BackendError('tb_gemm_sub_tf32x3: a bounded wait in the tensor-core kernel ran out')
 
 
 def dev_solve_mixed(A, F, max_iter=12, tol=1e-12):

@@ -361,6 +361,7 @@ enum Status : int {
   NONFINITE = 3,
   UNSUPPORTED = 4,
   SINGULAR = 5,
+  TIMEOUT = 6,  // a bounded wait inside a kernel ran out
 };
 
 // Per-particle tracer status.

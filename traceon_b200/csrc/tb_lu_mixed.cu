@@ -10,7 +10,10 @@
 // graded meshes from the condition number (about 9.6e4 -> 2.3e3 at
 // N = 1000), which is what lets FP32 factors converge under refinement.
 //
-// Blocked right-looking factorisation, per panel of NB columns:
+// The mixed solve factors with lu_nopiv_f32_tc (256-column panels, trailing
+// updates on the tensor cores, below); tb_lu_nopiv_f32 / _f64 keep the plain
+// one-level blocking.  Blocked right-looking factorisation, per panel of NB
+// columns:
 //   k_diag_lu      one CTA factors the NB x NB diagonal block in shared memory
 //   k_trsm_right   L21 = A21 U11^-1   (one thread per row)
 //   k_trsm_left    U12 = L11^-1 A12   (one thread per column)
@@ -19,6 +22,7 @@
 
 #include "tb_common.cuh"
 #include "tb_internal.cuh"
+#include "tb_tc.cuh"
 #include "../../include/traceon_b200.h"
 
 namespace tb {
@@ -65,14 +69,15 @@ __global__ void __launch_bounds__(128) k_trsm_right(T* __restrict__ A, int64_t l
   }
 }
 
-// columns j >= k0 + nb: A[k0:k0+nb, j] <- L11^-1 A[k0:k0+nb, j] (L11 unit lower)
+// columns c0 <= j < c1: A[k0:k0+nb, j] <- L11^-1 A[k0:k0+nb, j] (L11 unit lower)
 template <class T>
-__global__ void __launch_bounds__(128) k_trsm_left(T* __restrict__ A, int64_t lda, int64_t N, int64_t k0, int nb) {
+__global__ void __launch_bounds__(128)
+    k_trsm_left(T* __restrict__ A, int64_t lda, int64_t c0, int64_t c1, int64_t k0, int nb) {
   __shared__ T L[MX_NB][MX_NB + 1];
   for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) L[e / nb][e % nb] = A[(k0 + e / nb) * lda + k0 + e % nb];
   __syncthreads();
-  int64_t c = k0 + nb + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c >= N) return;
+  int64_t c = c0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= c1) return;
   T x[MX_NB];
 #pragma unroll
   for (int i = 0; i < MX_NB; i++) {
@@ -141,6 +146,216 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------- tensor cores
+// C (M x Nc, ldc) -= A (M x K, lda) . B (K x Nc, ldb), FP32 row-major, on
+// the 5th-generation tensor cores (tcgen05.mma kind::tf32) with 3xTF32:
+// every operand is split into a TF32 head (cvt.rna.tf32) and the FP32 tail
+// x - head, and head.head + head.tail + tail.head is accumulated in FP32 in
+// tensor memory -- about FP32 accuracy at tensor-core speed.  CTA tile
+// 128 x 256 (TMEM: 256 FP32 columns), K in chunks of 32 (one SWIZZLE_128B
+// atom of FP32 per row), staged by all 256 threads into two buffers so that
+// the staging of chunk k + 1 overlaps the MMAs of chunk k.  B is staged
+// transposed (N rows x K), so both operands are K-major.
+constexpr int GT_M = 128, GT_N = 256, GT_K = 32, GT_THREADS = 256;
+constexpr long long GT_WAIT_CYCLES = 2000000000LL;  // ~1 s
+
+struct GemmSmem {
+  uint8_t a_hi[2][GT_M * 128];
+  uint8_t a_lo[2][GT_M * 128];
+  uint8_t b_hi[2][GT_N * 128];
+  uint8_t b_lo[2][GT_N * 128];
+  uint64_t mbar[2];
+  uint32_t tmem_base;
+};
+constexpr int GT_SMEM_BYTES = int(sizeof(GemmSmem)) + 1024;
+
+__device__ __forceinline__ void split_tf32(float v, float& hi, float& lo) {
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(v));
+  hi = __uint_as_float(h);
+  lo = v - hi;
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__global__ void __launch_bounds__(GT_THREADS, 1)
+    k_gemm_sub_tf32x3(float* __restrict__ C, int64_t ldc, const float* __restrict__ A, int64_t lda,
+                      const float* __restrict__ B, int64_t ldb, int64_t M, int64_t Nc, int K, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char gt_raw[];
+  const uint32_t raw = tc::smem_u32(gt_raw);
+  GemmSmem& sm = *reinterpret_cast<GemmSmem*>(gt_raw + (((raw + 1023u) & ~1023u) - raw));
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int64_t m0 = (int64_t)blockIdx.y * GT_M, n0 = (int64_t)blockIdx.x * GT_N;
+  if (tid < 2) tc::mbar_init(&sm.mbar[tid], 1);
+  if (tid == 0) tc::fence_mbar_init();
+  if (warp == 0) {
+    tc::tmem_alloc(&sm.tmem_base, GT_N);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t dtm = sm.tmem_base;
+  // kind::tf32: A, B TF32 (format 2), D FP32, K-major, M = 128, N = 256
+  constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(GT_N >> 3) << 17) |
+                             (uint32_t(GT_M >> 4) << 24);
+  const int nk = (K + GT_K - 1) / GT_K;
+  bool ok = true;
+  for (int kc = 0; kc < nk; kc++) {
+    const int b = kc & 1;
+    if (kc >= 2) {  // the MMAs of chunk kc - 2 read buffer b
+      const bool w = tc::mbar_wait_bounded(&sm.mbar[b], uint32_t((kc - 2) >> 1) & 1u, GT_WAIT_CYCLES);
+      if (__syncthreads_or(!w)) {
+        ok = false;
+        break;
+      }
+    }
+    const int k0 = kc * GT_K;
+    const uint32_t ah = tc::smem_u32(sm.a_hi[b]), al = tc::smem_u32(sm.a_lo[b]);
+    const uint32_t bh = tc::smem_u32(sm.b_hi[b]), bl = tc::smem_u32(sm.b_lo[b]);
+    // A: rows r (warp-strided), k = k0 + lane (one coalesced 128-byte row segment per warp)
+    for (int r = warp; r < GT_M; r += GT_THREADS / 32) {
+      const int64_t gr = m0 + r;
+      const int k = k0 + lane;
+      const float v = (gr < M && k < K) ? A[gr * lda + k] : 0.f;
+      float hi, lo;
+      split_tf32(v, hi, lo);
+      const uint32_t off = tc::sw128(r, lane >> 2) + (lane & 3) * 4;
+      asm volatile("st.shared.f32 [%0], %1;" ::"r"(ah + off), "f"(hi) : "memory");
+      asm volatile("st.shared.f32 [%0], %1;" ::"r"(al + off), "f"(lo) : "memory");
+    }
+    // B: k-rows (warp-strided), n = 32 seg + lane; stored transposed (row n, column k)
+    for (int kk = warp; kk < GT_K; kk += GT_THREADS / 32) {
+      const int k = k0 + kk;
+#pragma unroll
+      for (int seg = 0; seg < GT_N / 32; seg++) {
+        const int n = 32 * seg + lane;
+        const int64_t gn = n0 + n;
+        const float v = (k < K && gn < Nc) ? B[(int64_t)k * ldb + gn] : 0.f;
+        float hi, lo;
+        split_tf32(v, hi, lo);
+        const uint32_t off = tc::sw128(n, kk >> 2) + (kk & 3) * 4;
+        asm volatile("st.shared.f32 [%0], %1;" ::"r"(bh + off), "f"(hi) : "memory");
+        asm volatile("st.shared.f32 [%0], %1;" ::"r"(bl + off), "f"(lo) : "memory");
+      }
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < GT_K / 8; ks++) {  // K = 8 (32 bytes) per instruction
+        const uint64_t dah = tc::desc_sw128(ah + 32 * ks), dal = tc::desc_sw128(al + 32 * ks);
+        const uint64_t dbh = tc::desc_sw128(bh + 32 * ks), dbl = tc::desc_sw128(bl + 32 * ks);
+        mma_tf32(dtm, dal, dbh, IDESC, (kc > 0 || ks > 0) ? 1u : 0u);
+        mma_tf32(dtm, dah, dbl, IDESC, 1u);
+        mma_tf32(dtm, dah, dbh, IDESC, 1u);
+      }
+      tc::mma_commit(&sm.mbar[b]);
+    }
+  }
+  if (ok && nk > 0) {
+    const int bl = (nk - 1) & 1;
+    const bool w = tc::mbar_wait_bounded(&sm.mbar[bl], uint32_t((nk - 1) >> 1) & 1u, GT_WAIT_CYCLES);
+    ok = !__syncthreads_or(!w);
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+  } else if (nk > 0) {
+    tc::fence_after_sync();
+    // warp w: TMEM lanes 32 (w % 4) .. (rows), columns 128 (w / 4) ..
+    const int row = 32 * (warp % 4) + lane;
+    const int64_t gr = m0 + row;
+    const uint32_t tbase = dtm + (uint32_t(32 * (warp % 4)) << 16) + uint32_t(128 * (warp / 4));
+#pragma unroll 1
+    for (int c = 0; c < 8; c++) {
+      uint32_t v[16];
+      tc::tmem_ld16(tbase + 16 * c, v);
+      tc::tmem_wait_ld();
+      if (gr < M) {
+        float* crow = C + gr * ldc + n0 + 128 * (warp / 4) + 16 * c;
+        const int64_t col0 = n0 + 128 * (warp / 4) + 16 * c;
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+          if (col0 + j < Nc) crow[j] -= __uint_as_float(v[j]);
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(dtm, GT_N);
+  }
+}
+
+static int gemm_sub_tf32x3(float* C, int64_t ldc, const float* A, int64_t lda, const float* B, int64_t ldb,
+                           int64_t M, int64_t Nc, int K, int* err, cudaStream_t s) {
+  if (M <= 0 || Nc <= 0 || K <= 0) return OK;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return CUDA_ERR;
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    if (cudaFuncSetAttribute(k_gemm_sub_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, GT_SMEM_BYTES) !=
+        cudaSuccess)
+      return CUDA_ERR;
+    attr_set[dev] = true;
+  }
+  dim3 grid(unsigned((Nc + GT_N - 1) / GT_N), unsigned((M + GT_M - 1) / GT_M));
+  k_gemm_sub_tf32x3<<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err);
+  return launch_status();
+}
+
+// FP32 LU without pivoting, two-level blocked: panels of 256 columns are
+// factored with the 64-wide kernels above (diagonal block, triangular
+// solves, SIMT updates inside the panel and its row block), and the
+// trailing matrix is updated once per panel on the tensor cores
+// (K = 256).  err receives 1 if a tensor-core wait ran out.
+constexpr int TC_PANEL = 256;
+static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, cudaStream_t s) {
+  for (int64_t p0 = 0; p0 < N; p0 += TC_PANEL) {
+    const int64_t pe = p0 + TC_PANEL < N ? p0 + TC_PANEL : N;
+    for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
+      const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
+      k_diag_lu<float><<<1, 256, 0, s>>>(A, lda, k0, nb);
+      const int64_t below = N - k0 - nb, right = pe - k0 - nb;
+      if (below > 0) k_trsm_right<float><<<unsigned((below + 127) / 128), 128, 0, s>>>(A, lda, N, k0, nb);
+      if (right > 0) {
+        k_trsm_left<float><<<unsigned((right + 127) / 128), 128, 0, s>>>(A, lda, k0 + nb, pe, k0, nb);
+        dim3 grid(unsigned((right + 127) / 128), unsigned((below + 127) / 128));
+        k_gemm_update<float><<<grid, 256, 0, s>>>(A + (k0 + nb) * lda + k0 + nb, lda, A + (k0 + nb) * lda + k0, lda,
+                                                  A + k0 * lda + k0 + nb, lda, below, right, nb);
+      }
+    }
+    const int64_t rest = N - pe;
+    if (rest <= 0) break;
+    // row block right of the panel: U12 = L11^-1 A12, 64 rows at a time
+    for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
+      const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
+      k_trsm_left<float><<<unsigned((rest + 127) / 128), 128, 0, s>>>(A, lda, pe, N, k0, nb);
+      const int64_t rows = pe - k0 - nb;
+      if (rows > 0) {
+        dim3 grid(unsigned((rest + 127) / 128), unsigned((rows + 127) / 128));
+        k_gemm_update<float><<<grid, 256, 0, s>>>(A + (k0 + nb) * lda + pe, lda, A + (k0 + nb) * lda + k0, lda,
+                                                  A + k0 * lda + pe, lda, rows, rest, nb);
+      }
+    }
+    const int st = gemm_sub_tf32x3(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest,
+                                   int(pe - p0), err, s);
+    if (st != OK) return st;
+  }
+  return launch_status();
+}
+
 // ---------------------------------------------------------------- mixed solve
 // c[j] = 1 / max_i |A[i, j]| (one block of 8 warps per 32 columns, rows strided over the warps)
 __global__ void k_col_maxabs(const double* __restrict__ A, int64_t lda, int64_t N, double* __restrict__ c) {
@@ -194,52 +409,151 @@ __global__ void k_residual(const double* __restrict__ A, int64_t lda, const doub
   }
 }
 
-// Triangular solves with FP32 factors and FP64 right-hand sides (the
-// correction equation of the refinement), blocked like tb_lu_solve_perm.
-template <bool LOWER>
-__global__ void k_trsv_block_f32(const float* __restrict__ LU, int64_t lda, double* __restrict__ X, int64_t N,
-                                 int64_t b0, int nb, int nrhs) {
-  __shared__ double Tm[MX_NB][MX_NB + 1];
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) Tm[e / nb][e % nb] = LU[(b0 + e / nb) * lda + b0 + e % nb];
-  __syncthreads();
-  int r = threadIdx.x;
-  if (r >= nrhs) return;
-  double* x = X + r * N + b0;
-  if (LOWER) {
-    for (int i = 0; i < nb; i++) {
-      double v = x[i];
-      for (int m = 0; m < i; m++) v = fma(-Tm[i][m], x[m], v);
-      x[i] = v;
-    }
-  } else {
-    for (int i = nb - 1; i >= 0; i--) {
-      double v = x[i];
-      for (int m = i + 1; m < nb; m++) v = fma(-Tm[i][m], x[m], v);
-      x[i] = v / Tm[i][i];
-    }
-  }
+// ---------------------------------------------------------------- sweeps
+// One launch per triangular sweep of the refinement's correction equation.
+// CTA q owns row block b (64 rows; b = q for the forward sweep with the unit
+// lower factor, b = nblk - 1 - q for the backward sweep with the upper
+// factor), so every block it depends on belongs to a CTA launched before it.
+// It accumulates the products of its off-diagonal factor tiles with the
+// finished blocks' solutions as their flags appear, then applies the FP64
+// inverse of its diagonal block (computed once after the factorisation) and
+// publishes its block: solution to X, then the flag (release / acquire).
+// Waits are bounded: after TRSV_WAIT_CYCLES the CTA records an error and
+// writes NaN, which the refinement reports as non-convergence.
+constexpr int TS_B = 64;
+constexpr long long TRSV_WAIT_CYCLES = 2000000000LL;  // ~1 s
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__global__ void k_trsv_update_f32(const float* __restrict__ LU, int64_t lda, double* __restrict__ X, int64_t N,
-                                  int64_t b0, int nb, int64_t i0, int64_t i1, int nrhs) {
-  __shared__ double xs[MX_MAX_RHS][MX_NB];
-  for (int e = threadIdx.x; e < nrhs * nb; e += blockDim.x) xs[e / nb][e % nb] = X[(e / nb) * N + b0 + e % nb];
-  __syncthreads();
-  int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= i1) return;
-  const float* row = LU + i * lda + b0;
-  double acc[MX_MAX_RHS];
-#pragma unroll
-  for (int r = 0; r < MX_MAX_RHS; r++) acc[r] = 0.0;
-  for (int m = 0; m < nb; m++) {
-    double l = row[m];
-#pragma unroll
-    for (int r = 0; r < MX_MAX_RHS; r++)
-      if (r < nrhs) acc[r] = fma(l, xs[r][m], acc[r]);
+// Dinv[blk] = inverse of the 64 x 64 diagonal block blk of the factor (unit
+// lower or upper triangle of LU), in FP64; rows / columns beyond N are the
+// identity.  One CTA of 64 threads per block, one column per thread.
+template <bool LOWER>
+__global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__ LU, int64_t lda, int64_t N,
+                                                      double* __restrict__ Dinv) {
+  __shared__ float T[TS_B][TS_B];    // the factor block (FP32 values, exact)
+  __shared__ double Xc[TS_B][TS_B];  // Xc[row][col]; thread k owns column k
+  const int64_t b0 = (int64_t)blockIdx.x * TS_B;
+  const int nb = N - b0 < TS_B ? int(N - b0) : TS_B;
+  for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) {
+    const int i = e / TS_B, j = e % TS_B;
+    float v = (i == j) ? 1.f : 0.f;
+    if (i < nb && j < nb) {
+      const float a = LU[(b0 + i) * lda + b0 + j];
+      if (LOWER ? (i > j) : (i <= j)) v = a;
+    }
+    T[i][j] = v;
   }
+  __syncthreads();
+  const int k = threadIdx.x;  // column k of the inverse: T x = e_k
+  if (LOWER) {
+    for (int i = 0; i < TS_B; i++) {
+      double v = (i == k) ? 1.0 : 0.0;
+      for (int m = 0; m < i; m++) v = fma(-double(T[i][m]), Xc[m][k], v);
+      Xc[i][k] = v;
+    }
+  } else {
+    for (int i = TS_B - 1; i >= 0; i--) {
+      double v = (i == k) ? 1.0 : 0.0;
+      for (int m = i + 1; m < TS_B; m++) v = fma(-double(T[i][m]), Xc[m][k], v);
+      Xc[i][k] = v / double(T[i][i]);
+    }
+  }
+  __syncthreads();
+  // stored column-major: D[m * 64 + i] = (T^-1)[i][m]
+  double* D = Dinv + (int64_t)blockIdx.x * TS_B * TS_B;
+  for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) D[e] = Xc[e % TS_B][e / TS_B];
+}
+
+// X (nrhs x N, row r at X + r N) <- T^-1 X with T the unit lower (LOWER) or
+// upper triangle of LU.  256 threads: thread = (row i of the block, group of
+// 4 right-hand sides).  flags[blk] == epoch marks a published block.
+template <bool LOWER>
+__global__ void __launch_bounds__(256) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
+                                                   const double* __restrict__ Dinv, double* __restrict__ X, int nrhs,
+                                                   int* __restrict__ flags, int epoch, int* __restrict__ err) {
+  __shared__ float Lt[TS_B][TS_B + 1];
+  __shared__ double xs[MX_MAX_RHS][TS_B];
+  __shared__ int s_fail;
+  const int nblk = int((N + TS_B - 1) / TS_B);
+  const int q = blockIdx.x;
+  const int b = LOWER ? q : nblk - 1 - q;
+  const int64_t b0 = (int64_t)b * TS_B;
+  const int i = threadIdx.x % TS_B, rg = threadIdx.x / TS_B;
+  if (threadIdx.x == 0) s_fail = 0;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int t = 0; t < q; t++) {
+    const int j = LOWER ? t : nblk - 1 - t;  // a finished block, in publication order
+    const int64_t j0 = (int64_t)j * TS_B;
+    // factor tile (rows of block b, columns of block j), coalesced along rows
+    for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) {
+      const int r = e / TS_B, c = e % TS_B;
+      Lt[r][c] = (b0 + r < N && j0 + c < N) ? LU[(b0 + r) * lda + j0 + c] : 0.f;
+    }
+    if (threadIdx.x == 0) {
+      const long long t0 = clock64();
+      while (ld_acquire(flags + j) != epoch) {
+        if (clock64() - t0 > TRSV_WAIT_CYCLES) {
+          s_fail = 1;
+          atomicExch(err, 1);
+          break;
+        }
+      }
+    }
+    __syncthreads();
+    if (s_fail) break;
+    for (int e = threadIdx.x; e < nrhs * TS_B; e += blockDim.x) {
+      const int r = e / TS_B, c = e % TS_B;
+      xs[r][c] = (j0 + c < N) ? __ldcg(X + (int64_t)r * N + j0 + c) : 0.0;  // published by another CTA: via L2
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int m = 0; m < TS_B; m++) {
+      const double l = Lt[i][m];
 #pragma unroll
-  for (int r = 0; r < MX_MAX_RHS; r++)
-    if (r < nrhs) X[r * N + i] -= acc[r];
+      for (int u = 0; u < 4; u++) {
+        const int r = 4 * rg + u;
+        if (r < nrhs) acc[u] = fma(l, xs[r][m], acc[u]);
+      }
+    }
+    __syncthreads();
+  }
+  // right-hand side minus the accumulated products, then the diagonal inverse
+  __shared__ double rs[MX_MAX_RHS][TS_B];
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int r = 4 * rg + u;
+    if (r < nrhs) rs[r][i] = (b0 + i < N) ? X[(int64_t)r * N + b0 + i] - acc[u] : 0.0;
+  }
+  __syncthreads();
+  const double* D = Dinv + (int64_t)b * TS_B * TS_B;
+  double out[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int m = 0; m < TS_B; m++) {
+    const double d = D[m * TS_B + i];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int r = 4 * rg + u;
+      if (r < nrhs) out[u] = fma(d, rs[r][m], out[u]);
+    }
+  }
+  const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int r = 4 * rg + u;
+    if (r < nrhs && b0 + i < N) X[(int64_t)r * N + b0 + i] = s_fail ? nan : out[u];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release(flags + b, epoch);
+  }
 }
 
 // X[r, j] += c[j] D[r, j]; also the largest |c D| / |X| over all entries
@@ -269,7 +583,7 @@ static int lu_nopiv(T* A, int64_t lda, int64_t N, cudaStream_t s) {
     if (rest > 0) {
       unsigned g = unsigned((rest + 127) / 128);
       k_trsm_right<T><<<g, 128, 0, s>>>(A, lda, N, k0, nb);
-      k_trsm_left<T><<<g, 128, 0, s>>>(A, lda, N, k0, nb);
+      k_trsm_left<T><<<g, 128, 0, s>>>(A, lda, k0 + nb, N, k0, nb);
       dim3 grid(unsigned((rest + 127) / 128), unsigned((rest + 127) / 128));
       k_gemm_update<T><<<grid, 256, 0, s>>>(A + (k0 + nb) * lda + k0 + nb, lda, A + (k0 + nb) * lda + k0, lda,
                                             A + k0 * lda + k0 + nb, lda, rest, rest, nb);
@@ -294,10 +608,30 @@ extern "C" int tb_lu_nopiv_f32(float* A, int64_t lda, int64_t N, tb_stream_t str
   return lu_nopiv<float>(A, lda, N, (cudaStream_t)stream);
 }
 
+static int64_t round256(int64_t b) { return (b + 255) / 256 * 256; }
+
+extern "C" int tb_lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, tb_stream_t stream) {
+  if (N < 0 || lda < N || (N > 0 && (!A || !err)) || N > 0x7fffffff) return BAD_ARG;
+  if (N == 0) return OK;
+  return lu_nopiv_f32_tc(A, lda, N, err, (cudaStream_t)stream);
+}
+
+extern "C" int tb_gemm_sub_tf32x3(float* C, int64_t ldc, const float* A, int64_t lda, const float* B, int64_t ldb,
+                                  int64_t M, int64_t N, int64_t K, int* err, tb_stream_t stream) {
+  if (M < 0 || N < 0 || K < 0 || K > 0x7fffffff || !err) return BAD_ARG;
+  if (M == 0 || N == 0 || K == 0) return OK;
+  if (!C || !A || !B || ldc < N || lda < K || ldb < N) return BAD_ARG;
+  return gemm_sub_tf32x3(C, ldc, A, lda, B, ldb, M, N, int(K), err, (cudaStream_t)stream);
+}
+
 extern "C" int64_t tb_solve_mixed_workspace(int64_t N, int64_t nrhs) {
   if (N <= 0 || nrhs <= 0) return 0;
-  // FP32 factors, column scales, correction / residual block, 2 * nrhs maxima
-  return N * N * 4 + 256 + N * 8 + 256 + nrhs * N * 8 + 256 + 256;
+  const int64_t nblk = (N + TS_B - 1) / TS_B;
+  // FP32 factors, column scales, correction / residual block, 2 * nrhs
+  // maxima, inverses of the diagonal blocks of both factors, sweep flags and
+  // the error word
+  return round256(N * N * 4) + round256(N * 8) + round256(nrhs * N * 8) + 256 +
+         2 * round256(nblk * TS_B * TS_B * 8) + round256(nblk * 4) + 256;
 }
 
 extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const double* F, double* X, int64_t nrhs,
@@ -308,18 +642,32 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   if (work_bytes < tb_solve_mixed_workspace(N, nrhs)) return BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   char* w = static_cast<char*>(work);
+  const int64_t nblk = (N + TS_B - 1) / TS_B;
   float* S = reinterpret_cast<float*>(w);
-  w += ((N * N * 4 + 255) / 256) * 256;
+  w += round256(N * N * 4);
   double* c = reinterpret_cast<double*>(w);
-  w += ((N * 8 + 255) / 256) * 256;
+  w += round256(N * 8);
   double* D = reinterpret_cast<double*>(w);
-  w += ((nrhs * N * 8 + 255) / 256) * 256;
+  w += round256(nrhs * N * 8);
   unsigned long long* maxes = reinterpret_cast<unsigned long long*>(w);
+  w += 256;
+  double* dinv_l = reinterpret_cast<double*>(w);
+  w += round256(nblk * TS_B * TS_B * 8);
+  double* dinv_u = reinterpret_cast<double*>(w);
+  w += round256(nblk * TS_B * TS_B * 8);
+  int* flags = reinterpret_cast<int*>(w);
+  w += round256(nblk * 4);
+  int* err = reinterpret_cast<int*>(w);
 
   k_col_maxabs<<<unsigned((N + 31) / 32), 256, 0, s>>>(A, lda, N, c);
   k_scale_to_f32<<<unsigned((N * N + 255) / 256), 256, 0, s>>>(A, lda, c, S, N);
-  int st = lu_nopiv<float>(S, N, N, s);
+  if (cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) return CUDA_ERR;
+  int st = lu_nopiv_f32_tc(S, N, N, err, s);
   if (st != OK) return st;
+  k_diag_inverse<true><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_l);
+  k_diag_inverse<false><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_u);
+  if (cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s) != cudaSuccess) return CUDA_ERR;
+  int epoch = 0;
   if (cudaMemsetAsync(X, 0, sizeof(double) * N * nrhs, s) != cudaSuccess) return CUDA_ERR;
   const int nr = int(nrhs);
   int it = 0;
@@ -327,18 +675,8 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   for (it = 1; it <= max_iter; it++) {
     // D = F - A X (FP64), then D <- (L U)^-1 D with the FP32 factors
     k_residual<<<unsigned((N * 32 + 255) / 256), 256, 0, s>>>(A, lda, X, F, D, N, nr);
-    for (int64_t b0 = 0; b0 < N; b0 += MX_NB) {
-      int nb = N - b0 < MX_NB ? int(N - b0) : MX_NB;
-      k_trsv_block_f32<true><<<1, 32, 0, s>>>(S, N, D, N, b0, nb, nr);
-      int64_t i0 = b0 + nb;
-      if (i0 < N) k_trsv_update_f32<<<unsigned((N - i0 + 127) / 128), 128, 0, s>>>(S, N, D, N, b0, nb, i0, N, nr);
-    }
-    for (int64_t b = (N + MX_NB - 1) / MX_NB - 1; b >= 0; b--) {
-      int64_t b0 = b * MX_NB;
-      int nb = N - b0 < MX_NB ? int(N - b0) : MX_NB;
-      k_trsv_block_f32<false><<<1, 32, 0, s>>>(S, N, D, N, b0, nb, nr);
-      if (b0 > 0) k_trsv_update_f32<<<unsigned((b0 + 127) / 128), 128, 0, s>>>(S, N, D, N, b0, nb, 0, b0, nr);
-    }
+    k_trsv_sweep<true><<<unsigned(nblk), 256, 0, s>>>(S, N, N, dinv_l, D, nr, flags, ++epoch, err);
+    k_trsv_sweep<false><<<unsigned(nblk), 256, 0, s>>>(S, N, N, dinv_u, D, nr, flags, ++epoch, err);
     if (cudaMemsetAsync(maxes, 0, sizeof(unsigned long long) * 2 * nr, s) != cudaSuccess) return CUDA_ERR;
     k_apply_correction<<<unsigned((N * nrhs + 255) / 256), 256, 0, s>>>(X, D, c, N, nr, maxes);
     unsigned long long bits[2 * MX_MAX_RHS];
@@ -368,6 +706,11 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   }
   if (iters_out) *iters_out = it > max_iter ? max_iter : it;
   if (last_rel_out) *last_rel_out = rel;
+  int err_h = 0;  // a bounded wait in the factorisation or a sweep ran out
+  if (cudaMemcpyAsync(&err_h, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return CUDA_ERR;
+  if (err_h) return TIMEOUT;
   if (st != OK) return st;
   if (rel > tol) return SINGULAR;  // did not converge: the caller falls back to the pivoted FP64 LU
   return launch_status();

@@ -38,7 +38,9 @@ struct MlpDomain {
 // with h = z / 2.  tanh.approx.f32 (one MUFU operation instead of the exp and
 // reciprocal of z / (1 + exp(-z))) has a maximum relative error of about
 // 2^-11, below the BF16 rounding of the activations that follows; training
-// and the tracer use the same function.
+// and both tracer engines use the same function.  (A paired FP16 variant,
+// tanh.approx.f16x2, halves the MUFU operations but its conversions made the
+// tracer slower.)
 __device__ __forceinline__ float tanh_fast(float x) {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -52,6 +54,8 @@ __device__ __forceinline__ float silu_grad(float z) {
   const float s = fmaf(0.5f, tanh_fast(0.5f * z), 0.5f);  // sigmoid(z)
   return s * fmaf(z, 1.f - s, 1.f);
 }
+// BF16 pair {silu(z0), silu(z1)} (z0 in the low half).
+__device__ __forceinline__ uint32_t silu2_bf16(float z0, float z1);
 
 // Input features of a point (r, z): polynomial terms in rho^2 and zeta (the
 // field is even in r) and five Fourier pairs in zeta, sin/cos(k pi zeta) for
@@ -91,6 +95,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<uint32_t*>(&v);
 }
+__device__ __forceinline__ uint32_t silu2_bf16(float z0, float z1) { return pack_bf16(silu(z0), silu(z1)); }
 
 // Shared-memory image of the network for the warp-level forward pass.
 constexpr int MLP_LD_IN = MLP_IN + 8;  // padded row strides (bf16 elements)
@@ -156,10 +161,10 @@ __device__ __forceinline__ void mlp_hidden_layer(const __nv_bfloat16 (*W)[MLP_LD
       c1[c] += d1[c];
     }
     int col0 = 16 * kb + 2 * q, col1 = 16 * kb + 8 + 2 * q;
-    out[kb][0] = pack_bf16(silu(c0[0] + bias[col0]), silu(c0[1] + bias[col0 + 1]));
-    out[kb][1] = pack_bf16(silu(c0[2] + bias[col0]), silu(c0[3] + bias[col0 + 1]));
-    out[kb][2] = pack_bf16(silu(c1[0] + bias[col1]), silu(c1[1] + bias[col1 + 1]));
-    out[kb][3] = pack_bf16(silu(c1[2] + bias[col1]), silu(c1[3] + bias[col1 + 1]));
+    out[kb][0] = silu2_bf16(c0[0] + bias[col0], c0[1] + bias[col0 + 1]);
+    out[kb][1] = silu2_bf16(c0[2] + bias[col0], c0[3] + bias[col0 + 1]);
+    out[kb][2] = silu2_bf16(c1[0] + bias[col1], c1[1] + bias[col1 + 1]);
+    out[kb][3] = silu2_bf16(c1[2] + bias[col1], c1[3] + bias[col1 + 1]);
   }
 }
 
@@ -193,10 +198,10 @@ __device__ inline void mlp_warp_forward(const MlpSmem& s, const __nv_bfloat16 (*
       mma_bf16_16816(c0, a1, b0);
       mma_bf16_16816(c1, a1, b1);
       int col0 = 16 * kb + 2 * q, col1 = 16 * kb + 8 + 2 * q;
-      h[kb][0] = pack_bf16(silu(c0[0] + s.b1[col0]), silu(c0[1] + s.b1[col0 + 1]));
-      h[kb][1] = pack_bf16(silu(c0[2] + s.b1[col0]), silu(c0[3] + s.b1[col0 + 1]));
-      h[kb][2] = pack_bf16(silu(c1[0] + s.b1[col1]), silu(c1[1] + s.b1[col1 + 1]));
-      h[kb][3] = pack_bf16(silu(c1[2] + s.b1[col1]), silu(c1[3] + s.b1[col1 + 1]));
+      h[kb][0] = silu2_bf16(c0[0] + s.b1[col0], c0[1] + s.b1[col0 + 1]);
+      h[kb][1] = silu2_bf16(c0[2] + s.b1[col0], c0[3] + s.b1[col0 + 1]);
+      h[kb][2] = silu2_bf16(c1[0] + s.b1[col1], c1[1] + s.b1[col1 + 1]);
+      h[kb][3] = silu2_bf16(c1[2] + s.b1[col1], c1[3] + s.b1[col1 + 1]);
     }
     // the three hidden layers share one copy of the code (smaller kernel:
     // fewer instruction-fetch stalls)

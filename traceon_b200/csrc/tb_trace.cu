@@ -602,7 +602,9 @@ __device__ __forceinline__ bool near_segments(const double (*seg)[5], int nseg, 
 }
 
 // Exact BEM field of the electrostatic rings at one point, by one lane.
-__device__ void bem_point_field(const TraceParams& P, const double* p, double* E) {
+// Out of line: it is the rare path of the surrogate tracer, and inlined its
+// ring kernel's registers would count against the whole tracer.
+__device__ __noinline__ void bem_point_field(const TraceParams& P, const double* p, double* E) {
   double r0 = sqrt(p[0] * p[0] + p[1] * p[1]);
   double Sr = 0, Sz = 0, dummy = 0;
   const double* er = P.esrc;
@@ -680,7 +682,7 @@ __device__ void surrogate_field(const TraceParams& P, const SurrogateParams& S, 
 template <class Engine>
 __device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams& S, Engine& eng) {
   bool engine_failed = false;
-  double y[6], ks[6][6];
+  double y[6];
   double t = 0, h = 0, hmax = 0, qm = 0;
   int64_t accepted = 0, attempts = 0, fallbacks = 0;
   int status = TRACE_EXITED;
@@ -729,14 +731,26 @@ __device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams
       go = active && in_bounds(P.bounds, y) && attempts < P.max_attempts;
     }
     if (go) attempts++;
+    // Stage sums kept as running accumulators with static indices (no
+    // dynamically indexed array, so nothing goes to local memory):
+    // off[i] = sum_j B[i+1][j] k_j (input of stage i + 1), k5 = sum_j CH[j] k_j
+    // (fifth-order increment), ke = sum_j CT[j] k_j (error estimate).
+    double off[5][6], k5[6], ke[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      k5[c] = ke[c] = 0.0;
+#pragma unroll
+      for (int i = 0; i < 5; i++) off[i][c] = 0.0;
+    }
 #pragma unroll 1
     for (int s = 0; s < 6; s++) {
       double ys[6];
 #pragma unroll
       for (int c = 0; c < 6; c++) {
-        double v = y[c];
-        for (int j = 0; j < s; j++) v += RK_B[s][j] * ks[j][c];
-        ys[c] = v;
+        double o = 0.0;
+#pragma unroll
+        for (int i = 0; i < 5; i++) o = (s == i + 1) ? off[i][c] : o;
+        ys[c] = y[c] + o;
       }
       if (!go) {
         ys[0] = 0.5 * S.dom.r_max;
@@ -751,12 +765,21 @@ __device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams
       }
       if (go) {
         fallbacks += used_bem ? 1 : 0;
-        ks[s][0] = h * ys[3];
-        ks[s][1] = h * ys[4];
-        ks[s][2] = h * ys[5];
-        ks[s][3] = h * qm * E[0];
-        ks[s][4] = h * qm * E[1];
-        ks[s][5] = h * qm * E[2];
+        const double k[6] = {h * ys[3], h * ys[4], h * ys[5], h * qm * E[0], h * qm * E[1], h * qm * E[2]};
+        const double ch = RK_CH[s], ct = RK_CT[s];
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+          k5[c] = fma(ch, k[c], k5[c]);
+          ke[c] = fma(ct, k[c], ke[c]);
+        }
+        if (s < 5) {
+#pragma unroll
+          for (int i = 0; i < 5; i++) {
+            const double b = RK_B[i + 1][s];  // zero for s >= i + 1
+#pragma unroll
+            for (int c = 0; c < 6; c++) off[i][c] = fma(b, k[c], off[i][c]);
+          }
+        }
       }
     }
     if (engine_failed) {
@@ -781,13 +804,8 @@ __device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams
     double ep = 0.0, ev = 0.0;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      double a = 0.0, b = 0.0;
-      for (int j = 0; j < 6; j++) {
-        a += RK_CT[j] * ks[j][c];
-        b += RK_CT[j] * ks[j][c + 3];
-      }
-      ep = fmax(ep, fabs(a));
-      ev = fmax(ev, fabs(b));
+      ep = fmax(ep, fabs(ke[c]));
+      ev = fmax(ev, fabs(ke[c + 3]));
     }
     double err = ep + h * ev;
     if (!(err == err)) {
@@ -799,9 +817,7 @@ __device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams
     if (err <= P.atol) {
       double yn[6];
 #pragma unroll
-      for (int c = 0; c < 6; c++)
-        yn[c] = y[c] + (RK_CH[0] * ks[0][c] + RK_CH[1] * ks[1][c] + RK_CH[2] * ks[2][c] + RK_CH[3] * ks[3][c] +
-                        RK_CH[4] * ks[4][c] + RK_CH[5] * ks[5][c]);
+      for (int c = 0; c < 6; c++) yn[c] = y[c] + k5[c];
       if (P.record_plane && ((y[2] - P.plane_z > 0) != (yn[2] - P.plane_z > 0))) {
         double cr[7];
         hermite_crossing(h, y, yn, P.plane_z, t, cr);
@@ -893,7 +909,10 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
 // the next layer's BF16 activations into the same tile.  The weights are
 // staged once per CTA; one CTA per SM (shared memory ~218 KB).
 // ============================================================================
-constexpr int TC_GROUPS = 3;
+#ifndef TB_TC_GROUPS
+#define TB_TC_GROUPS 3
+#endif
+constexpr int TC_GROUPS = TB_TC_GROUPS;
 constexpr int TC_THREADS = 128 * TC_GROUPS;
 constexpr uint32_t TC_TMEM_COLS = 512;              // 3 x 128 used
 constexpr long long TC_WAIT_CYCLES = 2000000000LL;  // ~1 s; an MMA chain takes microseconds
@@ -1001,21 +1020,19 @@ struct TcEngine {
       if (layer < 4) {
         const float* bias = layer == 0 ? s.b1 : s.bh[layer - 1];
 #pragma unroll 1
-        for (int c = 0; c < 4; c++) {  // columns 32c .. 32c + 31
-          uint32_t v[32];
-          tc::tmem_ld32(tld + 32 * c, v);
+        for (int c = 0; c < 8; c++) {  // columns 16c .. 16c + 15
+          uint32_t v[16];
+          tc::tmem_ld16(tld + 16 * c, v);
           tc::tmem_wait_ld();
-          uint32_t q[16];
+          uint32_t q[8];
 #pragma unroll
-          for (int j = 0; j < 16; j++)
-            q[j] = pack_bf16(silu(__uint_as_float(v[2 * j]) + bias[32 * c + 2 * j]),
-                             silu(__uint_as_float(v[2 * j + 1]) + bias[32 * c + 2 * j + 1]));
-          // next layer's K = 32c .. 32c + 31: atom c / 2, chunks 4 (c % 2) .. + 3
-          const uint32_t base = act + (c >> 1) * TC_ATOM;
-#pragma unroll
-          for (int j = 0; j < 4; j++)
-            tc::st_shared_v4(base + tc::sw128(row, 4 * (c & 1) + j), q[4 * j], q[4 * j + 1], q[4 * j + 2],
-                             q[4 * j + 3]);
+          for (int j = 0; j < 8; j++)
+            q[j] = silu2_bf16(__uint_as_float(v[2 * j]) + bias[16 * c + 2 * j],
+                              __uint_as_float(v[2 * j + 1]) + bias[16 * c + 2 * j + 1]);
+          // next layer's K = 16c .. 16c + 15: atom c / 4, chunks 2 (c % 4), 2 (c % 4) + 1
+          const uint32_t base = act + (c >> 2) * TC_ATOM;
+          tc::st_shared_v4(base + tc::sw128(row, 2 * (c & 3)), q[0], q[1], q[2], q[3]);
+          tc::st_shared_v4(base + tc::sw128(row, 2 * (c & 3) + 1), q[4], q[5], q[6], q[7]);
         }
       } else {
         uint32_t v[16];
