@@ -15,6 +15,10 @@ crossing of the exit plane z = +9.5 mm.  Synthetic inputs; no dataset.
       on a 16,384-electron slice of the same beam (`plain_bem`).
   --field bem: the plain FP64 BEM field only.
   --impl reference: the reference C backend's plain BEM tracer on host cores.
+  --workload solve: only the precision workload's solve (the lens at
+      --precision-n elements, 8 right-hand sides): GPU FP64 fill, FP64
+      pivoted LU and the mixed tensor-core solve (also reported, as
+      `precision_solve`, beside the tracer in the default run).
 
 `value` is whole-job electrons/s with the start states resident in HBM;
 `e2e` is the same through the public API with host arrays, host<->device
@@ -49,7 +53,7 @@ def workload_config(electrons, field):
     return {'workload': f'einzel lens, {N_ELEMENTS} cubic elements, {desc}, {electrons} electrons/step at '
                         f'1 keV +-5%, +-20 mrad, r0<=0.2 mm, RKF45 atol=1e-10 m, exit plane z=+9.5 mm',
             'elements': N_ELEMENTS, 'electrons_per_step': electrons, 'atol_m': ATOL, 'seed': SEED,
-            'field': field, 'l2': 'L2 flushed (256 MiB write) between timed steps'}
+            'field': field, 'l2': 'L2 flushed (256 MiB write, inside the step time) before every timed step'}
 
 
 def dist_info():
@@ -199,9 +203,11 @@ def run_reference(args):
     for _ in range(args.warmup):
         cpu_reference_rate(geo, q, jac, pos, p0, v0, cores, 2.0)
     rates, n_total, t_total = [], 0, 0.0
+    # each step a bounded sample: about two minutes of CPU work in total
+    step_s = min(args.ref_seconds, max(2.0, 120.0 / max(args.steps, 1)))
     for s in range(args.steps):
         sl = slice((s * cores * 4) % len(p0), None)
-        r, n, kind = cpu_reference_rate(geo, q, jac, pos, p0[sl], v0[sl], cores, args.ref_seconds)
+        r, n, kind = cpu_reference_rate(geo, q, jac, pos, p0[sl], v0[sl], cores, step_s)
         rates.append(r)
         n_total += n
         t_total += n / r if r else 0
@@ -213,7 +219,7 @@ def run_reference(args):
             'reference_field': 'plain BEM (the reference has no learned surrogate)',
             'cpu_baseline': {'value': value, 'unit': 'electrons/s', 'cores': cores,
                              'kind': 'reference' if kind == 'ref' else 'port',
-                             'sample': f'{n_total} electrons over {args.steps} steps of ~{args.ref_seconds:.0f} s '
+                             'sample': f'{n_total} electrons over {args.steps} steps of ~{step_s:.0f} s '
                                        f'(reference C backend trace_particle + field_radial_traceable, '
                                        f'{cores} threads)'},
             'e2e': {'value': value, 'unit': 'electrons/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
@@ -221,7 +227,7 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- precision solve
-def precision_solve(n, nrhs=8, seed=2):
+def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True):
     """The precision workload's charge solve: the three-electrode lens meshed
     to n cubic elements, nrhs right-hand sides with every electrode voltage
     ~U[-3, 3] kV.  GPU FP64 fill (+ singular self terms), then (a) the FP64
@@ -262,19 +268,63 @@ def precision_solve(n, nrhs=8, seed=2):
         _, perm = B.dev_lu_factor(LU)
         return B.dev_lu_solve(LU, perm, F)
 
-    lu64()
-    lu_ms, X64 = timed(lu64)
     B.dev_solve_mixed(A, F)
     mixed_ms, (Xm, iters, rel) = timed(lambda: B.dev_solve_mixed(A, F))
-    err = float(((Xm - X64).abs().amax(1) / X64.abs().amax(1)).max())
+    if fp64_lu:
+        lu64()
+        lu_ms, X64 = timed(lu64)
+        err = float(((Xm - X64).abs().amax(1) / X64.abs().amax(1)).max())
+    else:  # profiling the mixed solve alone
+        lu_ms, err = None, None
     out = {'workload': f'einzel lens, {n} cubic elements, {nrhs} right-hand sides (electrode voltages U[-3,3] kV)',
            'fill_fp64_ms': fill_ms, 'solve_fp64_lu_ms': lu_ms, 'solve_mixed_ms': mixed_ms,
            'mixed_iterations': iters, 'mixed_last_correction': rel, 'charges_rel_err_vs_fp64': err,
-           'speedup_solve': lu_ms / mixed_ms, 'speedup_fill_plus_solve': (fill_ms + lu_ms) / (fill_ms + mixed_ms),
+           'speedup_solve': lu_ms / mixed_ms if lu_ms else None,
+           'speedup_fill_plus_solve': (fill_ms + lu_ms) / (fill_ms + mixed_ms) if lu_ms else None,
            'lu_flop': 2.0 / 3.0 * n ** 3}
     del A
     torch.cuda.empty_cache()
+    if field_points:
+        out.update(precision_fields(geo, Xm[0], field_points, seed))
     return out
+
+
+def precision_fields(geo, charges_t, m, seed, check=64):
+    """Potential and field of the first right-hand side's charges at m points
+    (x = r ~ U[0, 0.9] mm, y = 0, z ~ U[-8, 8] mm), FP64 ring sums on the GPU;
+    `check` of them re-evaluated by the CPU oracle (its own element
+    quadrature and the same charges) as the judge."""
+    import torch
+    from traceon_b200 import backend as B
+    from oracle.oracle import Oracle
+    rng = np.random.default_rng(seed + 1)
+    pts = np.zeros((m, 3))
+    pts[:, 0] = rng.uniform(0.0, 0.9e-3, m)
+    pts[:, 2] = rng.uniform(-8e-3, 8e-3, m)
+    pts_t = B.to_dev(pts, torch.float64)
+    v = B.to_dev(geo.vertices, torch.float64)
+    jac, pos = B.dev_jacobian_buffer(v)
+    src = B.dev_pack_sources(charges_t.contiguous(), jac, pos)
+    B.dev_field_points(pts_t[:1024], src)  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    pot, fld = B.dev_field_points(pts_t, src)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    sample = rng.choice(m, check, replace=False)
+    port = Oracle('port')
+    q = charges_t.cpu().numpy()
+    jac_o, pos_o = port.fill_jacobian_buffer_radial(geo.vertices)
+    f_or = port.field_radial_many(pts[sample], q, jac_o, pos_o)
+    p_or = port.potential_radial_many(pts[sample], q, jac_o, pos_o)
+    f_gpu, p_gpu = fld.cpu().numpy()[sample], pot.cpu().numpy()[sample]
+    ferr = float(np.max(np.abs(f_gpu - f_or)) / np.max(np.abs(f_or)))
+    perr = float(np.max(np.abs(p_gpu - p_or)) / np.max(np.abs(p_or)))
+    pairs = m * src.shape[1]
+    return {'field_points': m, 'field_ms': ms, 'field_ring_pairs_per_s': pairs / (ms * 1e-3),
+            'field_rel_err_vs_oracle': ferr, 'potential_rel_err_vs_oracle': perr, 'field_checked_points': check}
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -309,20 +359,24 @@ MLP_FLOP_PER_EVAL = 2 * (16 * 128 + 3 * 128 * 128 + 128 * 16)  # dense BF16 flop
 
 
 def time_steps(fn, steps, flush):
-    """CUDA-event time of `steps` calls of fn (L2 flushed before each)."""
+    """Device time of `steps` calls of fn, enqueued back to back between CUDA
+    events on the launching stream (the host runs ahead of the GPU, so a host
+    pause -- garbage collection, the OS -- does not enter the measurement).
+    L2 is flushed (a 256 MiB write, ~0.04 ms) before every step; that write
+    is inside the step's time."""
     import torch
-    ms, results = [], []
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    results = []
+    torch.cuda.synchronize()
     torch.cuda.nvtx.range_push('timed_steps')  # lets a profiler select the timed launches
-    for _ in range(steps):
+    ev[0].record()
+    for i in range(steps):
         flush.fill_(1.0)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        r = fn()
-        e1.record()
-        torch.cuda.synchronize()
-        ms.append(e0.elapsed_time(e1))
-        results.append(r)
+        results.append(fn())
+        ev[i + 1].record()
+    torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
+    ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
     return ms, results
 
 
@@ -373,8 +427,15 @@ def run_gpu(args):
         return bem_tracer.trace_device(st, q, atol=ATOL, plane_z=G.LENS_EXIT_Z, team_warps=args.team_warps,
                                        max_attempts=20000)
 
+    sess = None
+    if sur is not None:
+        # the public batched API: static buffers, the step captured as a CUDA graph
+        sess = sur.trace_session(E, G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=ATOL, max_attempts=20000)
+        sess.start.copy_(start)  # start states resident in HBM for `value`
+
     def step_sur():
-        return sur.trace_device(start, qm, G.LENS_BOUNDS, ATOL, plane_z=G.LENS_EXIT_Z, max_attempts=20000)
+        sess.replay_device()
+        return sess
 
     step = step_sur if sur is not None else step_bem
     for _ in range(args.warmup):
@@ -391,29 +452,38 @@ def run_gpu(args):
         from traceon_b200.parallel import max_over_ranks
         total_ms = max_over_ranks(total_ms, device='cuda')
     res = results[-1]
-    attempts = [int(r.counters[:, 1].sum().item()) for r in results]
     status = res.status.cpu().numpy()
     plane = res.plane.cpu().numpy()
     counters = res.counters.cpu().numpy()
+    attempts = [int(counters[:, 1].sum())] * args.steps if sess is not None else \
+        [int(r.counters[:, 1].sum().item()) for r in results]
     value = ws * E * args.steps / (total_ms * 1e-3)
 
-    # ---- e2e through the public API with host arrays
+    # ---- e2e through the public API with host arrays: every step copies the
+    # start states in (pinned staging, H2D) and the endpoints out (D2H)
     e2e_ms = []
-    for _ in range(max(1, min(args.steps, 3))):
+    for _ in range(max(1, min(args.steps, 5))):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        if sur is not None:
-            sur.trace_endpoints(p0, v0, G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=ATOL, max_attempts=20000)
+        if sess is not None:
+            sess.run(p0, v0)
         else:
             bem_tracer.trace_endpoints(p0, v0, G.LENS_EXIT_Z, atol=ATOL, team_warps=args.team_warps,
                                        max_attempts=20000)
         torch.cuda.synchronize()
         e2e_ms.append((time.perf_counter() - t1) * 1e3)
-    e2e_value = ws * E / (np.mean(e2e_ms) * 1e-3)
-    ncnt = 3 if sur is not None else 2
-    h2d = E * 6 * 8 + E * 8
-    d2h = E * (7 + 7) * 8 + E * 4 + E * ncnt * 8
+    e2e_value = ws * E / (np.median(e2e_ms) * 1e-3)
+    if sess is not None:
+        h2d, d2h = sess.h2d_bytes, sess.d2h_bytes
+        e2e_api = 'FieldSurrogate.trace_session(...).run(positions, velocities): pinned staging, one CUDA-graph replay'
+    else:
+        h2d, d2h = E * 6 * 8 + E * 8, E * (7 + 7) * 8 + E * 4 + E * 2 * 8
+        e2e_api = 'Tracer.trace_endpoints(positions, velocities, ...)'
+    if sess is not None:  # the session's pinned outputs against the device-resident run
+        pl_h = sess.plane_h.numpy()
+        assert np.array_equal(np.nan_to_num(pl_h), np.nan_to_num(plane)), 'session outputs differ from the device run'
+
 
     # ---- plain BEM tracer on a slice of the same beam (for the comparison)
     plain = None
@@ -483,10 +553,14 @@ def run_gpu(args):
                          f'for ~{args.cpu_seconds:.0f} s'}
 
     line = {'metric': METRIC, 'value': value, 'unit': 'electrons/s', 'n_gpus': ws, 'steps': args.steps,
-            'warmup': args.warmup, 'ms_per_step': total_ms / args.steps, 'higher_is_better': True,
+            'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
+            'step_ms': {'min': float(np.min(ms_list)), 'median': float(np.median(ms_list)),
+                        'max': float(np.max(ms_list))},
+            'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'bf16+f64' if sur is not None else 'f64',
             'data': 'synthetic', 'config': workload_config(E, args.field),
-            'e2e': {'value': e2e_value, 'unit': 'electrons/s', 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
+            'e2e': {'value': e2e_value, 'unit': 'electrons/s', 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
+                    'api': e2e_api},
             'gpu_launches': args.steps, 'roofline': roof, 'plain_bem': plain,
             'speedup_vs_plain_bem': (value / plain['value']) if plain else None,
             'cpu_baseline': cpu, 'clocks': clk.summary(),
@@ -505,12 +579,27 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+def run_solve(args):
+    """--workload solve: only the precision workload's fill and solves (one
+    JSON line; used for the solver's profiles)."""
+    import torch
+    torch.cuda.set_device(dist_info()[2])
+    p = precision_solve(args.precision_n, fp64_lu=not args.skip_fp64_lu)
+    line = {'metric': 'mixed-precision charge solve time (precision workload)', 'value': p['solve_mixed_ms'],
+            'unit': 'ms', 'higher_is_better': False, 'n_gpus': 1, 'dtype': 'f32 tensor-core LU + f64 refinement',
+            'data': 'synthetic', 'config': {'workload': p['workload'], 'elements': args.precision_n},
+            'precision_solve': p}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='tracer', choices=['tracer', 'solve'],
+                    help='tracer: the headline metric (default); solve: only the precision-workload solve')
     ap.add_argument('--electrons', type=int, default=262144)
     ap.add_argument('--field', default='surrogate', choices=['surrogate', 'bem'])
     ap.add_argument('--bem-electrons', type=int, default=16384, help='slice traced with the plain BEM field')
@@ -521,6 +610,8 @@ def main():
                     help='surrogate network engine: tcgen05 (tc) or warp-level mma.sync (warp)')
     ap.add_argument('--check', type=int, default=16, help='electrons checked against the CPU oracle')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
+    ap.add_argument('--skip-fp64-lu', action='store_true',
+                    help='--workload solve: time only the mixed solve (for profiles)')
     ap.add_argument('--precision-n', type=int, default=16384,
                     help='elements of the precision-workload solve measured beside the tracer (0: skip)')
     ap.add_argument('--ref-seconds', type=float, default=20.0)
@@ -531,6 +622,8 @@ def main():
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.workload == 'solve':
+        run_solve(args)
     else:
         run_gpu(args)
 

@@ -204,6 +204,37 @@ int tb_fill_matrix_radial(double *A, int64_t lda, const double *vertices, const 
                           const double *values, const double *jac, const double *pos, int64_t N, int64_t row0,
                           int64_t row1, int accumulate, int gauss_diagonal, tb_stream_t stream);
 
+/* One geometry of a batch (device pointers).  tile0 / elem0 are set by
+ * tb_batch_plan. */
+typedef struct {
+  const double *vertices;   /* (N, 4, 3) cubic line elements */
+  const uint8_t *types;     /* (N) excitation types */
+  const double *values;     /* (N) excitation values */
+  const double *jac;        /* (N, 16) from tb_jacobian_buffer_radial */
+  const double *pos;        /* (N, 16, 2) */
+  double *A;                /* (N, lda) the geometry's matrix */
+  int64_t lda;
+  int64_t N;
+  int64_t tile0;            /* first global fill tile (set by tb_batch_plan) */
+  int64_t elem0;            /* first global element (set by tb_batch_plan) */
+} tb_geometry_t;
+
+/* Host helper: numbers the fill tiles and elements of n_geoms geometries
+ * (host array; sets tile0 / elem0) and returns the total number of tiles
+ * (-1 on bad sizes); *total_elements receives the sum of N.  Copy the array
+ * to device memory for the two calls below. */
+int64_t tb_batch_plan(tb_geometry_t *geoms, int n_geoms, int64_t *total_elements);
+
+/* fill_matrix_radial (radial.c:249-310, off-diagonal entries) of many
+ * geometries of uneven N in one persistent launch; geoms is a DEVICE array
+ * prepared by tb_batch_plan.  No counterpart in the reference (its Python
+ * solver fills one geometry at a time, solver.py:204-232). */
+int tb_fill_matrix_radial_batched(const tb_geometry_t *geoms, int n_geoms, int64_t total_tiles, tb_stream_t stream);
+
+/* The singular self terms (as tb_self_integrals) of every element of a batch,
+ * stored on each geometry's matrix diagonal; one launch. */
+int tb_self_integrals_batched(const tb_geometry_t *geoms, int n_geoms, int64_t total_elements, tb_stream_t stream);
+
 /* Singular self terms: diag[i] = integral over alpha in [-1, 1] of the
  * self integrand of element i (self_potential_radial, radial.c:182-196, for
  * voltage rows; self_field_dot_normal_radial - 1, radial.c:203-222 and

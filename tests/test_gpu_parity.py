@@ -370,3 +370,31 @@ def test_solver_api_end_to_end(cuda, g96):
     assert np.max(np.abs(E - g96['E_points'])) / np.abs(g96['E_points']).max() < 1e-10
     assert np.allclose(field.field_at_point(g96['points'][0]), g96['E_points'][0], rtol=1e-10,
                        atol=1e-10 * np.abs(g96['E_points']).max())
+
+
+def test_autotuned_team_size(cuda, port):
+    """team_warps='tune': the measured choice (one of 1, 2, 4, 8) is cached per
+    device and problem size, and the traces it gives match the oracle."""
+    from traceon_b200 import autotune
+    from traceon_b200.field import EffectivePointCharges, FieldRadialBEM
+    from traceon_b200.tracing import Tracer
+    from traceon_b200 import geometry as G
+    from oracle.oracle import EM, hermite_plane_crossing
+    autotune.clear()
+    q, jac, pos = _geometry_field(cuda, port)
+    field = FieldRadialBEM(EffectivePointCharges(q, jac, pos))
+    p0, v0 = G.electron_beam(40, 5)
+    tr = Tracer(field, G.LENS_BOUNDS)
+    plane, _, status, _ = tr.trace_endpoints(p0, v0, G.LENS_EXIT_Z, atol=1e-10, team_warps='tune')
+    assert np.all(status == cuda.TRACE_EXITED)
+    tab = autotune.table()
+    keys = [k for k in tab if k[0] == 'bem_team_warps' and len(k) == 4]
+    assert len(keys) == 1 and tab[keys[0]] in autotune.TEAM_CANDIDATES
+    timings = tab[keys[0] + ('times_ms',)]
+    assert set(timings) == set(autotune.TEAM_CANDIDATES)
+    tr.trace_endpoints(p0, v0, G.LENS_EXIT_Z, atol=1e-10, team_warps='tune')  # served from the table
+    assert autotune.table() == tab
+    for i in range(0, 40, 13):
+        t, s = port.trace_bem(p0[i], v0[i], EM, q, jac, pos, G.LENS_BOUNDS, 1e-10)
+        h = hermite_plane_crossing(t, s, G.LENS_EXIT_Z)
+        assert np.max(np.abs(plane[i, 1:4] - h[:3])) < 1e-12

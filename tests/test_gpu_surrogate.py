@@ -213,3 +213,21 @@ def test_tc_engine_traces_vs_bem_oracle(cuda, port, trained):
     assert d < 1e-10
     err, _ = _endpoint_errors(port, fs_t, p0[:12], v0[:12])
     assert err.max() < 1e-9
+
+
+def test_trace_session_graph_replays(cuda, trained):
+    """TraceSession: pinned staging + the whole step captured as a CUDA graph.
+    Two batches through one session give exactly the endpoints of the eager
+    public call on the same inputs (each particle's path depends only on its
+    own state), and the buffers are reused between runs."""
+    from traceon_b200 import geometry as G
+    fs, _ = _fields(trained, np.array([0.0, 1500.0, 0.0]))
+    n = 700
+    sess = fs.trace_session(n, G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=1e-10)
+    for seed in (31, 32):
+        p0, v0 = G.surrogate_beam(n, seed)
+        plane, final, status, counters = fs.trace_endpoints(p0, v0, G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=1e-10)
+        sp, sf, ss, sc = (a.copy() for a in sess.run(p0, v0))
+        assert (ss == 0).all() and np.array_equal(ss, status)
+        assert np.array_equal(sp, plane) and np.array_equal(sf, final) and np.array_equal(sc, counters)
+    assert sess.h2d_bytes == n * 48 and sess.d2h_bytes == n * (112 + 4 + 24)

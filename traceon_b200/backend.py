@@ -139,6 +139,12 @@ class TbField(C.Structure):
                 ("axial_elec", vp), ("axial_mag", vp), ("axial_nz", i64)]
 
 
+class TbGeometry(C.Structure):
+    """tb_geometry_t of include/traceon_b200.h"""
+    _fields_ = [("vertices", vp), ("types", vp), ("values", vp), ("jac", vp), ("pos", vp), ("A", vp),
+                ("lda", i64), ("N", i64), ("tile0", i64), ("elem0", i64)]
+
+
 class TbTraceOpts(C.Structure):
     """tb_trace_opts_t of include/traceon_b200.h"""
     _fields_ = [("bounds", dbl * 6), ("atol", dbl), ("plane_z", dbl), ("record_plane", C.c_int),
@@ -215,6 +221,8 @@ _DEV = {
     'tb_lu_nopiv_f64': (vp, i64, i64, vp),
     'tb_lu_nopiv_f32': (vp, i64, i64, vp),
     'tb_lu_nopiv_f32_tc': (vp, i64, i64, vp, vp),
+    'tb_fill_matrix_radial_batched': (vp, C.c_int, i64, vp),
+    'tb_self_integrals_batched': (vp, C.c_int, i64, vp),
     'tb_gemm_sub_tf32x3': (vp, i64, vp, i64, vp, i64, i64, i64, i64, vp, vp),
     'tb_solve_mixed': (vp, i64, i64, vp, vp, i64, vp, i64, C.c_int, dbl, C.POINTER(C.c_int), C.POINTER(dbl), vp),
 }
@@ -574,6 +582,31 @@ def dev_self_integrals(vertices_t, types_t, values_t, A=None):
     _call('tb_self_integrals', _ptr(vertices_t), _ptr(types_t), _ptr(values_t), _ptr(diag), _ptr(A),
           A.stride(0) if A is not None else N, N, _stream())
     return diag
+
+
+backend_lib.tb_batch_plan.restype = i64
+backend_lib.tb_batch_plan.argtypes = [vp, C.c_int, C.POINTER(i64)]
+
+
+def dev_fill_batched(items):
+    """Fills the matrices of many geometries (off-diagonal entries in one
+    persistent launch, self terms in one more).  items: list of (vertices,
+    types, values, jac, pos, A) device tensors, A (N, N) FP64."""
+    torch = _torch()
+    n = len(items)
+    if n == 0:
+        return
+    arr = (TbGeometry * n)()
+    for k, (v, t, val, jac, pos, A) in enumerate(items):
+        arr[k] = TbGeometry(v.data_ptr(), t.data_ptr(), val.data_ptr(), jac.data_ptr(), pos.data_ptr(), A.data_ptr(),
+                            A.stride(0), v.shape[0], 0, 0)
+    total = i64(0)
+    tiles = backend_lib.tb_batch_plan(arr, n, C.byref(total))
+    if tiles < 0:
+        raise BackendError('tb_batch_plan: bad geometry sizes')
+    dev = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).to(items[0][0].device)
+    _call('tb_fill_matrix_radial_batched', _ptr(dev), n, tiles, _stream())
+    _call('tb_self_integrals_batched', _ptr(dev), n, total.value, _stream())
 
 
 def dev_self_integrals_np(vertices, types, values):

@@ -57,6 +57,33 @@ __global__ void k_element_targets(const double* __restrict__ vertices, double* _
 constexpr int FILL_COLS = 32;
 constexpr int FILL_ROWS = 8;
 
+// Entry (i, j) of the matrix (radial.c:249-310): the collocation point of
+// element i against the 16 Gauss rings of element j (staged in r[], z[], w[]),
+// by the row's excitation type.
+__device__ __forceinline__ double fill_entry(const double* __restrict__ vertices, const uint8_t* __restrict__ types,
+                                             const double* __restrict__ values, int64_t i, const double* r,
+                                             const double* z, const double* w) {
+  Cubic cu;
+  cu.load(vertices + i * 12);
+  double tr, tz, tj;
+  cu.point(0.0, false, tr, tz, tj);
+  const int ty_ = types[i];
+  double acc = 0.0;
+  if (ty_ == VOLTAGE_FIXED || ty_ == VOLTAGE_FUN || ty_ == MAGNETOSTATIC_POT) {
+#pragma unroll 4
+    for (int k = 0; k < NQ; k++) acc += w[k] * (ring_pot_nopi(tr, tz, r[k], z[k]) * INV_PI);
+  } else if (ty_ == DIELECTRIC || ty_ == MAGNETIZABLE) {
+    double nr, nz;
+    cu.normal(0.0, nr, nz);
+    double f = flux_factor(values[i]);
+#pragma unroll 4
+    for (int k = 0; k < NQ; k++) acc += w[k] * field_dot_normal_ring(tr, tz, r[k] - tr, z[k] - tz, nr, nz, f);
+  } else {
+    acc = __longlong_as_double(0x7ff8000000000000LL);  // unknown type: NaN
+  }
+  return acc;
+}
+
 __global__ void __launch_bounds__(FILL_COLS* FILL_ROWS)
     k_fill_matrix(double* __restrict__ A, int64_t lda, const double* __restrict__ vertices,
                   const uint8_t* __restrict__ types, const double* __restrict__ values,
@@ -84,27 +111,54 @@ __global__ void __launch_bounds__(FILL_COLS* FILL_ROWS)
   const int64_t j = j0 + tx;
   if (i >= row1 || j >= N) return;
   if (j == i && !gauss_diagonal) return;
-  Cubic cu;
-  cu.load(vertices + i * 12);
-  double tr, tz, tj;
-  cu.point(0.0, false, tr, tz, tj);
-  const int ty_ = types[i];
-  double acc = 0.0;
-  if (ty_ == VOLTAGE_FIXED || ty_ == VOLTAGE_FUN || ty_ == MAGNETOSTATIC_POT) {
-#pragma unroll 4
-    for (int k = 0; k < NQ; k++) acc += s_w[tx][k] * (ring_pot_nopi(tr, tz, s_r[tx][k], s_z[tx][k]) * INV_PI);
-  } else if (ty_ == DIELECTRIC || ty_ == MAGNETIZABLE) {
-    double nr, nz;
-    cu.normal(0.0, nr, nz);
-    double f = flux_factor(values[i]);
-#pragma unroll 4
-    for (int k = 0; k < NQ; k++)
-      acc += s_w[tx][k] * field_dot_normal_ring(tr, tz, s_r[tx][k] - tr, s_z[tx][k] - tz, nr, nz, f);
-  } else {
-    acc = __longlong_as_double(0x7ff8000000000000LL);  // unknown type: NaN
-  }
+  const double acc = fill_entry(vertices, types, values, i, s_r[tx], s_z[tx], s_w[tx]);
   double* a = A + (i * lda + j);
   *a = accumulate ? *a + acc : acc;
+}
+
+// ---------------------------------------------------------------- batched fill
+// Many geometries of uneven N in one persistent launch: the tiles (32 columns
+// x 8 rows) of all matrices are numbered globally (geometry g owns tiles
+// [tile0[g], tile0[g] + tiles_x[g] tiles_y[g])); CTAs stride over them and
+// find their geometry by binary search.  Diagonal entries are left to the
+// self integrals, as in the single-geometry fill.
+__global__ void __launch_bounds__(FILL_COLS* FILL_ROWS)
+    k_fill_matrix_batched(const tb_geometry_t* __restrict__ geoms, int n_geoms, int64_t total_tiles) {
+  __shared__ double s_r[FILL_COLS][NQ + 1], s_z[FILL_COLS][NQ + 1], s_w[FILL_COLS][NQ + 1];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * FILL_COLS + tx;
+  for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    int lo = 0, hi = n_geoms - 1;  // last geometry with tile0 <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (geoms[mid].tile0 <= t)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const tb_geometry_t& g = geoms[lo];
+    const int64_t N = g.N;
+    const int64_t tiles_x = (N + FILL_COLS - 1) / FILL_COLS;
+    const int64_t local = t - g.tile0;
+    const int64_t j0 = (local % tiles_x) * FILL_COLS, i0 = (local / tiles_x) * FILL_ROWS;
+    __syncthreads();  // the previous tile's rings are no longer read
+    for (int e = tid; e < FILL_COLS * NQ; e += FILL_COLS * FILL_ROWS) {
+      const int c = e / NQ, k = e % NQ;
+      const int64_t j = j0 + c;
+      double r = 0, z = 0, w = 0;
+      if (j < N) {
+        r = g.pos[(j * NQ + k) * 2];
+        z = g.pos[(j * NQ + k) * 2 + 1];
+        w = g.jac[j * NQ + k];
+      }
+      s_r[c][k] = r;
+      s_z[c][k] = z;
+      s_w[c][k] = w;
+    }
+    __syncthreads();
+    const int64_t i = i0 + ty, j = j0 + tx;
+    if (i < N && j < N && i != j) g.A[i * g.lda + j] = fill_entry(g.vertices, g.types, g.values, i, s_r[tx], s_z[tx], s_w[tx]);
+  }
 }
 
 // ---------------------------------------------------------------- self terms
@@ -125,12 +179,47 @@ __device__ __forceinline__ double self_integrand(const Cubic& c, double tr, doub
 }
 
 // One warp per element.
+// Self term of element i by one warp (all lanes call it; lane 0 gets the value).
+__device__ double self_term_warp(const double* __restrict__ vertices, const uint8_t* __restrict__ types,
+                                 const double* __restrict__ values, int64_t i, int lane);
+
 __global__ void k_self_integrals(const double* __restrict__ vertices, const uint8_t* __restrict__ types,
                                  const double* __restrict__ values, double* __restrict__ diag,
                                  double* __restrict__ A, int64_t lda, int64_t N) {
   int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32;
   int lane = threadIdx.x & 31;
   if (i >= N) return;
+  const double v = self_term_warp(vertices, types, values, i, lane);
+  if (lane == 0) {
+    if (diag) diag[i] = v;
+    if (A) A[i * lda + i] = v;
+  }
+}
+
+// The self terms of all elements of many geometries (one warp per element,
+// grid-strided over the global element numbering), onto their matrices'
+// diagonals.
+__global__ void k_self_integrals_batched(const tb_geometry_t* __restrict__ geoms, int n_geoms, int64_t total) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * blockDim.x / 32;
+  for (int64_t e = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32; e < total; e += warps) {
+    int lo = 0, hi = n_geoms - 1;  // last geometry with elem0 <= e
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (geoms[mid].elem0 <= e)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const tb_geometry_t& g = geoms[lo];
+    const int64_t i = e - g.elem0;
+    const double v = self_term_warp(g.vertices, g.types, g.values, i, lane);
+    if (lane == 0) g.A[i * g.lda + i] = v;
+  }
+}
+
+__device__ double self_term_warp(const double* __restrict__ vertices, const uint8_t* __restrict__ types,
+                                 const double* __restrict__ values, int64_t i, int lane) {
   Cubic c;
   c.load(vertices + i * 12);
   double tr, tz, tj, nr, nz;
@@ -152,12 +241,9 @@ __global__ void k_self_integrals(const double* __restrict__ vertices, const uint
     acc += half * gauss_w(k) * self_integrand(c, tr, tz, nr, nz, flux, factor, a);
   }
   acc = warp_sum(acc);
-  if (lane == 0) {
-    double v = flux ? acc - 1.0 : acc;
-    if (!flux && !pot) v = __longlong_as_double(0x7ff8000000000000LL);  // unknown type: NaN
-    if (diag) diag[i] = v;
-    if (A) A[i * lda + i] = v;
-  }
+  double v = flux ? acc - 1.0 : acc;
+  if (!flux && !pot) v = __longlong_as_double(0x7ff8000000000000LL);  // unknown type: NaN
+  return v;
 }
 
 __global__ void k_rhs(const uint8_t* __restrict__ types, const double* __restrict__ values,
@@ -547,6 +633,41 @@ extern "C" int tb_self_integrals(const double* vertices, const uint8_t* types, c
   int64_t threads = N * 32;
   k_self_integrals<<<unsigned((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(vertices, types, values, diag,
                                                                                       A, lda, N);
+  return launch_status();
+}
+
+extern "C" int64_t tb_batch_plan(tb_geometry_t* geoms, int n_geoms, int64_t* total_elements) {
+  if (!geoms || n_geoms <= 0) return -1;
+  int64_t tiles = 0, elems = 0;
+  for (int g = 0; g < n_geoms; g++) {
+    const int64_t N = geoms[g].N;
+    if (N <= 0 || geoms[g].lda < N) return -1;
+    geoms[g].tile0 = tiles;
+    geoms[g].elem0 = elems;
+    tiles += ((N + FILL_COLS - 1) / FILL_COLS) * ((N + FILL_ROWS - 1) / FILL_ROWS);
+    elems += N;
+  }
+  if (total_elements) *total_elements = elems;
+  return tiles;
+}
+
+extern "C" int tb_fill_matrix_radial_batched(const tb_geometry_t* geoms, int n_geoms, int64_t total_tiles,
+                                             tb_stream_t stream) {
+  if (!geoms || n_geoms <= 0 || total_tiles <= 0) return BAD_ARG;
+  // persistent: a few CTAs per SM stride over all tiles of all geometries
+  int64_t blocks = (int64_t)num_sms() * 8;
+  if (blocks > total_tiles) blocks = total_tiles;
+  k_fill_matrix_batched<<<unsigned(blocks), dim3(FILL_COLS, FILL_ROWS), 0, (cudaStream_t)stream>>>(geoms, n_geoms,
+                                                                                                  total_tiles);
+  return launch_status();
+}
+
+extern "C" int tb_self_integrals_batched(const tb_geometry_t* geoms, int n_geoms, int64_t total_elements,
+                                         tb_stream_t stream) {
+  if (!geoms || n_geoms <= 0 || total_elements <= 0) return BAD_ARG;
+  int64_t blocks = (total_elements * 32 + 255) / 256;
+  if (blocks > (int64_t)num_sms() * 16) blocks = (int64_t)num_sms() * 16;
+  k_self_integrals_batched<<<unsigned(blocks), 256, 0, (cudaStream_t)stream>>>(geoms, n_geoms, total_elements);
   return launch_status();
 }
 

@@ -18,6 +18,7 @@
 //   k_trsm_right   L21 = A21 U11^-1   (one thread per row)
 //   k_trsm_left    U12 = L11^-1 A12   (one thread per column)
 //   k_gemm_update  A22 -= L21 U12     (register-tiled SIMT GEMM)
+#include <cstdint>
 #include <cstring>
 
 #include "tb_common.cuh"
@@ -146,6 +147,121 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------- FP32 panel kernels
+// Panel kernels of lu_nopiv_f32_tc (64-wide blocks).  Each thread keeps its
+// row (or column) of the block in registers and eliminates right-looking
+// with the pivots' reciprocals, fully unrolled: no divisions and no dynamic
+// register indexing in the loop.
+
+// D (the nb x nb diagonal block at (k0, k0)) <- its LU factors in place.
+// Thread t owns column j = t % 64 of rows t / 64 + 4 s (s = 0..15) in
+// registers; at step k the owners publish column k and row k to shared
+// memory (double-buffered by the parity of k: one barrier per step) and
+// every thread updates its elements.  Fully unrolled (k and s are constants
+// in every iteration).  Rows and columns beyond nb are the identity.
+__global__ void __launch_bounds__(256) k_diag_lu_f32(float* __restrict__ A, int64_t lda, int64_t k0, int nb) {
+  __shared__ float colk[2][MX_NB], rowk[2][MX_NB];
+  const int j = threadIdx.x % MX_NB, i0 = threadIdx.x / MX_NB;
+  float v[16];
+#pragma unroll
+  for (int sI = 0; sI < 16; sI++) {
+    const int i = i0 + 4 * sI;
+    v[sI] = (i < nb && j < nb) ? A[(k0 + i) * lda + k0 + j] : (i == j ? 1.f : 0.f);
+  }
+#pragma unroll
+  for (int k = 0; k < MX_NB - 1; k++) {
+    if (k >= nb - 1) break;
+    const int buf = k & 1;
+    if (j == k) {
+#pragma unroll
+      for (int sI = 0; sI < 16; sI++) colk[buf][i0 + 4 * sI] = v[sI];
+    }
+    if (i0 == (k & 3)) rowk[buf][j] = v[k >> 2];
+    __syncthreads();
+    const float inv = 1.f / rowk[buf][k];
+    const float u = rowk[buf][j];
+#pragma unroll
+    for (int sI = 0; sI < 16; sI++) {
+      const int i = i0 + 4 * sI;
+      if (i > k) {
+        const float l = colk[buf][i] * inv;
+        if (j == k)
+          v[sI] = l;
+        else if (j > k)
+          v[sI] = fmaf(-l, u, v[sI]);
+      }
+    }
+  }
+#pragma unroll
+  for (int sI = 0; sI < 16; sI++) {
+    const int i = i0 + 4 * sI;
+    if (i < nb && j < nb) A[(k0 + i) * lda + k0 + j] = v[sI];
+  }
+}
+
+// rows r0 <= i < r1: A[i, k0:k0+nb] <- A[i, k0:k0+nb] U11^-1 (one thread per row)
+__global__ void __launch_bounds__(128)
+    k_trsm_right_f32(float* __restrict__ A, int64_t lda, int64_t r0, int64_t r1, int64_t k0, int nb) {
+  __shared__ float U[MX_NB][MX_NB];
+  __shared__ float inv[MX_NB];
+  for (int e = threadIdx.x; e < MX_NB * MX_NB; e += blockDim.x) {
+    const int m = e / MX_NB, jj = e % MX_NB;
+    U[m][jj] = (m < nb && jj < nb) ? A[(k0 + m) * lda + k0 + jj] : 0.f;
+  }
+  __syncthreads();
+  for (int m = threadIdx.x; m < MX_NB; m += blockDim.x) inv[m] = m < nb ? 1.f / U[m][m] : 1.f;
+  __syncthreads();
+  const int64_t i = r0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= r1) return;
+  float* row = A + i * lda + k0;
+  float v[MX_NB];
+#pragma unroll
+  for (int jj = 0; jj < MX_NB; jj++) v[jj] = jj < nb ? row[jj] : 0.f;
+#pragma unroll
+  for (int m = 0; m < MX_NB; m++) {
+    const float x = v[m] * inv[m];
+    v[m] = x;
+#pragma unroll
+    for (int jj = m + 1; jj < MX_NB; jj++) v[jj] = fmaf(-x, U[m][jj], v[jj]);
+  }
+#pragma unroll
+  for (int jj = 0; jj < MX_NB; jj++)
+    if (jj < nb) row[jj] = v[jj];
+}
+
+// columns c0 <= c < c1: A[k0:k0+nb, c] <- L11^-1 A[k0:k0+nb, c] (L11 unit
+// lower).  The CTA's 64 x 128 column tile passes through shared memory
+// (coalesced global access, constant-offset shared reads into registers).
+__global__ void __launch_bounds__(128)
+    k_trsm_left_f32(float* __restrict__ A, int64_t lda, int64_t c0, int64_t c1, int64_t k0, int nb) {
+  __shared__ float Lr[MX_NB][MX_NB];
+  __shared__ float T[MX_NB][128];
+  const int64_t cb = c0 + blockIdx.x * (int64_t)128;
+  const int ncol = c1 - cb < 128 ? int(c1 - cb) : 128;
+  for (int e = threadIdx.x; e < MX_NB * MX_NB; e += blockDim.x) {
+    const int ii = e / MX_NB, m = e % MX_NB;
+    Lr[ii][m] = (ii < nb && m < nb && m < ii) ? A[(k0 + ii) * lda + k0 + m] : 0.f;
+  }
+  for (int ii = 0; ii < MX_NB; ii++) T[ii][threadIdx.x] = (ii < nb && threadIdx.x < ncol) ? A[(k0 + ii) * lda + cb + threadIdx.x] : 0.f;
+  __syncthreads();
+  float v[MX_NB];
+#pragma unroll
+  for (int ii = 0; ii < MX_NB; ii++) v[ii] = T[ii][threadIdx.x];
+  // left-looking: v[ii] -= sum_{m < ii} L[ii][m] v[m] (rows of L read contiguously)
+#pragma unroll
+  for (int ii = 1; ii < MX_NB; ii++) {
+    float acc = v[ii];
+#pragma unroll
+    for (int m = 0; m < ii; m++) acc = fmaf(-Lr[ii][m], v[m], acc);
+    v[ii] = acc;
+  }
+#pragma unroll
+  for (int ii = 0; ii < MX_NB; ii++) T[ii][threadIdx.x] = v[ii];
+  __syncthreads();
+  for (int ii = 0; ii < nb; ii++)
+    if (threadIdx.x < ncol) A[(k0 + ii) * lda + cb + threadIdx.x] = T[ii][threadIdx.x];
+}
+
 // ---------------------------------------------------------------- tensor cores
 // C (M x Nc, ldc) -= A (M x K, lda) . B (K x Nc, ldb), FP32 row-major, on
 // the 5th-generation tensor cores (tcgen05.mma kind::tf32) with 3xTF32:
@@ -186,6 +302,73 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64
       : "memory");
 }
 
+// Global -> register staging of one K chunk (prefetched while the previous
+// chunk's MMAs run).  A: 128 rows x 32 k, item (row r = i / 8, k-quad i % 8):
+// the 8 lanes of a row read its 128 contiguous bytes.  B: 32 k x 256 n, thread
+// t owns column n = t, all 8 k-quads: each load is coalesced along n.
+template <bool VEC>
+__device__ __forceinline__ void gt_load(const float* __restrict__ A, int64_t lda, const float* __restrict__ B,
+                                        int64_t ldb, int64_t M, int64_t Nc, int K, int64_t m0, int64_t n0, int k0,
+                                        float (&ra)[16], float (&rb)[32]) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int it = tid + GT_THREADS * j, r = it >> 3, kq = it & 7;
+    const int64_t gr = m0 + r;
+    const int k = k0 + 4 * kq;
+    if (VEC && gr < M && k + 3 < K) {
+      const float4 v = *reinterpret_cast<const float4*>(A + gr * lda + k);
+      ra[4 * j] = v.x;
+      ra[4 * j + 1] = v.y;
+      ra[4 * j + 2] = v.z;
+      ra[4 * j + 3] = v.w;
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; u++) ra[4 * j + u] = (gr < M && k + u < K) ? A[gr * lda + k + u] : 0.f;
+    }
+  }
+  const int64_t gn = n0 + tid;
+#pragma unroll
+  for (int kq = 0; kq < 8; kq++)
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int k = k0 + 4 * kq + u;
+      rb[4 * kq + u] = (k < K && gn < Nc) ? B[(int64_t)k * ldb + gn] : 0.f;
+    }
+}
+
+// Registers -> shared memory (TF32 head and tail), 16-byte swizzled stores:
+// eight consecutive lanes write eight different chunk positions, no bank
+// conflicts.
+__device__ __forceinline__ void gt_store(uint32_t ah, uint32_t al, uint32_t bh, uint32_t bl, const float (&ra)[16],
+                                         const float (&rb)[32]) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int it = tid + GT_THREADS * j, r = it >> 3, kq = it & 7;
+    float h[4], l[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) split_tf32(ra[4 * j + u], h[u], l[u]);
+    const uint32_t off = tc::sw128(r, kq);
+    tc::st_shared_v4(ah + off, __float_as_uint(h[0]), __float_as_uint(h[1]), __float_as_uint(h[2]),
+                     __float_as_uint(h[3]));
+    tc::st_shared_v4(al + off, __float_as_uint(l[0]), __float_as_uint(l[1]), __float_as_uint(l[2]),
+                     __float_as_uint(l[3]));
+  }
+#pragma unroll
+  for (int kq = 0; kq < 8; kq++) {
+    float h[4], l[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) split_tf32(rb[4 * kq + u], h[u], l[u]);
+    const uint32_t off = tc::sw128(tid, kq);
+    tc::st_shared_v4(bh + off, __float_as_uint(h[0]), __float_as_uint(h[1]), __float_as_uint(h[2]),
+                     __float_as_uint(h[3]));
+    tc::st_shared_v4(bl + off, __float_as_uint(l[0]), __float_as_uint(l[1]), __float_as_uint(l[2]),
+                     __float_as_uint(l[3]));
+  }
+}
+
+template <bool VEC>
 __global__ void __launch_bounds__(GT_THREADS, 1)
     k_gemm_sub_tf32x3(float* __restrict__ C, int64_t ldc, const float* __restrict__ A, int64_t lda,
                       const float* __restrict__ B, int64_t ldb, int64_t M, int64_t Nc, int K, int* __restrict__ err) {
@@ -209,6 +392,8 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
                              (uint32_t(GT_M >> 4) << 24);
   const int nk = (K + GT_K - 1) / GT_K;
   bool ok = true;
+  float ra[16], rb[32];
+  gt_load<VEC>(A, lda, B, ldb, M, Nc, K, m0, n0, 0, ra, rb);
   for (int kc = 0; kc < nk; kc++) {
     const int b = kc & 1;
     if (kc >= 2) {  // the MMAs of chunk kc - 2 read buffer b
@@ -218,35 +403,10 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
         break;
       }
     }
-    const int k0 = kc * GT_K;
     const uint32_t ah = tc::smem_u32(sm.a_hi[b]), al = tc::smem_u32(sm.a_lo[b]);
     const uint32_t bh = tc::smem_u32(sm.b_hi[b]), bl = tc::smem_u32(sm.b_lo[b]);
-    // A: rows r (warp-strided), k = k0 + lane (one coalesced 128-byte row segment per warp)
-    for (int r = warp; r < GT_M; r += GT_THREADS / 32) {
-      const int64_t gr = m0 + r;
-      const int k = k0 + lane;
-      const float v = (gr < M && k < K) ? A[gr * lda + k] : 0.f;
-      float hi, lo;
-      split_tf32(v, hi, lo);
-      const uint32_t off = tc::sw128(r, lane >> 2) + (lane & 3) * 4;
-      asm volatile("st.shared.f32 [%0], %1;" ::"r"(ah + off), "f"(hi) : "memory");
-      asm volatile("st.shared.f32 [%0], %1;" ::"r"(al + off), "f"(lo) : "memory");
-    }
-    // B: k-rows (warp-strided), n = 32 seg + lane; stored transposed (row n, column k)
-    for (int kk = warp; kk < GT_K; kk += GT_THREADS / 32) {
-      const int k = k0 + kk;
-#pragma unroll
-      for (int seg = 0; seg < GT_N / 32; seg++) {
-        const int n = 32 * seg + lane;
-        const int64_t gn = n0 + n;
-        const float v = (k < K && gn < Nc) ? B[(int64_t)k * ldb + gn] : 0.f;
-        float hi, lo;
-        split_tf32(v, hi, lo);
-        const uint32_t off = tc::sw128(n, kk >> 2) + (kk & 3) * 4;
-        asm volatile("st.shared.f32 [%0], %1;" ::"r"(bh + off), "f"(hi) : "memory");
-        asm volatile("st.shared.f32 [%0], %1;" ::"r"(bl + off), "f"(lo) : "memory");
-      }
-    }
+    gt_store(ah, al, bh, bl, ra, rb);
+    if (kc + 1 < nk) gt_load<VEC>(A, lda, B, ldb, M, Nc, K, m0, n0, (kc + 1) * GT_K, ra, rb);
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
@@ -281,12 +441,24 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
       uint32_t v[16];
       tc::tmem_ld16(tbase + 16 * c, v);
       tc::tmem_wait_ld();
-      if (gr < M) {
-        float* crow = C + gr * ldc + n0 + 128 * (warp / 4) + 16 * c;
-        const int64_t col0 = n0 + 128 * (warp / 4) + 16 * c;
+      const int64_t col0 = n0 + 128 * (warp / 4) + 16 * c;
+      if (gr < M && col0 < Nc) {
+        float* crow = C + gr * ldc + col0;
+        if (VEC && col0 + 16 <= Nc) {
 #pragma unroll
-        for (int j = 0; j < 16; j++)
-          if (col0 + j < Nc) crow[j] -= __uint_as_float(v[j]);
+          for (int q = 0; q < 4; q++) {
+            float4 x = *reinterpret_cast<float4*>(crow + 4 * q);
+            x.x -= __uint_as_float(v[4 * q]);
+            x.y -= __uint_as_float(v[4 * q + 1]);
+            x.z -= __uint_as_float(v[4 * q + 2]);
+            x.w -= __uint_as_float(v[4 * q + 3]);
+            *reinterpret_cast<float4*>(crow + 4 * q) = x;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; j++)
+            if (col0 + j < Nc) crow[j] -= __uint_as_float(v[j]);
+        }
       }
     }
   }
@@ -301,24 +473,26 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
 static int gemm_sub_tf32x3(float* C, int64_t ldc, const float* A, int64_t lda, const float* B, int64_t ldb,
                            int64_t M, int64_t Nc, int K, int* err, cudaStream_t s) {
   if (M <= 0 || Nc <= 0 || K <= 0) return OK;
-  static bool attr_set[64] = {false};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return CUDA_ERR;
-  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    if (cudaFuncSetAttribute(k_gemm_sub_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, GT_SMEM_BYTES) !=
-        cudaSuccess)
-      return CUDA_ERR;
-    attr_set[dev] = true;
-  }
+  if (cudaFuncSetAttribute(k_gemm_sub_tf32x3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, GT_SMEM_BYTES) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_gemm_sub_tf32x3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, GT_SMEM_BYTES) !=
+          cudaSuccess)
+    return CUDA_ERR;
   dim3 grid(unsigned((Nc + GT_N - 1) / GT_N), unsigned((M + GT_M - 1) / GT_M));
-  k_gemm_sub_tf32x3<<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err);
+  // 16-byte vector access of A rows and C rows when every row start is aligned
+  const bool vec = (lda % 4 == 0) && (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0) &&
+                   (reinterpret_cast<uintptr_t>(C) % 16 == 0);
+  if (vec)
+    k_gemm_sub_tf32x3<true><<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err);
+  else
+    k_gemm_sub_tf32x3<false><<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err);
   return launch_status();
 }
 
 // FP32 LU without pivoting, two-level blocked: panels of 256 columns are
 // factored with the 64-wide kernels above (diagonal block, triangular
-// solves, SIMT updates inside the panel and its row block), and the
-// trailing matrix is updated once per panel on the tensor cores
+// solves) and tensor-core updates (K = 64) inside the panel and its row
+// block; the trailing matrix is updated once per panel on the tensor cores
 // (K = 256).  err receives 1 if a tensor-core wait ran out.
 constexpr int TC_PANEL = 256;
 static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, cudaStream_t s) {
@@ -326,14 +500,14 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, cudaStrea
     const int64_t pe = p0 + TC_PANEL < N ? p0 + TC_PANEL : N;
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
       const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
-      k_diag_lu<float><<<1, 256, 0, s>>>(A, lda, k0, nb);
+      k_diag_lu_f32<<<1, 256, 0, s>>>(A, lda, k0, nb);
       const int64_t below = N - k0 - nb, right = pe - k0 - nb;
-      if (below > 0) k_trsm_right<float><<<unsigned((below + 127) / 128), 128, 0, s>>>(A, lda, N, k0, nb);
+      if (below > 0) k_trsm_right_f32<<<unsigned((below + 127) / 128), 128, 0, s>>>(A, lda, k0 + nb, N, k0, nb);
       if (right > 0) {
-        k_trsm_left<float><<<unsigned((right + 127) / 128), 128, 0, s>>>(A, lda, k0 + nb, pe, k0, nb);
-        dim3 grid(unsigned((right + 127) / 128), unsigned((below + 127) / 128));
-        k_gemm_update<float><<<grid, 256, 0, s>>>(A + (k0 + nb) * lda + k0 + nb, lda, A + (k0 + nb) * lda + k0, lda,
-                                                  A + k0 * lda + k0 + nb, lda, below, right, nb);
+        k_trsm_left_f32<<<unsigned((right + 127) / 128), 128, 0, s>>>(A, lda, k0 + nb, pe, k0, nb);
+        const int st = gemm_sub_tf32x3(A + (k0 + nb) * lda + k0 + nb, lda, A + (k0 + nb) * lda + k0, lda,
+                                       A + k0 * lda + k0 + nb, lda, below, right, nb, err, s);
+        if (st != OK) return st;
       }
     }
     const int64_t rest = N - pe;
@@ -341,12 +515,12 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, cudaStrea
     // row block right of the panel: U12 = L11^-1 A12, 64 rows at a time
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
       const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
-      k_trsm_left<float><<<unsigned((rest + 127) / 128), 128, 0, s>>>(A, lda, pe, N, k0, nb);
+      k_trsm_left_f32<<<unsigned((rest + 127) / 128), 128, 0, s>>>(A, lda, pe, N, k0, nb);
       const int64_t rows = pe - k0 - nb;
       if (rows > 0) {
-        dim3 grid(unsigned((rest + 127) / 128), unsigned((rows + 127) / 128));
-        k_gemm_update<float><<<grid, 256, 0, s>>>(A + (k0 + nb) * lda + pe, lda, A + (k0 + nb) * lda + k0, lda,
-                                                  A + k0 * lda + pe, lda, rows, rest, nb);
+        const int st = gemm_sub_tf32x3(A + (k0 + nb) * lda + pe, lda, A + (k0 + nb) * lda + k0, lda, A + k0 * lda + pe,
+                                       lda, rows, rest, nb, err, s);
+        if (st != OK) return st;
       }
     }
     const int st = gemm_sub_tf32x3(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest,
@@ -382,29 +556,55 @@ __global__ void k_scale_to_f32(const double* __restrict__ A, int64_t lda, const 
   S[g] = float(A[i * lda + j] * c[j]);
 }
 
-// R[r, i] = F[r, i] - sum_j A[i, j] X[r, j]; one warp per row i, all right-hand
-// sides at once (A read once; nrhs <= 16).
+// R[r, i] = F[r, i] - sum_j A[i, j] X[r, j] (nrhs <= 16).  A CTA of 8 warps
+// takes 8 RPW rows; X is staged in shared memory in column chunks and
+// reused by all of them, so X is read N / (8 RPW) times instead of N times
+// and the kernel streams A.
 constexpr int MX_MAX_RHS = 16;
-__global__ void k_residual(const double* __restrict__ A, int64_t lda, const double* __restrict__ X,
-                           const double* __restrict__ F, double* __restrict__ R, int64_t N, int nrhs) {
-  int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32;
-  int lane = threadIdx.x & 31;
-  if (i >= N) return;
-  double acc[MX_MAX_RHS];
+template <int RPW>  // rows per warp: 4 for nrhs <= 8, 2 for nrhs <= 16
+__global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, int64_t lda,
+                                                 const double* __restrict__ X, const double* __restrict__ F,
+                                                 double* __restrict__ R, int64_t N, int nrhs) {
+  constexpr int NR = RPW == 4 ? 8 : 16;
+  constexpr int RES_COLS = RPW == 4 ? 512 : 256;  // 32 KB of X per chunk
+  __shared__ double xs[NR][RES_COLS];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int64_t row0 = ((int64_t)blockIdx.x * 8 + warp) * RPW;
+  double acc[RPW][NR];
 #pragma unroll
-  for (int r = 0; r < MX_MAX_RHS; r++) acc[r] = 0.0;
-  const double* row = A + i * lda;
-  for (int64_t j = lane; j < N; j += 32) {
-    double a = row[j];
+  for (int q = 0; q < RPW; q++)
 #pragma unroll
-    for (int r = 0; r < MX_MAX_RHS; r++)
-      if (r < nrhs) acc[r] = fma(a, X[r * N + j], acc[r]);
+    for (int r = 0; r < NR; r++) acc[q][r] = 0.0;
+  for (int64_t c0 = 0; c0 < N; c0 += RES_COLS) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < NR * RES_COLS; e += blockDim.x) {
+      const int r = e / RES_COLS, c = e % RES_COLS;
+      xs[r][c] = (r < nrhs && c0 + c < N) ? X[(int64_t)r * N + c0 + c] : 0.0;
+    }
+    __syncthreads();
+    // the warp's rows interleaved: RPW independent loads per column, and each
+    // staged x value read once for all of them
+#pragma unroll 4
+    for (int c = lane; c < RES_COLS; c += 32) {
+      if (c0 + c >= N) break;
+      double a[RPW];
+#pragma unroll
+      for (int q = 0; q < RPW; q++) a[q] = row0 + q < N ? A[(row0 + q) * lda + c0 + c] : 0.0;
+#pragma unroll
+      for (int r = 0; r < NR; r++) {
+        const double x = xs[r][c];
+#pragma unroll
+        for (int q = 0; q < RPW; q++) acc[q][r] = fma(a[q], x, acc[q][r]);
+      }
+    }
   }
 #pragma unroll
-  for (int r = 0; r < MX_MAX_RHS; r++) {
-    if (r < nrhs) {
-      double v = warp_sum(acc[r]);
-      if (lane == 0) R[r * N + i] = F[r * N + i] - v;
+  for (int q = 0; q < RPW; q++) {
+    const int64_t i = row0 + q;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      const double v = warp_sum(acc[q][r]);
+      if (lane == 0 && i < N && r < nrhs) R[(int64_t)r * N + i] = F[(int64_t)r * N + i] - v;
     }
   }
 }
@@ -473,80 +673,125 @@ __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__
 }
 
 // X (nrhs x N, row r at X + r N) <- T^-1 X with T the unit lower (LOWER) or
-// upper triangle of LU.  256 threads: thread = (row i of the block, group of
-// 4 right-hand sides).  flags[blk] == epoch marks a published block.
-template <bool LOWER>
+// upper triangle of LU.  256 threads (8 warps).  Every finished block's tile
+// is shared by all 8 warps (warp w: columns 8w .. 8w + 7, lane: rows lane and
+// lane + 32): per tile one bounded wait for the block's flag, one staging of
+// its solution in shared memory, and 16 factor values per lane prefetched
+// into registers before the wait -- so the step that gates publication (the
+// tile of the block just before) costs one short pass, not a full tile on
+// one warp.  Partial sums meet in shared memory, then the FP64 inverse of
+// the diagonal block (staged before any waiting) is applied.
+// flags[blk] == epoch marks a published block.
+template <bool LOWER, int NR>
 __global__ void __launch_bounds__(256) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
                                                    const double* __restrict__ Dinv, double* __restrict__ X, int nrhs,
                                                    int* __restrict__ flags, int epoch, int* __restrict__ err) {
-  __shared__ float Lt[TS_B][TS_B + 1];
-  __shared__ double xs[MX_MAX_RHS][TS_B];
+  extern __shared__ __align__(16) double sw_dyn[];  // the block's diagonal inverse, 64 x 64 (column-major)
+  __shared__ double accs[TS_B][NR];
+  __shared__ double rs[NR][TS_B];
+  __shared__ double xs[NR][TS_B];
   __shared__ int s_fail;
   const int nblk = int((N + TS_B - 1) / TS_B);
   const int q = blockIdx.x;
   const int b = LOWER ? q : nblk - 1 - q;
   const int64_t b0 = (int64_t)b * TS_B;
-  const int i = threadIdx.x % TS_B, rg = threadIdx.x / TS_B;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  // everything that does not depend on other blocks first: the diagonal
+  // inverse and this block's right-hand side
+  const double* Dg = Dinv + (int64_t)b * TS_B * TS_B;
+  for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) sw_dyn[e] = Dg[e];
+  for (int e = threadIdx.x; e < TS_B * NR; e += blockDim.x) accs[e / NR][e % NR] = 0.0;
+  for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
+    const int r = e / TS_B, c = e % TS_B;
+    rs[r][c] = (r < nrhs && b0 + c < N) ? X[(int64_t)r * N + b0 + c] : 0.0;
+  }
   if (threadIdx.x == 0) s_fail = 0;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int t = 0; t < q; t++) {
-    const int j = LOWER ? t : nblk - 1 - t;  // a finished block, in publication order
-    const int64_t j0 = (int64_t)j * TS_B;
-    // factor tile (rows of block b, columns of block j), coalesced along rows
-    for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) {
-      const int r = e / TS_B, c = e % TS_B;
-      Lt[r][c] = (b0 + r < N && j0 + c < N) ? LU[(b0 + r) * lda + j0 + c] : 0.f;
+  __syncthreads();
+  double acc[2][NR];
+#pragma unroll
+  for (int h = 0; h < 2; h++)
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[h][r] = 0.0;
+  // this lane's factor values of a tile: rows b0 + lane + 32 h, columns j0 + 8 warp + c
+  float lv[2][8];
+  auto load_lu = [&](int j) {
+    const int64_t j0 = (int64_t)j * TS_B + 8 * warp;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int64_t row = b0 + lane + 32 * h;
+#pragma unroll
+      for (int c = 0; c < 8; c++) lv[h][c] = (row < N && j0 + c < N) ? LU[row * lda + j0 + c] : 0.f;
     }
+  };
+  if (q > 0) load_lu(LOWER ? 0 : nblk - 1);
+  for (int t = 0; t < q; t++) {
+    const int j = LOWER ? t : nblk - 1 - t;  // finished blocks in publication order
+    const int64_t j0 = (int64_t)j * TS_B;
     if (threadIdx.x == 0) {
       const long long t0 = clock64();
+      unsigned ns = 32;  // back off so that hundreds of waiting CTAs do not flood L2
       while (ld_acquire(flags + j) != epoch) {
         if (clock64() - t0 > TRSV_WAIT_CYCLES) {
           s_fail = 1;
           atomicExch(err, 1);
           break;
         }
+        __nanosleep(ns);
+        ns = ns < 256 ? 2 * ns : 256;
       }
     }
     __syncthreads();
     if (s_fail) break;
-    for (int e = threadIdx.x; e < nrhs * TS_B; e += blockDim.x) {
-      const int r = e / TS_B, c = e % TS_B;
-      xs[r][c] = (j0 + c < N) ? __ldcg(X + (int64_t)r * N + j0 + c) : 0.0;  // published by another CTA: via L2
+    for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
+      const int r = e / TS_B, c = e % TS_B;  // published by another CTA: read via L2
+      xs[r][c] = (r < nrhs && j0 + c < N) ? __ldcg(X + (int64_t)r * N + j0 + c) : 0.0;
     }
     __syncthreads();
-#pragma unroll 4
-    for (int m = 0; m < TS_B; m++) {
-      const double l = Lt[i][m];
+    float lc[2][8];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int r = 4 * rg + u;
-        if (r < nrhs) acc[u] = fma(l, xs[r][m], acc[u]);
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int c = 0; c < 8; c++) lc[h][c] = lv[h][c];
+    if (t + 1 < q) load_lu(LOWER ? t + 1 : nblk - 2 - t);
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+#pragma unroll
+      for (int r = 0; r < NR; r++) {
+        const double x = xs[r][8 * warp + c];
+#pragma unroll
+        for (int h = 0; h < 2; h++) acc[h][r] = fma(double(lc[h][c]), x, acc[h][r]);
       }
     }
-    __syncthreads();
+    __syncthreads();  // xs is rewritten by the next tile
   }
-  // right-hand side minus the accumulated products, then the diagonal inverse
-  __shared__ double rs[MX_MAX_RHS][TS_B];
 #pragma unroll
-  for (int u = 0; u < 4; u++) {
-    const int r = 4 * rg + u;
-    if (r < nrhs) rs[r][i] = (b0 + i < N) ? X[(int64_t)r * N + b0 + i] - acc[u] : 0.0;
+  for (int h = 0; h < 2; h++)
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+      if (r < nrhs) atomicAdd(&accs[lane + 32 * h][r], acc[h][r]);
+  __syncthreads();
+  // right-hand side minus the accumulated products, then the diagonal inverse
+  const int i = threadIdx.x % TS_B, rg = threadIdx.x / TS_B;
+  for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
+    const int r = e / TS_B, c = e % TS_B;
+    rs[r][c] -= accs[c][r];
   }
   __syncthreads();
-  const double* D = Dinv + (int64_t)b * TS_B * TS_B;
-  double out[4] = {0.0, 0.0, 0.0, 0.0};
+  const double* D = sw_dyn;
+  constexpr int RPT = NR / 4;  // right-hand sides per thread
+  double out[RPT];
+#pragma unroll
+  for (int u = 0; u < RPT; u++) out[u] = 0.0;
+#pragma unroll 8
   for (int m = 0; m < TS_B; m++) {
     const double d = D[m * TS_B + i];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int r = 4 * rg + u;
-      if (r < nrhs) out[u] = fma(d, rs[r][m], out[u]);
-    }
+    for (int u = 0; u < RPT; u++) out[u] = fma(d, rs[RPT * rg + u][m], out[u]);
   }
   const double nan = __longlong_as_double(0x7ff8000000000000LL);
 #pragma unroll
-  for (int u = 0; u < 4; u++) {
-    const int r = 4 * rg + u;
+  for (int u = 0; u < RPT; u++) {
+    const int r = RPT * rg + u;
     if (r < nrhs && b0 + i < N) X[(int64_t)r * N + b0 + i] = s_fail ? nan : out[u];
   }
   __syncthreads();
@@ -667,6 +912,14 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   k_diag_inverse<true><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_l);
   k_diag_inverse<false><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_u);
   if (cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s) != cudaSuccess) return CUDA_ERR;
+  constexpr int SW_DYN = TS_B * TS_B * int(sizeof(double));  // 32 KB: the diagonal inverse
+  if (cudaFuncSetAttribute(k_trsv_sweep<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_DYN) != cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_DYN) != cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_DYN) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_DYN) !=
+          cudaSuccess)
+    return CUDA_ERR;
   int epoch = 0;
   if (cudaMemsetAsync(X, 0, sizeof(double) * N * nrhs, s) != cudaSuccess) return CUDA_ERR;
   const int nr = int(nrhs);
@@ -674,9 +927,17 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   double rel = 1e300;
   for (it = 1; it <= max_iter; it++) {
     // D = F - A X (FP64), then D <- (L U)^-1 D with the FP32 factors
-    k_residual<<<unsigned((N * 32 + 255) / 256), 256, 0, s>>>(A, lda, X, F, D, N, nr);
-    k_trsv_sweep<true><<<unsigned(nblk), 256, 0, s>>>(S, N, N, dinv_l, D, nr, flags, ++epoch, err);
-    k_trsv_sweep<false><<<unsigned(nblk), 256, 0, s>>>(S, N, N, dinv_u, D, nr, flags, ++epoch, err);
+    if (nr <= 8)
+      k_residual<4><<<unsigned((N + 31) / 32), 256, 0, s>>>(A, lda, X, F, D, N, nr);
+    else
+      k_residual<2><<<unsigned((N + 15) / 16), 256, 0, s>>>(A, lda, X, F, D, N, nr);
+    if (nr <= 8) {
+      k_trsv_sweep<true, 8><<<unsigned(nblk), 256, SW_DYN, s>>>(S, N, N, dinv_l, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<false, 8><<<unsigned(nblk), 256, SW_DYN, s>>>(S, N, N, dinv_u, D, nr, flags, ++epoch, err);
+    } else {
+      k_trsv_sweep<true, 16><<<unsigned(nblk), 256, SW_DYN, s>>>(S, N, N, dinv_l, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<false, 16><<<unsigned(nblk), 256, SW_DYN, s>>>(S, N, N, dinv_u, D, nr, flags, ++epoch, err);
+    }
     if (cudaMemsetAsync(maxes, 0, sizeof(unsigned long long) * 2 * nr, s) != cudaSuccess) return CUDA_ERR;
     k_apply_correction<<<unsigned((N * nrhs + 255) / 256), 256, 0, s>>>(X, D, c, N, nr, maxes);
     unsigned long long bits[2 * MX_MAX_RHS];

@@ -935,28 +935,35 @@ constexpr int TC_SMEM_BYTES = int(sizeof(TcSmem)) + 1024;  // + alignment slack 
 
 __device__ __forceinline__ void st_bf16(uint8_t* dst, __nv_bfloat16 v) { *reinterpret_cast<__nv_bfloat16*>(dst) = v; }
 
+// x / 2 of a BF16 value (exact: a power-of-two scale).
+__device__ __forceinline__ __nv_bfloat16 half_bf16(__nv_bfloat16 x) {
+  return __float2bfloat16(0.5f * __bfloat162float(x));
+}
+
 // Stages the network in the swizzled operand layout (all threads take part).
+// The four SiLU layers' weights and biases are stored scaled by 1/2 (exact),
+// so their accumulators hold h = z / 2 directly (silu(z) = h + h tanh(h)).
 __device__ void tc_load_network(TcSmem& s, const __nv_bfloat16* __restrict__ wb, const float* __restrict__ pf) {
   const int nt = blockDim.x;
   for (int e = threadIdx.x; e < MLP_H * MLP_IN; e += nt) {
     const int n = e / MLP_IN, k = e % MLP_IN;
-    st_bf16(s.w1 + tc::sw128(n, k >> 3) + (k & 7) * 2, wb[MLP_OFF_W1 + e]);
+    st_bf16(s.w1 + tc::sw128(n, k >> 3) + (k & 7) * 2, half_bf16(wb[MLP_OFF_W1 + e]));
   }
   const int64_t off[3] = {MLP_OFF_W2, MLP_OFF_W3, MLP_OFF_W4};
   for (int l = 0; l < 3; l++)
     for (int e = threadIdx.x; e < MLP_H * MLP_H; e += nt) {
       const int n = e / MLP_H, k = e % MLP_H;
-      st_bf16(s.wh[l][k >> 6] + tc::sw128(n, (k & 63) >> 3) + (k & 7) * 2, wb[off[l] + e]);
+      st_bf16(s.wh[l][k >> 6] + tc::sw128(n, (k & 63) >> 3) + (k & 7) * 2, half_bf16(wb[off[l] + e]));
     }
   for (int e = threadIdx.x; e < MLP_OUT * MLP_H; e += nt) {
     const int n = e / MLP_H, k = e % MLP_H;
     st_bf16(s.w5[k >> 6] + tc::sw128(n, (k & 63) >> 3) + (k & 7) * 2, wb[MLP_OFF_W5 + e]);
   }
   for (int e = threadIdx.x; e < MLP_H; e += nt) {
-    s.b1[e] = pf[MLP_OFF_B1 + e];
-    s.bh[0][e] = pf[MLP_OFF_B2 + e];
-    s.bh[1][e] = pf[MLP_OFF_B3 + e];
-    s.bh[2][e] = pf[MLP_OFF_B4 + e];
+    s.b1[e] = 0.5f * pf[MLP_OFF_B1 + e];
+    s.bh[0][e] = 0.5f * pf[MLP_OFF_B2 + e];
+    s.bh[1][e] = 0.5f * pf[MLP_OFF_B3 + e];
+    s.bh[2][e] = 0.5f * pf[MLP_OFF_B4 + e];
   }
   for (int e = threadIdx.x; e < MLP_OUT; e += nt) s.b5[e] = pf[MLP_OFF_B5 + e];
 }
@@ -1019,25 +1026,35 @@ struct TcEngine {
       tc::fence_after_sync();
       if (layer < 4) {
         const float* bias = layer == 0 ? s.b1 : s.bh[layer - 1];
-#pragma unroll 1
+        // 16 columns at a time, the TMEM load of the next chunk in flight
+        // while this one is processed.  The staged weights and biases of
+        // these layers are pre-scaled by 1/2 (exact), so acc + bias is
+        // h = z / 2 and silu(z) = h + h tanh(h).
+        uint32_t va[16], vb[16];
+        tc::tmem_ld16(tld, va);
+        tc::tmem_wait_ld16(va);
+#pragma unroll
         for (int c = 0; c < 8; c++) {  // columns 16c .. 16c + 15
-          uint32_t v[16];
-          tc::tmem_ld16(tld + 16 * c, v);
-          tc::tmem_wait_ld();
+          uint32_t* cur = (c & 1) ? vb : va;
+          uint32_t* nxt = (c & 1) ? va : vb;
+          if (c < 7) tc::tmem_ld16(tld + 16 * (c + 1), nxt);
           uint32_t q[8];
 #pragma unroll
-          for (int j = 0; j < 8; j++)
-            q[j] = silu2_bf16(__uint_as_float(v[2 * j]) + bias[16 * c + 2 * j],
-                              __uint_as_float(v[2 * j + 1]) + bias[16 * c + 2 * j + 1]);
+          for (int j = 0; j < 8; j++) {
+            const float h0 = __uint_as_float(cur[2 * j]) + bias[16 * c + 2 * j];
+            const float h1 = __uint_as_float(cur[2 * j + 1]) + bias[16 * c + 2 * j + 1];
+            q[j] = pack_bf16(fmaf(h0, tanh_fast(h0), h0), fmaf(h1, tanh_fast(h1), h1));
+          }
           // next layer's K = 16c .. 16c + 15: atom c / 4, chunks 2 (c % 4), 2 (c % 4) + 1
           const uint32_t base = act + (c >> 2) * TC_ATOM;
           tc::st_shared_v4(base + tc::sw128(row, 2 * (c & 3)), q[0], q[1], q[2], q[3]);
           tc::st_shared_v4(base + tc::sw128(row, 2 * (c & 3) + 1), q[4], q[5], q[6], q[7]);
+          if (c < 7) tc::tmem_wait_ld16(nxt);
         }
       } else {
         uint32_t v[16];
         tc::tmem_ld16(tld, v);
-        tc::tmem_wait_ld();
+        tc::tmem_wait_ld16(v);
 #pragma unroll
         for (int j = 0; j < MLP_OUT; j++) y[j] = __uint_as_float(v[j]) + s.b5[j];
       }
@@ -1135,6 +1152,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
 using namespace tb;
 
+// cudaFuncSetAttribute once per device and kernel (a later call, e.g. inside
+// a stream capture, then only launches).
+template <class K>
+static int set_smem_once(K* kernel, int bytes, bool (&done)[64]) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return CUDA_ERR;
+  if (dev >= 0 && dev < 64 && done[dev]) return OK;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+    return CUDA_ERR;
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return OK;
+}
+static bool g_attr_trace_tc[64], g_attr_points_tc[64], g_attr_trace_warp[64], g_attr_points_warp[64];
+
 static int fill_surrogate_params(const tb_field_t* field, const tb_surrogate_t* sur, TraceParams& P,
                                  SurrogateParams& S) {
   if (!field->axial_z || field->axial_nz < 2 || !field->axial_elec) return BAD_ARG;
@@ -1177,9 +1208,7 @@ extern "C" int tb_surrogate_field_points(const double* points, int64_t M, const 
   int st = fill_surrogate_params(field, sur, P, S);
   if (st != OK) return st;
   if (sur->engine == 0) {
-    if (cudaFuncSetAttribute(k_surrogate_points_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES) !=
-        cudaSuccess)
-      return CUDA_ERR;
+    if (set_smem_once(k_surrogate_points_tc, TC_SMEM_BYTES, g_attr_points_tc) != OK) return CUDA_ERR;
     int64_t blocks = (M + TC_THREADS - 1) / TC_THREADS;
     if (blocks > num_sms()) blocks = num_sms();
     k_surrogate_points_tc<<<unsigned(blocks), TC_THREADS, TC_SMEM_BYTES, (cudaStream_t)stream>>>(P, S, points, M, out,
@@ -1187,8 +1216,7 @@ extern "C" int tb_surrogate_field_points(const double* points, int64_t M, const 
     return launch_status();
   }
   const int smem = int(sizeof(SurrogateSmem));
-  if (cudaFuncSetAttribute(k_surrogate_points, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-    return CUDA_ERR;
+  if (set_smem_once(k_surrogate_points, smem, g_attr_points_warp) != OK) return CUDA_ERR;
   int64_t blocks = (M + SG_THREADS - 1) / SG_THREADS;
   if (blocks > 4 * num_sms()) blocks = 4 * num_sms();
   k_surrogate_points<<<unsigned(blocks), SG_THREADS, smem, (cudaStream_t)stream>>>(P, S, points, M, out, used_bem);
@@ -1226,9 +1254,7 @@ extern "C" int tb_trace_surrogate(const double* start, const double* t0, const d
   if (sur->engine == 0) {
     // one CTA (3 groups of 128 particles) per SM; fewer only when there are
     // fewer particles than that
-    if (cudaFuncSetAttribute(k_trace_surrogate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES) !=
-        cudaSuccess)
-      return CUDA_ERR;
+    if (set_smem_once(k_trace_surrogate_tc, TC_SMEM_BYTES, g_attr_trace_tc) != OK) return CUDA_ERR;
     int64_t blocks = num_sms();
     const int64_t by_work = (n + TC_THREADS - 1) / TC_THREADS;
     if (blocks > by_work) blocks = by_work;
@@ -1236,8 +1262,7 @@ extern "C" int tb_trace_surrogate(const double* start, const double* t0, const d
     return launch_status();
   }
   const int smem = int(sizeof(SurrogateSmem));
-  if (cudaFuncSetAttribute(k_trace_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-    return CUDA_ERR;
+  if (set_smem_once(k_trace_surrogate, smem, g_attr_trace_warp) != OK) return CUDA_ERR;
   // one block per SM; fewer only when there is not a warp of particles per SM
   int64_t blocks = num_sms();
   int64_t by_work = (n + 31) / 32;

@@ -115,6 +115,23 @@ class Field:
     def copy(self):
         return copy.copy(self)
 
+    def map_points(self, fun):
+        """Copy of the field in the frame moved by the point map `fun`
+        (traceon/field.py:168-177): the origin goes to fun(origin), the basis
+        vectors to fun(b + origin) - fun(origin)."""
+        f = self.copy()
+        f._origin = np.asarray(fun(self._origin), dtype=np.float64)
+        assert f._origin.shape == (3,), 'Transformation of field did not map origin to a 3D point'
+        f._basis = np.array([np.asarray(fun(b + self._origin), dtype=np.float64) - f._origin for b in self._basis])
+        assert f._basis.shape == (3, 3), 'Transformation of field did not map unit vectors to a 3D vector'
+        assert np.linalg.det(f._basis) != 0, 'Transformations of field have resulted in a two-dimensional system'
+        return f
+
+    def move(self, dx=0.0, dy=0.0, dz=0.0):
+        """Translated copy (traceon/mesher.py:46-65)."""
+        d = np.array([dx, dy, dz], dtype=np.float64)
+        return self.map_points(lambda p: np.asarray(p, dtype=np.float64) + d)
+
     def map_points_to_local(self, point):
         # global = basis @ local + origin (traceon/field.py:154-200)
         p = np.asarray(point, dtype=np.float64) - self._origin
@@ -214,10 +231,28 @@ class Field:
         return Tracer(self, bounds)
 
 
+def _axial_shift(field):
+    """z offset of a field whose frame keeps the symmetry axis: origin on the z
+    axis and a basis that maps z to z (any rotation about z).  A radially
+    symmetric field in such a frame is the same field shifted along z, which
+    is what lets superposed radial fields be traced as one source set."""
+    o, b = field._origin, field._basis
+    if abs(o[0]) > 0 or abs(o[1]) > 0 or not np.allclose(b[:, 2], [0.0, 0.0, 1.0]) or \
+            not np.allclose(b[2, :2], 0.0) or not np.allclose(b.T @ b, np.eye(3)):
+        raise NotImplementedError('GPU tracing of a superposition needs every member field to keep the z axis '
+                                  '(origin on the axis, rotations about z only)')
+    return float(o[2])
+
+
 class FieldSuperposition(Field):
     """Linear combination of fields (traceon/field.py:424-507).  Point
-    evaluations sum the member fields; tracing needs a single BEM or axial
-    field (a superposition of BEM fields on one geometry collapses to one)."""
+    evaluations sum the member fields.  Tracing is GPU-native (the reference
+    calls back into Python for every field evaluation of a superposition,
+    traceon/field.py:464-465, tracing.py): radial BEM members collapse into
+    one source set (charges times factors, concatenated, shifted along z by
+    their origins) and radial axial members on one z grid into one
+    coefficient table; mixing BEM and axial members, field bounds on members,
+    and frames that move the symmetry axis are not supported."""
 
     def __init__(self, fields, factors=None):
         super().__init__()
@@ -247,6 +282,11 @@ class FieldSuperposition(Field):
             return FieldSuperposition(self.fields + other.fields, np.concatenate([self.factors, other.factors]))
         return FieldSuperposition(self.fields + [other], np.concatenate([self.factors, [1.0]]))
 
+    def __radd__(self, other):
+        if isinstance(other, Field):
+            return FieldSuperposition([other] + self.fields, np.concatenate([[1.0], self.factors]))
+        return NotImplemented
+
     def __mul__(self, other):
         if _is_numeric(other):
             return FieldSuperposition(self.fields, other * self.factors)
@@ -254,6 +294,56 @@ class FieldSuperposition(Field):
 
     def __len__(self):
         return len(self.fields)
+
+    def _members(self):
+        """(factor, field) pairs with nested superpositions expanded."""
+        out = []
+        for fa, f in zip(self.factors, self.fields):
+            if isinstance(f, FieldSuperposition):
+                out += [(float(fa) * g_fa, g) for g_fa, g in f._members()]
+            else:
+                out.append((float(fa), f))
+        return out
+
+    def _trace_field(self):
+        """(tb_field_t, keep-alive tensors) of the whole superposition."""
+        torch = B._torch()
+        members = self._members()
+        if not members:
+            raise ValueError('empty superposition')
+        if any(f.field_bounds is not None for _, f in members):
+            raise NotImplementedError('GPU tracing of a superposition whose members have field bounds')
+        if all(isinstance(f, FieldRadialBEM) for _, f in members):
+            groups = ([], [], [])
+            for fa, f in members:
+                dz = _axial_shift(f)
+                for lst, pc in zip(groups, (f.electrostatic_point_charges, f.magnetostatic_point_charges,
+                                            f.current_point_charges)):
+                    if len(pc):
+                        src = pc.device_sources().clone()
+                        src[1] += dz
+                        src[2] *= fa
+                        lst.append(src)
+            dev = B.device()
+            e, m, c = (torch.cat(lst, 1).contiguous() if lst else torch.empty((3, 0), dtype=torch.float64, device=dev)
+                       for lst in groups)
+            f = B.TbField(e.data_ptr() if e.numel() else None, e.shape[1], m.data_ptr() if m.numel() else None,
+                          m.shape[1], c.data_ptr() if c.numel() else None, c.shape[1], None, None, None, None, 0)
+            return f, (e, m, c)
+        if all(isinstance(f, FieldRadialAxial) for _, f in members):
+            fa0, f0 = members[0]
+            z0 = f0.z + _axial_shift(f0)
+            ec = np.zeros_like(f0.electrostatic_coeffs)
+            mc = np.zeros_like(f0.magnetostatic_coeffs)
+            for fa, f in members:
+                if f.z.shape != f0.z.shape or not np.allclose(f.z + _axial_shift(f), z0, rtol=0, atol=1e-15):
+                    raise NotImplementedError('GPU tracing of a superposition of axial fields on different z grids')
+                ec += fa * f.electrostatic_coeffs
+                mc += fa * f.magnetostatic_coeffs
+            zt, ect, mct = B.to_dev(z0, torch.float64), B.to_dev(ec, torch.float64), B.to_dev(mc, torch.float64)
+            f = B.TbField(None, 0, None, 0, None, 0, None, zt.data_ptr(), ect.data_ptr(), mct.data_ptr(), len(z0))
+            return f, (zt, ect, mct)
+        raise NotImplementedError('GPU tracing of a superposition that mixes BEM and axial fields')
 
 
 class FieldBEM(Field):

@@ -146,3 +146,35 @@ def surrogate_beam(n: int, seed: int):
 
 LENS_BOUNDS = np.array([[-2 * MM, 2 * MM], [-2 * MM, 2 * MM], [-10 * MM, 10 * MM]])
 LENS_EXIT_Z = 9.5 * MM
+
+
+def random_lens(seed: int, n_range=(500, 6000), tubes_range=(2, 5), r_range=(0.5 * MM, 3.0 * MM),
+                gap_range=(0.2 * MM, 1.0 * MM), length_range=(1.0 * MM, 4.0 * MM), cap=0.5 * MM,
+                volt_range=(-5000.0, 5000.0)):
+    """A synthetic coaxial lens of the batching workload: N ~ U[n_range]
+    elements over 2-5 tubes along z with radii ~ U[0.5, 3] mm, gaps between
+    consecutive tubes ~ U[0.2, 1] mm, lengths ~ U[1, 4] mm, annular caps of
+    0.5 mm; returns (geometry, voltages ~ U[-5, 5] kV per electrode)."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(n_range[0], n_range[1] + 1))
+    k = int(rng.integers(tubes_range[0], tubes_range[1] + 1))
+    radii = rng.uniform(*r_range, k)
+    lengths = rng.uniform(*length_range, k)
+    gaps = rng.uniform(*gap_range, k - 1)
+    z = -0.5 * (lengths.sum() + gaps.sum())
+    spans = []
+    for i in range(k):
+        spans.append((z, z + lengths[i]))
+        z += lengths[i] + (gaps[i] if i < k - 1 else 0.0)
+    # elements per electrode in proportion to its outline length
+    outline = lengths + 2 * cap
+    per = split_counts(n, outline) if k > 1 else [n]
+    verts, idx, segs = [], [], []
+    for e, ((z0, z1), r, m) in enumerate(zip(spans, radii, per)):
+        v = aperture_tube(r, r + cap, z0, z1, max(int(m), 6))
+        verts.append(v)
+        idx.append(np.full(len(v), e))
+        corners = [(r + cap, z0), (r, z0), (r, z1), (r + cap, z1)]
+        segs += [(a[0], a[1], b[0], b[1]) for a, b in zip(corners[:-1], corners[1:])]
+    geo = LensGeometry(np.concatenate(verts), np.concatenate(idx), [f'electrode{i}' for i in range(k)], segs)
+    return geo, rng.uniform(*volt_range, k)

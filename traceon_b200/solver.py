@@ -99,6 +99,10 @@ class SolverRadial:
     def get_matrix_device(self):
         """The full BEM matrix as an (N, N) FP64 device tensor."""
         torch = B._torch()
+        pre = getattr(self, '_prefilled', None)
+        if pre is not None:  # filled by solve_direct_batch
+            self._prefilled = None
+            return pre
         v, t, val, jac, pos = self.device()
         N = len(self.vertices)
         A = torch.empty((N, N), dtype=torch.float64, device=v.device)
@@ -195,6 +199,28 @@ def solve_direct_superposition(excitation):
         F = np.array([MagnetostaticSolverRadial(mag[n]).get_right_hand_side() for n in names])
         for n, f in zip(names, MagnetostaticSolverRadial(excitation).solve_matrix(F)):
             out[n] = f
+    return out
+
+
+def solve_direct_batch(excitations, method='mixed'):
+    """Electrostatic fields of many excitations (geometries of uneven N): all
+    matrices are filled in one persistent launch (tb_fill_matrix_radial_batched)
+    plus one launch for every self term, then each geometry's charges are
+    solved on the device.  No counterpart in the reference, which solves one
+    excitation at a time (traceon/solver.py:402-431); each result equals
+    solve_direct(excitation)."""
+    torch = B._torch()
+    solvers = [ElectrostaticSolverRadial(e) for e in excitations]
+    items = []
+    for s_ in solvers:
+        v, t, val, jac, pos = s_.device()
+        N = len(s_.vertices)
+        items.append((v, t, val, jac, pos, torch.empty((N, N), dtype=torch.float64, device=v.device)))
+    B.dev_fill_batched(items)
+    out = []
+    for s_, item in zip(solvers, items):
+        s_._prefilled = item[5]
+        out.append(s_.solve_matrix(method=method)[0])
     return out
 
 

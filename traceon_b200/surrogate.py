@@ -429,6 +429,10 @@ class FieldSurrogate:
         return (res.plane.cpu().numpy(), res.final.cpu().numpy(), res.status.cpu().numpy(),
                 res.counters.cpu().numpy())
 
+    def trace_session(self, n, bounds, plane_z, mass=None, charge=None, atol=1e-8, max_attempts=100_000):
+        """A TraceSession for repeated batches of n particles (see there)."""
+        return TraceSession(self, n, bounds, plane_z, mass, charge, atol, max_attempts)
+
     def kernel_field_at_points(self, points):
         """Surrogate E at points (M, 3) as the tracer's kernel evaluates it
         (electrode fallback included); returns (E, used_bem)."""
@@ -469,3 +473,95 @@ _lib.tb_trace_surrogate.argtypes = _tb_trace_surrogate_args
 _lib.tb_surrogate_field_points.argtypes = [_vp, _i64, C.POINTER(B.TbField), C.POINTER(TbSurrogate), _vp, _vp, _vp]
 _lib.tb_surrogate_field_points.restype = C.c_int
 _lib.tb_trace_surrogate.restype = C.c_int
+
+
+class TraceSession:
+    """Repeated endpoint tracing of batches of n particles through one
+    surrogate field, for callers that trace many batches: pinned host staging
+    buffers, static device buffers, and the whole step -- host-to-device copy
+    of the start states, the tracer launch (work-queue reset + kernel),
+    device-to-host copies of the endpoints -- captured once in a CUDA graph.
+    Each run() is one graph replay and one stream synchronisation.
+
+    run(position, velocity) returns views of the pinned output buffers
+    (plane (n,7), final (n,7), status (n,), counters (n,3)), valid until the
+    next run(); copy them to keep them.  replay_device() replays only the
+    device part (start states already in `start`), for timing."""
+
+    def __init__(self, field, n, bounds, plane_z, mass=None, charge=None, atol=1e-8, max_attempts=100_000):
+        from scipy.constants import e as qe, m_e
+        torch = B._torch()
+        dev = B.device()
+        mass = m_e if mass is None else mass
+        charge = -qe if charge is None else charge
+        self.n = int(n)
+        self.field = field
+        self.start_h = torch.empty((n, 6), dtype=torch.float64).pin_memory()
+        self.plane_h = torch.empty((n, 7), dtype=torch.float64).pin_memory()
+        self.final_h = torch.empty((n, 7), dtype=torch.float64).pin_memory()
+        self.status_h = torch.empty(n, dtype=torch.int32).pin_memory()
+        self.counters_h = torch.empty((n, 3), dtype=torch.int64).pin_memory()
+        self.start = torch.zeros((n, 6), dtype=torch.float64, device=dev)
+        self.qm = torch.full((n,), float(charge) / float(mass), dtype=torch.float64, device=dev)
+        self.status = torch.empty(n, dtype=torch.int32, device=dev)
+        self.final = torch.empty((n, 7), dtype=torch.float64, device=dev)
+        self.plane = torch.empty((n, 7), dtype=torch.float64, device=dev)
+        self.counters = torch.empty((n, 3), dtype=torch.int64, device=dev)
+        self.work = torch.empty(1, dtype=torch.int32, device=dev)
+        self.f, self.s = field._descriptor()
+        o = B.TbTraceOpts()
+        for i, v in enumerate(np.asarray(bounds, dtype=np.float64).reshape(-1)):
+            o.bounds[i] = float(v)
+        o.atol = float(atol)
+        o.plane_z = float(plane_z)
+        o.record_plane = 1
+        o.max_attempts = int(max_attempts)
+        o.max_rows = 0
+        o.team_warps = 0
+        self.o = o
+        # capture on a side stream after one eager launch (kernel attributes
+        # and the library's lazy set-up happen outside the capture)
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self._launch(side.cuda_stream)
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        self.graph_device = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph_device):
+            self._launch(torch.cuda.current_stream().cuda_stream)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.start.copy_(self.start_h, non_blocking=True)
+            self._launch(torch.cuda.current_stream().cuda_stream)
+            self.plane_h.copy_(self.plane, non_blocking=True)
+            self.final_h.copy_(self.final, non_blocking=True)
+            self.status_h.copy_(self.status, non_blocking=True)
+            self.counters_h.copy_(self.counters, non_blocking=True)
+
+    def _launch(self, stream):
+        r = _lib.tb_trace_surrogate(self.start.data_ptr(), None, self.qm.data_ptr(), self.n, C.byref(self.f),
+                                    C.byref(self.s), C.byref(self.o), self.status.data_ptr(), self.final.data_ptr(),
+                                    self.plane.data_ptr(), self.counters.data_ptr(), self.work.data_ptr(), stream)
+        if r != B.TB_OK:
+            raise B.BackendError(f'tb_trace_surrogate failed with status {r}')
+
+    @property
+    def h2d_bytes(self):
+        return self.n * 6 * 8
+
+    @property
+    def d2h_bytes(self):
+        return self.n * (7 + 7) * 8 + self.n * 4 + self.n * 3 * 8
+
+    def run(self, position, velocity):
+        torch = B._torch()
+        sh = self.start_h.numpy()
+        sh[:, :3] = position
+        sh[:, 3:] = velocity
+        self.graph.replay()
+        torch.cuda.current_stream().synchronize()
+        return self.plane_h.numpy(), self.final_h.numpy(), self.status_h.numpy(), self.counters_h.numpy()
+
+    def replay_device(self):
+        self.graph_device.replay()

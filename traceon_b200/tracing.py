@@ -82,11 +82,19 @@ class Tracer:
     def trace_device(self, start, qm, t0=None, atol=1e-8, plane_z=None, max_rows=0,
                      max_attempts=DEFAULT_MAX_ATTEMPTS, team_warps=0, stream=None):
         """Traces particles whose start states (n, 6) and charge/mass (n,) are
-        already device tensors; returns a TraceResult of device tensors."""
+        already device tensors; returns a TraceResult of device tensors.
+        team_warps: warps per particle for BEM fields (1, 2, 4, 8), 0 for the
+        built-in rule, or 'tune' for the measured choice (traceon_b200.autotune,
+        cached per device and problem size)."""
         torch = B._torch()
         n = start.shape[0]
         dev = start.device
         f, keep = self.field._trace_field()
+        if team_warps == 'tune':
+            from . import autotune
+            team_warps = 0
+            if f.axial_z is None and n:
+                team_warps = autotune.best_team_warps(self, start, qm, atol, max_attempts, f.n_elec + f.n_mag)
         o = B.TbTraceOpts()
         for i, v in enumerate(self.bounds.reshape(-1)):
             o.bounds[i] = float(v)
