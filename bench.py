@@ -270,15 +270,22 @@ def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True):
 
     B.dev_solve_mixed(A, F)
     mixed_ms, (Xm, iters, rel) = timed(lambda: B.dev_solve_mixed(A, F))
+    lib_ms = None
     if fp64_lu:
         lu64()
         lu_ms, X64 = timed(lu64)
         err = float(((Xm - X64).abs().amax(1) / X64.abs().amax(1)).max())
+        # context only: the vendor library's FP64 LU (getrf + getrs through
+        # torch.linalg.solve), not a path of this library
+        torch.linalg.solve(A, F.T)
+        lib_ms, _ = timed(lambda: torch.linalg.solve(A, F.T))
     else:  # profiling the mixed solve alone
         lu_ms, err = None, None
     out = {'workload': f'einzel lens, {n} cubic elements, {nrhs} right-hand sides (electrode voltages U[-3,3] kV)',
            'fill_fp64_ms': fill_ms, 'solve_fp64_lu_ms': lu_ms, 'solve_mixed_ms': mixed_ms,
            'mixed_iterations': iters, 'mixed_last_correction': rel, 'charges_rel_err_vs_fp64': err,
+           'solve_fp64_vendor_lu_ms': lib_ms,
+           'speedup_vs_vendor_fp64_lu': lib_ms / mixed_ms if lib_ms else None,
            'speedup_solve': lu_ms / mixed_ms if lu_ms else None,
            'speedup_fill_plus_solve': (fill_ms + lu_ms) / (fill_ms + mixed_ms) if lu_ms else None,
            'lu_flop': 2.0 / 3.0 * n ** 3}

@@ -123,3 +123,23 @@ def test_lu_nopiv_tc_factors(cuda):
     L = np.tril(LU, -1) + np.eye(700)
     U = np.triu(LU)
     assert np.abs(L @ U - S_h).max() < 2e-5 * np.abs(S_h).max()
+
+
+def test_mixed_solve_with_dielectric_rows(cuda, port):
+    """Flux (dielectric) rows in the matrix: the default mixed solve either
+    converges or falls back to the pivoted FP64 LU -- either way the charges
+    match LAPACK on the oracle's matrix to 1e-10."""
+    from traceon_b200 import geometry as G
+    from traceon_b200.excitation import Excitation, Mesh
+    from traceon_b200.solver import ElectrostaticSolverRadial
+    geo = G.einzel_lens(600)
+    exc = Excitation(Mesh.from_geometry(geo))
+    exc.add_voltage(ground_in=0.0, ground_out=800.0)
+    exc.add_dielectric(lens=4.0)
+    s = ElectrostaticSolverRadial(exc)
+    F = np.array([s.get_right_hand_side()])
+    X = s.solve_charges_device(F).cpu().numpy()[0]
+    A = port.matrix(s.vertices, s.excitation_types, s.excitation_values, threads=8)
+    q = np.linalg.solve(A, F[0])
+    assert s.solve_info['method'] in ('mixed', 'lu')
+    assert np.max(np.abs(X - q)) / np.max(np.abs(q)) < 1e-10

@@ -231,3 +231,30 @@ def test_trace_session_graph_replays(cuda, trained):
         assert (ss == 0).all() and np.array_equal(ss, status)
         assert np.array_equal(sp, plane) and np.array_equal(sf, final) and np.array_equal(sc, counters)
     assert sess.h2d_bytes == n * 48 and sess.d2h_bytes == n * (112 + 4 + 24)
+
+
+def test_surrogate_tracer_edge_cases(cuda, trained):
+    """Empty batch; particles that start outside the (inclusive) bounds end at
+    once with no step; an attempt cap of 1 ends every particle with
+    TRACE_MAX_ATTEMPTS after exactly one attempt (the reference would loop
+    until the particle leaves the bounds).  Both engines."""
+    import torch
+    from traceon_b200 import geometry as G
+    from oracle.oracle import EM
+    for engine in ('tc', 'warp'):
+        fs, _ = _fields(trained, np.array([0.0, 1500.0, 0.0]), engine)
+        empty = torch.empty((0, 6), dtype=torch.float64, device='cuda')
+        r = fs.trace_device(empty, torch.empty(0, dtype=torch.float64, device='cuda'), G.LENS_BOUNDS, 1e-10,
+                            plane_z=G.LENS_EXIT_Z)
+        assert r.status.numel() == 0
+        p0, v0 = G.surrogate_beam(130, 41)
+        p0[:5, 2] = -10.5e-3  # below z_min = -10 mm
+        plane, final, status, counters = fs.trace_endpoints(p0, v0, G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=1e-10)
+        assert (status == cuda.TRACE_EXITED).all()
+        assert (counters[:5, :2] == 0).all() and np.isnan(plane[:5, 1:]).all()
+        assert np.array_equal(final[:5, 1:4], p0[:5])
+        assert (counters[5:, 0] > 10).all()
+        plane, final, status, counters = fs.trace_endpoints(p0[5:], v0[5:], G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=1e-10,
+                                                            max_attempts=1)
+        assert (status == cuda.TRACE_MAX_ATTEMPTS).all()
+        assert (counters[:, 1] == 1).all()

@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
   for (int kc = 0; kc < nk; kc++) {
     const int b = kc & 1;
     if (kc >= 2) {  // the MMAs of chunk kc - 2 read buffer b
-      const bool w = tc::mbar_wait_bounded(&sm.mbar[b], uint32_t((kc - 2) >> 1) & 1u, GT_WAIT_CYCLES);
+      const bool w = tc::mbar_wait_warp(&sm.mbar[b], uint32_t((kc - 2) >> 1) & 1u, GT_WAIT_CYCLES);
       if (__syncthreads_or(!w)) {
         ok = false;
         break;
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
   }
   if (ok && nk > 0) {
     const int bl = (nk - 1) & 1;
-    const bool w = tc::mbar_wait_bounded(&sm.mbar[bl], uint32_t((nk - 1) >> 1) & 1u, GT_WAIT_CYCLES);
+    const bool w = tc::mbar_wait_warp(&sm.mbar[bl], uint32_t((nk - 1) >> 1) & 1u, GT_WAIT_CYCLES);
     ok = !__syncthreads_or(!w);
   }
   if (!ok) {

@@ -75,6 +75,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return true;
 }
 
+// The same wait by lane 0 of each warp only, the result broadcast to the
+// warp (all lanes must call it): a warp polls the barrier once instead of
+// 32 times, so waiting threads do not flood shared memory while the tensor
+// core reads its operands from it.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, long long max_cycles) {
+  int ok = 1;
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait_bounded(bar, parity, max_cycles) ? 1 : 0;
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
 // ---------------------------------------------------------------- fences
 // Generic-proxy shared-memory writes -> visible to the tensor core (async proxy).
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

@@ -1020,7 +1020,7 @@ struct TcEngine {
         tc_issue_layer(s, act, dtm, layer);
         tc::mma_commit(&s.mbar[g]);
       }
-      const bool ok = tc::mbar_wait_bounded(&s.mbar[g], phase, TC_WAIT_CYCLES);
+      const bool ok = tc::mbar_wait_warp(&s.mbar[g], phase, TC_WAIT_CYCLES);
       phase ^= 1u;
       if (tc::bar_any(1 + g, 128, !ok)) return false;
       tc::fence_after_sync();

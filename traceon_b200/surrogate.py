@@ -519,12 +519,13 @@ class TraceSession:
         o.max_rows = 0
         o.team_warps = 0
         self.o = o
-        # capture on a side stream after one eager launch (kernel attributes
-        # and the library's lazy set-up happen outside the capture)
+        # one eager single-particle launch first, so that the kernel
+        # attributes and the library's lazy set-up happen outside the capture
+        self.start[0, 5] = 1.0
         side = torch.cuda.Stream(device=dev)
         side.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(side):
-            self._launch(side.cuda_stream)
+            self._launch(side.cuda_stream, n=1)
         torch.cuda.current_stream().wait_stream(side)
         torch.cuda.synchronize()
         self.graph_device = torch.cuda.CUDAGraph()
@@ -539,8 +540,9 @@ class TraceSession:
             self.status_h.copy_(self.status, non_blocking=True)
             self.counters_h.copy_(self.counters, non_blocking=True)
 
-    def _launch(self, stream):
-        r = _lib.tb_trace_surrogate(self.start.data_ptr(), None, self.qm.data_ptr(), self.n, C.byref(self.f),
+    def _launch(self, stream, n=None):
+        n = self.n if n is None else n
+        r = _lib.tb_trace_surrogate(self.start.data_ptr(), None, self.qm.data_ptr(), n, C.byref(self.f),
                                     C.byref(self.s), C.byref(self.o), self.status.data_ptr(), self.final.data_ptr(),
                                     self.plane.data_ptr(), self.counters.data_ptr(), self.work.data_ptr(), stream)
         if r != B.TB_OK:
