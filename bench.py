@@ -33,6 +33,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -69,10 +70,10 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(HERE, 'gpurun_out', f'clocks_gpu{index}.csv')
+        fd, self.path = tempfile.mkstemp(prefix=f'traceon_b200_clocks_gpu{index}_', suffix='.csv')
+        os.close(fd)
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
@@ -300,7 +301,7 @@ def precision_fields(geo, charges_t, m, seed, check=64):
     """Potential and field of the first right-hand side's charges at m points
     (x = r ~ U[0, 0.9] mm, y = 0, z ~ U[-8, 8] mm), FP64 ring sums on the GPU;
     `check` of them re-evaluated by the CPU oracle (its own element
-    quadrature and the same charges) as the judge."""
+    quadrature and the same charges) as the check."""
     import torch
     from traceon_b200 import backend as B
     from oracle.oracle import Oracle
@@ -572,7 +573,7 @@ def run_gpu(args):
             'speedup_vs_plain_bem': (value / plain['value']) if plain else None,
             'cpu_baseline': cpu, 'clocks': clk.summary(),
             'accuracy': {'endpoint_err_max_nm': err_max_nm, 'endpoint_err_p99_nm': err_p99_nm,
-                         'checked_electrons': int(len(sample)), 'judge': 'CPU oracle FP64 BEM trace, Hermite crossing',
+                         'checked_electrons': int(len(sample)), 'checked_against': 'CPU oracle FP64 BEM trace, Hermite crossing',
                          'charges_rel_err': charge_err},
             'trace_stats': {'status_exited': int((status == 0).sum()),
                             'accepted_steps_mean': float(counters[:, 0].mean()),

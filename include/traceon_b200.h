@@ -277,16 +277,24 @@ int tb_pack_sources(const double *charges, const double *jac, const double *pos,
  * numpy.linalg.solve (solver.py:173). */
 int tb_lu_nopiv_f64(double *A, int64_t lda, int64_t N, tb_stream_t stream);
 int tb_lu_nopiv_f32(float *A, int64_t lda, int64_t N, tb_stream_t stream);
-/* The same FP32 factorisation with the trailing updates on the tensor cores
+/* The same FP32 factorisation with the updates on the tensor cores
  * (tcgen05, 3xTF32: TF32 head/tail split of both operands, FP32 accumulation
  * in tensor memory) and 256-column panels; err (device int) is set to 1 if a
- * bounded wait inside the tensor-core kernel ran out.  Used by
- * tb_solve_mixed. */
-int tb_lu_nopiv_f32_tc(float *A, int64_t lda, int64_t N, int *err, tb_stream_t stream);
+ * bounded wait inside a tensor-core kernel ran out.  With `work` (device
+ * scratch of tb_lu_nopiv_f32_tc_workspace(N) bytes, or NULL) the trailing
+ * updates split their operands once and stream them with bulk copies.  Used
+ * by tb_solve_mixed. */
+int64_t tb_lu_nopiv_f32_tc_workspace(int64_t N);
+int tb_lu_nopiv_f32_tc(float *A, int64_t lda, int64_t N, void *work, int64_t work_bytes, int *err,
+                       tb_stream_t stream);
 /* C (M x N, ldc) -= A (M x K, lda) . B (K x N, ldb), FP32 row-major, with
- * the 3xTF32 tensor-core kernel of tb_lu_nopiv_f32_tc (exposed for tests). */
+ * the 3xTF32 tensor-core kernels of tb_lu_nopiv_f32_tc (exposed for tests):
+ * work == NULL stages and splits the operands in every CTA; otherwise `work`
+ * (16-byte aligned, tb_gemm_tf32x3_workspace(M, N, K) bytes) receives the
+ * pre-split operands, which the GEMM streams with bulk copies. */
+int64_t tb_gemm_tf32x3_workspace(int64_t M, int64_t N, int64_t K);
 int tb_gemm_sub_tf32x3(float *C, int64_t ldc, const float *A, int64_t lda, const float *B, int64_t ldb, int64_t M,
-                       int64_t N, int64_t K, int *err, tb_stream_t stream);
+                       int64_t N, int64_t K, void *work, int64_t work_bytes, int *err, tb_stream_t stream);
 
 /* Mixed-precision solve of A x = f for the nrhs (<= 16) rows of F (nrhs, N)
  * into X (nrhs, N): FP32 LU without pivoting of A diag(c), c_j = 1 / max_i

@@ -82,8 +82,9 @@ def test_mixed_solve_reports_failure_and_solver_falls_back(cuda):
     assert _close(X, np.linalg.solve(A_h, F.cpu().numpy().T).T) < 1e-10
 
 
+@pytest.mark.parametrize('presplit', [False, True])
 @pytest.mark.parametrize('M,N,K', [(128, 256, 32), (300, 500, 256), (1000, 700, 100), (37, 9, 5)])
-def test_gemm_tf32x3_vs_fp64(cuda, M, N, K):
+def test_gemm_tf32x3_vs_fp64(cuda, M, N, K, presplit):
     """The tensor-core update C -= A B (tcgen05, 3xTF32) against FP64 numpy,
     on strided sub-matrices with sizes that are not multiples of the 128 x 256
     tile or the 32-wide K chunk: FP32-level accuracy."""
@@ -95,7 +96,7 @@ def test_gemm_tf32x3_vs_fp64(cuda, M, N, K):
     At = torch.as_tensor(big_a, device='cuda')[1:M + 1, 2:K + 2]
     Bt = torch.as_tensor(big_b, device='cuda')[1:K + 1, 3:N + 3]
     Ct = torch.as_tensor(big_c, device='cuda')
-    cuda.dev_gemm_sub_tf32x3(Ct[1:M + 1, 1:N + 1], At, Bt)
+    cuda.dev_gemm_sub_tf32x3(Ct[1:M + 1, 1:N + 1], At, Bt, presplit=presplit)
     out = Ct.cpu().numpy().astype(np.float64)
     ref = big_c.astype(np.float64)
     ref[1:M + 1, 1:N + 1] -= big_a[1:M + 1, 2:K + 2].astype(np.float64) @ big_b[1:K + 1, 3:N + 3].astype(np.float64)
@@ -117,12 +118,13 @@ def test_lu_nopiv_tc_factors(cuda):
     A_h = A.cpu().numpy()
     c = 1.0 / np.abs(A_h).max(axis=0)
     S_h = (A_h * c).astype(np.float32)
-    S = torch.as_tensor(S_h, device='cuda')
-    cuda.dev_lu_nopiv_tc(S)
-    LU = S.cpu().numpy().astype(np.float64)
-    L = np.tril(LU, -1) + np.eye(700)
-    U = np.triu(LU)
-    assert np.abs(L @ U - S_h).max() < 2e-5 * np.abs(S_h).max()
+    for presplit in (False, True):
+        S = torch.as_tensor(S_h, device='cuda')
+        cuda.dev_lu_nopiv_tc(S, presplit=presplit)
+        LU = S.cpu().numpy().astype(np.float64)
+        L = np.tril(LU, -1) + np.eye(700)
+        U = np.triu(LU)
+        assert np.abs(L @ U - S_h).max() < 2e-5 * np.abs(S_h).max()
 
 
 def test_mixed_solve_with_dielectric_rows(cuda, port):

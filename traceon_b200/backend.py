@@ -220,10 +220,10 @@ _DEV = {
     'tb_probe_math': (vp, i64, C.c_int, vp, vp),
     'tb_lu_nopiv_f64': (vp, i64, i64, vp),
     'tb_lu_nopiv_f32': (vp, i64, i64, vp),
-    'tb_lu_nopiv_f32_tc': (vp, i64, i64, vp, vp),
+    'tb_lu_nopiv_f32_tc': (vp, i64, i64, vp, i64, vp, vp),
     'tb_fill_matrix_radial_batched': (vp, C.c_int, i64, vp),
     'tb_self_integrals_batched': (vp, C.c_int, i64, vp),
-    'tb_gemm_sub_tf32x3': (vp, i64, vp, i64, vp, i64, i64, i64, i64, vp, vp),
+    'tb_gemm_sub_tf32x3': (vp, i64, vp, i64, vp, i64, i64, i64, i64, vp, i64, vp, vp),
     'tb_solve_mixed': (vp, i64, i64, vp, vp, i64, vp, i64, C.c_int, dbl, C.POINTER(C.c_int), C.POINTER(dbl), vp),
 }
 for _name, _args in _DEV.items():
@@ -647,25 +647,36 @@ def dev_lu_nopiv(A):
     _call(name, _ptr(A), A.stride(0), A.shape[0], _stream())
 
 
-def dev_lu_nopiv_tc(A):
-    """In-place FP32 LU without pivoting, trailing updates on the tensor
-    cores (3xTF32)."""
+backend_lib.tb_lu_nopiv_f32_tc_workspace.restype = i64
+backend_lib.tb_lu_nopiv_f32_tc_workspace.argtypes = [i64]
+backend_lib.tb_gemm_tf32x3_workspace.restype = i64
+backend_lib.tb_gemm_tf32x3_workspace.argtypes = [i64, i64, i64]
+
+
+def dev_lu_nopiv_tc(A, presplit=True):
+    """In-place FP32 LU without pivoting, updates on the tensor cores
+    (3xTF32); presplit: trailing updates from pre-split operands."""
     torch = _torch()
+    N = A.shape[0]
     err = torch.zeros(1, dtype=torch.int32, device=A.device)
-    _call('tb_lu_nopiv_f32_tc', _ptr(A), A.stride(0), A.shape[0], _ptr(err), _stream())
+    nbytes = backend_lib.tb_lu_nopiv_f32_tc_workspace(N) if presplit else 0
+    work = torch.empty(nbytes, dtype=torch.uint8, device=A.device) if nbytes else None
+    _call('tb_lu_nopiv_f32_tc', _ptr(A), A.stride(0), N, _ptr(work), nbytes, _ptr(err), _stream())
     if int(err.item()):
-        raise BackendError('tb_lu_nopiv_f32_tc: a bounded wait in the tensor-core kernel ran out')
+        raise BackendError('tb_lu_nopiv_f32_tc: a bounded wait in a tensor-core kernel ran out')
 
 
-def dev_gemm_sub_tf32x3(C, A, B):
+def dev_gemm_sub_tf32x3(C, A, B, presplit=False):
     """C -= A @ B (FP32 device matrices, unit column stride) on the tensor
-    cores with 3xTF32."""
+    cores with 3xTF32; presplit: the bulk-copy GEMM on pre-split operands."""
     torch = _torch()
     M, K = A.shape
     N = B.shape[1]
     err = torch.zeros(1, dtype=torch.int32, device=C.device)
-    _call('tb_gemm_sub_tf32x3', _ptr(C), C.stride(0), _ptr(A), A.stride(0), _ptr(B), B.stride(0), M, N, K, _ptr(err),
-          _stream())
+    nbytes = backend_lib.tb_gemm_tf32x3_workspace(M, N, K) if presplit else 0
+    work = torch.empty(nbytes, dtype=torch.uint8, device=C.device) if nbytes else None
+    _call('tb_gemm_sub_tf32x3', _ptr(C), C.stride(0), _ptr(A), A.stride(0), _ptr(B), B.stride(0), M, N, K, _ptr(work),
+          nbytes, _ptr(err), _stream())
     if int(err.item()):
         raise BackendError('tb_gemm_sub_tf32x3: a bounded wait in the tensor-core kernel ran out')
 

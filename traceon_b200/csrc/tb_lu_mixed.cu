@@ -489,13 +489,226 @@ static int gemm_sub_tf32x3(float* C, int64_t ldc, const float* A, int64_t lda, c
   return launch_status();
 }
 
+// ---------------------------------------------------------------- pre-split operands
+// For the large updates the operands are split once, not per CTA: A (M x K)
+// and B (K x N) FP32 become TF32 head / tail blocks already in the
+// tensor-core operand layout -- A block (mb, kc) = [head atom | tail atom] of
+// 128 rows x 32 k (16 KB each), B block (nb, kc) = [head | tail] of 256 rows
+// (n) x 32 k (32 KB each); rows or k beyond the matrix are zero.  The GEMM
+// below then moves whole blocks into shared memory with asynchronous bulk
+// copies (cp.async.bulk, completion counted on an mbarrier).
+constexpr uint32_t PA_BLOCK = 2u * GT_M * 128u;  // 32 KB
+constexpr uint32_t PB_BLOCK = 2u * GT_N * 128u;  // 64 KB
+
+__device__ __forceinline__ void st_global_v4(uint8_t* p, const float (&v)[4]) {
+  *reinterpret_cast<uint4*>(p) =
+      make_uint4(__float_as_uint(v[0]), __float_as_uint(v[1]), __float_as_uint(v[2]), __float_as_uint(v[3]));
+}
+
+__global__ void __launch_bounds__(256) k_split_a(const float* __restrict__ A, int64_t lda, int64_t M, int K,
+                                                uint8_t* __restrict__ out) {
+  const int nk = (K + GT_K - 1) / GT_K;
+  const int kc = blockIdx.x;
+  const int64_t mb = blockIdx.y;
+  uint8_t* blk = out + (mb * nk + kc) * (int64_t)PA_BLOCK;
+  for (int it = threadIdx.x; it < GT_M * 8; it += blockDim.x) {
+    const int r = it >> 3, kq = it & 7;
+    const int64_t gr = mb * GT_M + r;
+    const int k = kc * GT_K + 4 * kq;
+    float h[4], l[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) split_tf32((gr < M && k + u < K) ? A[gr * lda + k + u] : 0.f, h[u], l[u]);
+    st_global_v4(blk + tc::sw128(r, kq), h);
+    st_global_v4(blk + GT_M * 128 + tc::sw128(r, kq), l);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_split_b(const float* __restrict__ B, int64_t ldb, int K, int64_t N,
+                                                uint8_t* __restrict__ out) {
+  const int nk = (K + GT_K - 1) / GT_K;
+  const int kc = blockIdx.x;
+  const int64_t nb = blockIdx.y;
+  uint8_t* blk = out + (nb * nk + kc) * (int64_t)PB_BLOCK;
+  const int n = threadIdx.x;  // 256 threads: one column each, coalesced along n
+  const int64_t gn = nb * GT_N + n;
+#pragma unroll
+  for (int kq = 0; kq < 8; kq++) {
+    float h[4], l[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int k = kc * GT_K + 4 * kq + u;
+      split_tf32((k < K && gn < N) ? B[(int64_t)k * ldb + gn] : 0.f, h[u], l[u]);
+    }
+    st_global_v4(blk + tc::sw128(n, kq), h);
+    st_global_v4(blk + GT_N * 128 + tc::sw128(n, kq), l);
+  }
+}
+
+struct GemmPreSmem {
+  uint8_t a[2][PA_BLOCK];
+  uint8_t b[2][PB_BLOCK];
+  uint64_t full[2], empty[2];
+  uint32_t tmem_base;
+  int fail;
+};
+constexpr int GP_SMEM_BYTES = int(sizeof(GemmPreSmem)) + 1024;
+
+// C (M x Nc) -= A B from pre-split blocks: warp 0 lane 0 streams the K
+// chunks into two shared-memory stages with bulk copies (waiting for a stage
+// to be released by the MMAs two chunks back), warp 1 lane 0 issues the 3 x 4
+// MMAs of each chunk once its copies have landed and releases the stage with
+// tcgen05.commit; then all 8 warps drain the accumulator as in
+// k_gemm_sub_tf32x3.  Every wait is bounded.
+__global__ void __launch_bounds__(GT_THREADS, 1)
+    k_gemm_sub_pre(float* __restrict__ C, int64_t ldc, const uint8_t* __restrict__ Apre,
+                   const uint8_t* __restrict__ Bpre, int64_t M, int64_t Nc, int nk, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char gp_raw[];
+  const uint32_t raw = tc::smem_u32(gp_raw);
+  GemmPreSmem& sm = *reinterpret_cast<GemmPreSmem*>(gp_raw + (((raw + 1023u) & ~1023u) - raw));
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int64_t mb = blockIdx.y, nb = blockIdx.x;
+  const int64_t m0 = mb * GT_M, n0 = nb * GT_N;
+  if (tid < 2) {
+    tc::mbar_init(&sm.full[tid], 1);
+    tc::mbar_init(&sm.empty[tid], 1);
+  }
+  if (tid == 0) {
+    sm.fail = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(&sm.tmem_base, GT_N);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t dtm = sm.tmem_base;
+  constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(GT_N >> 3) << 17) |
+                             (uint32_t(GT_M >> 4) << 24);
+  const uint8_t* Ab = Apre + mb * nk * (int64_t)PA_BLOCK;
+  const uint8_t* Bb = Bpre + nb * nk * (int64_t)PB_BLOCK;
+  if (warp == 0) {
+    if (lane == 0) {  // producer
+      for (int kc = 0; kc < nk; kc++) {
+        const int st = kc & 1;
+        if (kc >= 2 && !tc::mbar_wait_bounded(&sm.empty[st], uint32_t((kc - 2) >> 1) & 1u, GT_WAIT_CYCLES)) {
+          sm.fail = 1;
+          break;
+        }
+        tc::mbar_arrive_expect_tx(&sm.full[st], PA_BLOCK + PB_BLOCK);
+        const uint32_t da = tc::smem_u32(sm.a[st]), db = tc::smem_u32(sm.b[st]);
+        for (uint32_t o = 0; o < PA_BLOCK; o += 16384u)
+          tc::bulk_copy_g2s(da + o, Ab + kc * (int64_t)PA_BLOCK + o, 16384u, &sm.full[st]);
+        for (uint32_t o = 0; o < PB_BLOCK; o += 16384u)
+          tc::bulk_copy_g2s(db + o, Bb + kc * (int64_t)PB_BLOCK + o, 16384u, &sm.full[st]);
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      for (int kc = 0; kc < nk; kc++) {
+        const int st = kc & 1;
+        if (!tc::mbar_wait_bounded(&sm.full[st], uint32_t(kc >> 1) & 1u, GT_WAIT_CYCLES)) {
+          sm.fail = 1;
+          break;
+        }
+        tc::fence_after_sync();
+        const uint32_t ah = tc::smem_u32(sm.a[st]), al = ah + GT_M * 128;
+        const uint32_t bh = tc::smem_u32(sm.b[st]), bl = bh + GT_N * 128;
+#pragma unroll
+        for (int ks = 0; ks < GT_K / 8; ks++) {
+          const uint64_t dah = tc::desc_sw128(ah + 32 * ks), dal = tc::desc_sw128(al + 32 * ks);
+          const uint64_t dbh = tc::desc_sw128(bh + 32 * ks), dbl = tc::desc_sw128(bl + 32 * ks);
+          mma_tf32(dtm, dal, dbh, IDESC, (kc > 0 || ks > 0) ? 1u : 0u);
+          mma_tf32(dtm, dah, dbl, IDESC, 1u);
+          mma_tf32(dtm, dah, dbh, IDESC, 1u);
+        }
+        tc::mma_commit(&sm.empty[st]);
+      }
+    }
+    __syncwarp();
+  }
+  bool ok = tc::mbar_wait_warp(&sm.empty[(nk - 1) & 1], uint32_t((nk - 1) >> 1) & 1u, GT_WAIT_CYCLES);
+  ok = !__syncthreads_or(!ok || sm.fail);
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+  } else {
+    tc::fence_after_sync();
+    const int row = 32 * (warp % 4) + lane;
+    const int64_t gr = m0 + row;
+    const uint32_t tbase = dtm + (uint32_t(32 * (warp % 4)) << 16) + uint32_t(128 * (warp / 4));
+    const bool vec = (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(C) % 16 == 0);
+#pragma unroll 1
+    for (int c = 0; c < 8; c++) {
+      uint32_t v[16];
+      tc::tmem_ld16(tbase + 16 * c, v);
+      tc::tmem_wait_ld16(v);
+      const int64_t col0 = n0 + 128 * (warp / 4) + 16 * c;
+      if (gr < M && col0 < Nc) {
+        float* crow = C + gr * ldc + col0;
+        if (vec && col0 + 16 <= Nc) {
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            float4 x = *reinterpret_cast<float4*>(crow + 4 * q);
+            x.x -= __uint_as_float(v[4 * q]);
+            x.y -= __uint_as_float(v[4 * q + 1]);
+            x.z -= __uint_as_float(v[4 * q + 2]);
+            x.w -= __uint_as_float(v[4 * q + 3]);
+            *reinterpret_cast<float4*>(crow + 4 * q) = x;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; j++)
+            if (col0 + j < Nc) crow[j] -= __uint_as_float(v[j]);
+        }
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(dtm, GT_N);
+  }
+}
+
+// Workspace of the pre-split GEMM for an M x N x K update.
+static int64_t gemm_pre_bytes(int64_t M, int64_t N, int64_t K) {
+  const int64_t nk = (K + GT_K - 1) / GT_K;
+  return ((M + GT_M - 1) / GT_M) * nk * PA_BLOCK + ((N + GT_N - 1) / GT_N) * nk * PB_BLOCK;
+}
+
+static bool g_attr_gemm_pre[64];
+
+static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, const float* B, int64_t ldb, int64_t M,
+                        int64_t Nc, int K, uint8_t* work, int* err, cudaStream_t s) {
+  if (M <= 0 || Nc <= 0 || K <= 0) return OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return CUDA_ERR;
+  if (dev >= 0 && dev < 64 && !g_attr_gemm_pre[dev]) {
+    if (cudaFuncSetAttribute(k_gemm_sub_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, GP_SMEM_BYTES) !=
+        cudaSuccess)
+      return CUDA_ERR;
+    g_attr_gemm_pre[dev] = true;
+  }
+  const int nk = (K + GT_K - 1) / GT_K;
+  const int64_t mbk = (M + GT_M - 1) / GT_M, nbk = (Nc + GT_N - 1) / GT_N;
+  uint8_t* pa = work;
+  uint8_t* pb = work + mbk * nk * (int64_t)PA_BLOCK;
+  k_split_a<<<dim3(unsigned(nk), unsigned(mbk)), 256, 0, s>>>(A, lda, M, K, pa);
+  k_split_b<<<dim3(unsigned(nk), unsigned(nbk)), 256, 0, s>>>(B, ldb, K, Nc, pb);
+  k_gemm_sub_pre<<<dim3(unsigned(nbk), unsigned(mbk)), GT_THREADS, GP_SMEM_BYTES, s>>>(C, ldc, pa, pb, M, Nc, nk, err);
+  return launch_status();
+}
+
 // FP32 LU without pivoting, two-level blocked: panels of 256 columns are
 // factored with the 64-wide kernels above (diagonal block, triangular
 // solves) and tensor-core updates (K = 64) inside the panel and its row
 // block; the trailing matrix is updated once per panel on the tensor cores
 // (K = 256).  err receives 1 if a tensor-core wait ran out.
 constexpr int TC_PANEL = 256;
-static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, cudaStream_t s) {
+static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* work, cudaStream_t s) {
   for (int64_t p0 = 0; p0 < N; p0 += TC_PANEL) {
     const int64_t pe = p0 + TC_PANEL < N ? p0 + TC_PANEL : N;
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
@@ -523,8 +736,10 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, cudaStrea
         if (st != OK) return st;
       }
     }
-    const int st = gemm_sub_tf32x3(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest,
-                                   int(pe - p0), err, s);
+    const int st = work ? gemm_sub_pre(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest,
+                                       rest, int(pe - p0), work, err, s)
+                        : gemm_sub_tf32x3(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda,
+                                          rest, rest, int(pe - p0), err, s);
     if (st != OK) return st;
   }
   return launch_status();
@@ -855,17 +1070,35 @@ extern "C" int tb_lu_nopiv_f32(float* A, int64_t lda, int64_t N, tb_stream_t str
 
 static int64_t round256(int64_t b) { return (b + 255) / 256 * 256; }
 
-extern "C" int tb_lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, tb_stream_t stream) {
+extern "C" int64_t tb_gemm_tf32x3_workspace(int64_t M, int64_t N, int64_t K) {
+  if (M <= 0 || N <= 0 || K <= 0) return 0;
+  return gemm_pre_bytes(M, N, K);
+}
+
+extern "C" int64_t tb_lu_nopiv_f32_tc_workspace(int64_t N) {
+  if (N <= 0) return 0;
+  return gemm_pre_bytes(N, N, TC_PANEL);
+}
+
+extern "C" int tb_lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, void* work, int64_t work_bytes, int* err,
+                                  tb_stream_t stream) {
   if (N < 0 || lda < N || (N > 0 && (!A || !err)) || N > 0x7fffffff) return BAD_ARG;
   if (N == 0) return OK;
-  return lu_nopiv_f32_tc(A, lda, N, err, (cudaStream_t)stream);
+  if (work && work_bytes < tb_lu_nopiv_f32_tc_workspace(N)) return BAD_ARG;
+  return lu_nopiv_f32_tc(A, lda, N, err, static_cast<uint8_t*>(work), (cudaStream_t)stream);
 }
 
 extern "C" int tb_gemm_sub_tf32x3(float* C, int64_t ldc, const float* A, int64_t lda, const float* B, int64_t ldb,
-                                  int64_t M, int64_t N, int64_t K, int* err, tb_stream_t stream) {
+                                  int64_t M, int64_t N, int64_t K, void* work, int64_t work_bytes, int* err,
+                                  tb_stream_t stream) {
   if (M < 0 || N < 0 || K < 0 || K > 0x7fffffff || !err) return BAD_ARG;
   if (M == 0 || N == 0 || K == 0) return OK;
   if (!C || !A || !B || ldc < N || lda < K || ldb < N) return BAD_ARG;
+  if (work) {
+    if (work_bytes < gemm_pre_bytes(M, N, K) || reinterpret_cast<uintptr_t>(work) % 16 != 0) return BAD_ARG;
+    return gemm_sub_pre(C, ldc, A, lda, B, ldb, M, N, int(K), static_cast<uint8_t*>(work), err,
+                        (cudaStream_t)stream);
+  }
   return gemm_sub_tf32x3(C, ldc, A, lda, B, ldb, M, N, int(K), err, (cudaStream_t)stream);
 }
 
@@ -876,7 +1109,7 @@ extern "C" int64_t tb_solve_mixed_workspace(int64_t N, int64_t nrhs) {
   // maxima, inverses of the diagonal blocks of both factors, sweep flags and
   // the error word
   return round256(N * N * 4) + round256(N * 8) + round256(nrhs * N * 8) + 256 +
-         2 * round256(nblk * TS_B * TS_B * 8) + round256(nblk * 4) + 256;
+         2 * round256(nblk * TS_B * TS_B * 8) + round256(nblk * 4) + 256 + round256(gemm_pre_bytes(N, N, TC_PANEL));
 }
 
 extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const double* F, double* X, int64_t nrhs,
@@ -903,11 +1136,13 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   int* flags = reinterpret_cast<int*>(w);
   w += round256(nblk * 4);
   int* err = reinterpret_cast<int*>(w);
+  w += 256;
+  uint8_t* gemm_work = reinterpret_cast<uint8_t*>(w);  // pre-split operands of the trailing updates
 
   k_col_maxabs<<<unsigned((N + 31) / 32), 256, 0, s>>>(A, lda, N, c);
   k_scale_to_f32<<<unsigned((N * N + 255) / 256), 256, 0, s>>>(A, lda, c, S, N);
   if (cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) return CUDA_ERR;
-  int st = lu_nopiv_f32_tc(S, N, N, err, s);
+  int st = lu_nopiv_f32_tc(S, N, N, err, gemm_work, s);
   if (st != OK) return st;
   k_diag_inverse<true><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_l);
   k_diag_inverse<false><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_u);

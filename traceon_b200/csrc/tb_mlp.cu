@@ -1,7 +1,7 @@
 // tb_mlp.cu -- the learned field surrogate: a small MLP (4 hidden layers of
 // 128, SiLU) trained on the GPU from BEM samples, in BF16 with FP32
 // accumulation.  No reference counterpart (the reference has no learned
-// part); its judge is the FP64 BEM field of tb_bem.cu.
+// part); it is checked against the FP64 BEM field of tb_bem.cu.
 //
 // Kernels:
 //   k_gemm_bf16<AT, BT>  C[M x N] (fp32) = A[M x K] . B[N x K]^T on the tensor

@@ -85,6 +85,23 @@ __device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, l
   return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
+// Arrive once on `bar` and add tx_bytes to the transaction count the current
+// phase waits for (the bytes of bulk copies that complete on it).
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t tx_bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(tx_bytes)
+               : "memory");
+}
+
+// Asynchronous bulk copy global -> this CTA's shared memory (no multicast),
+// completing `bytes` of transactions on `bar`.  Both addresses 16-byte
+// aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst_smem, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_smem),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // ---------------------------------------------------------------- fences
 // Generic-proxy shared-memory writes -> visible to the tensor core (async proxy).
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

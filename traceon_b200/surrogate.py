@@ -18,8 +18,8 @@ tracer falls back to the exact BEM sum.
 Training data come from the GPU BEM evaluator itself (tb_field_radial_points)
 and the GPU axial series (tb_axial_field_points); the network is trained on
 the GPU by this library's BF16 / FP32-accumulate kernels (tb_mlp_*), with
-Adam on FP32 master weights.  There is no reference counterpart; the judge
-of the surrogate is the FP64 BEM field and the FP64 BEM trace.
+Adam on FP32 master weights.  There is no reference counterpart; the
+surrogate is checked against the FP64 BEM field and the FP64 BEM trace.
 """
 from __future__ import annotations
 
