@@ -523,7 +523,8 @@ def run_gpu(args):
         achieved = evals * MLP_FLOP_PER_EVAL / launch_s / 1e12
         peak = peaks.get('bf16_tflops')
         roof = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
-                'frac': achieved / peak if peak else None, 'traffic': args.traffic,
+                'frac': achieved / peak if peak else None,
+                'traffic': args.traffic if args.engine == 'tc' else None, 'traffic_unit': 'bytes per launch (ncu)',
                 'kernel': 'k_trace_surrogate_tc' if args.engine == 'tc' else 'k_trace_surrogate',
                 'flop_per_unit': MLP_FLOP_PER_EVAL, 'units_per_launch': evals,
                 'unit_desc': 'network evaluations (dense BF16 flops of the 16-128x4-16 MLP)',
@@ -535,7 +536,7 @@ def run_gpu(args):
         pairs_per_launch = np.mean(attempts) * 6 * Nq
         achieved = pairs_per_launch * args.flop_per_pair / launch_s / 1e12
         roof = {'bound': 'fp64', 'achieved': achieved, 'peak': fp64_peak, 'unit': 'TFLOP/s',
-                'frac': achieved / fp64_peak if fp64_peak else None, 'traffic': args.traffic, 'kernel': 'k_trace_bem',
+                'frac': achieved / fp64_peak if fp64_peak else None, 'traffic': None, 'kernel': 'k_trace_bem',
                 'flop_per_unit': args.flop_per_pair, 'units_per_launch': pairs_per_launch,
                 'unit_desc': 'ring-pair field evaluations (executed FP64 flops per pair, ncu)',
                 'peak_source': 'measured FP64 FMA probe (tb_probe_fp64_fma) in this run'}
@@ -626,7 +627,10 @@ def main():
     # executed FP64 flops per ring-pair evaluation of the tracer's field sum
     # (dadd + dmul + 2 dfma per pair, from the ncu instruction counts)
     ap.add_argument('--flop-per-pair', type=float, default=162.0)
-    ap.add_argument('--traffic', type=float, default=None)
+    # DRAM bytes (read + write) of one full-size launch of the dominant kernel
+    # from an ncu capture of this workload (k_trace_surrogate_tc: 18.67 MB read
+    # + 4.96 MB written; see the profile summary of that kernel)
+    ap.add_argument('--traffic', type=float, default=23.63e6)
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
