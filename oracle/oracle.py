@@ -424,6 +424,21 @@ def axial_coefficients(z, derivs):
     return c
 
 
+def focus_position(positions):
+    """traceon/focus.py:9-42, the same least-squares system solved by the
+    same numpy.linalg.lstsq call: positions is a list of (N, 6)
+    trajectories; returns (x, y, z)."""
+    angles_x = np.array([p[-1, 3] / p[-1, 5] for p in positions])
+    angles_y = np.array([p[-1, 4] / p[-1, 5] for p in positions])
+    x, y, z = [np.array([p[-1, i] for p in positions]) for i in (0, 1, 2)]
+    n = len(positions)
+    a = np.array([np.concatenate((-angles_x, -angles_y)), np.concatenate((np.ones(n), np.zeros(n))),
+                  np.concatenate((np.zeros(n), np.ones(n)))]).T
+    rhs = np.concatenate((x - z * angles_x, y - z * angles_y))
+    zf, xf, yf = np.linalg.lstsq(a, rhs, rcond=None)[0]
+    return np.array([xf, yf, zf])
+
+
 def hermite_plane_crossing(times, states, z_plane):
     """Crossing of the plane z = z_plane by cubic Hermite interpolation of
     position between the two accepted states that bracket it (position and

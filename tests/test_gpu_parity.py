@@ -398,3 +398,28 @@ def test_autotuned_team_size(cuda, port):
         t, s = port.trace_bem(p0[i], v0[i], EM, q, jac, pos, G.LENS_BOUNDS, 1e-10)
         h = hermite_plane_crossing(t, s, G.LENS_EXIT_Z)
         assert np.max(np.abs(plane[i, 1:4] - h[:3])) < 1e-12
+
+
+def test_current_rings_vs_oracle(cuda, port):
+    """Current-ring field (radial.c:55-83) at many points through the device
+    API and the compat entry point, and the current rings' axial derivatives
+    (radial.c:85-103), against the oracle."""
+    import torch
+    from test_oracle import _coil_rings
+    I, jac, pos = _coil_rings(5, n=40)
+    rng = np.random.default_rng(6)
+    M = 300
+    pts = np.stack([rng.uniform(0, 2e-3, M), rng.uniform(-1e-3, 1e-3, M), rng.uniform(-8e-3, 8e-3, M)], 1)
+    src = cuda.dev_pack_current_sources(cuda.to_dev(I, torch.float64), cuda.to_dev(jac, torch.float64),
+                                        cuda.to_dev(pos, torch.float64))
+    H = cuda.dev_current_field_points(cuda.to_dev(pts, torch.float64), src).cpu().numpy()
+    H_or = np.array([port.current_field_radial(p, I, jac, pos) for p in pts])
+    assert np.max(np.abs(H - H_or)) < 1e-11 * np.max(np.abs(H_or))
+    for p in pts[:5]:
+        h = cuda.current_field_radial(p, I, jac, pos)
+        assert np.max(np.abs(h - port.current_field_radial(p, I, jac, pos))) < 1e-11 * np.max(np.abs(H_or))
+    z = np.linspace(-8e-3, 8e-3, 101)
+    d = cuda.dev_axial_derivatives(cuda.to_dev(z, torch.float64), src, current=True).cpu().numpy()
+    d_or = port.current_axial_derivatives_radial(z, I, jac, pos)
+    for c in range(d_or.shape[1]):
+        assert np.max(np.abs(d[:, c] - d_or[:, c])) < 1e-10 * np.max(np.abs(d_or[:, c]))

@@ -145,3 +145,34 @@ def test_mixed_solve_with_dielectric_rows(cuda, port):
     q = np.linalg.solve(A, F[0])
     assert s.solve_info['method'] in ('mixed', 'lu')
     assert np.max(np.abs(X - q)) / np.max(np.abs(q)) < 1e-10
+
+
+def test_magnetostatic_solve_with_current_rings(cuda, port):
+    """MagnetostaticSolverRadial (solver.py:267-353): a magnetizable tube
+    (mu_r = 1000) in the field of coil current rings.  The right-hand side
+    -factor(mu) H_coil . n (solver.py:128-144) and the charges against the
+    oracle: coil field by the oracle's current_field_radial, matrix by the
+    oracle's fill of the flux rows, LAPACK solve."""
+    from traceon_b200 import geometry as G
+    from traceon_b200 import backend as B
+    from traceon_b200.excitation import Excitation, Mesh
+    from traceon_b200.field import EffectivePointCharges
+    from traceon_b200.solver import MagnetostaticSolverRadial
+    from test_oracle import _coil_rings
+    geo = G.einzel_lens(300)
+    exc = Excitation(Mesh.from_geometry(geo))
+    exc.add_magnetizable(lens=1000.0)
+    I, jac, pos = _coil_rings(7, n=30)
+    s = MagnetostaticSolverRadial(exc, current_point_charges=EffectivePointCharges(I, jac, pos))
+    F = s.get_right_hand_side()
+    normals = s.get_normal_vectors()
+    F_or = np.zeros(len(F))
+    for i in range(len(F)):
+        H = port.current_field_radial(s.get_center_of_element(i), I, jac, pos)
+        F_or[i] = -B.flux_density_to_charge_factor(s.excitation_values[i]) * (H[0] * normals[i][0] + H[2] * normals[i][1])
+    assert np.max(np.abs(F - F_or)) < 1e-11 * np.max(np.abs(F_or))
+    field = s.solve_matrix()[0]
+    A = port.matrix(s.vertices, s.excitation_types, s.excitation_values, threads=8)
+    q = np.linalg.solve(A, F_or)
+    got = field.magnetostatic_point_charges.charges
+    assert np.max(np.abs(got - q)) / np.max(np.abs(q)) < 1e-10

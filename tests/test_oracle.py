@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import golden
-from oracle.oracle import Oracle, axial_coefficients, solve, EM, hermite_plane_crossing
+from oracle.oracle import Oracle, axial_coefficients, solve, EM, hermite_plane_crossing, focus_position
 
 
 def rel(a, b, floor=0.0):
@@ -156,6 +156,33 @@ def test_hermite_crossing_exact_on_cubic():
     assert abs(out[2] - zp) < 1e-15
 
 
+def _focus_beams():
+    """The beams of the reference's focus tests (tests/test_focus.py:10-43)
+    with the focus each one pins."""
+    from traceon_b200.tracing import velocity_vec, velocity_vec_spherical
+    v1, v2 = velocity_vec(10, [-1e-3, 0., -1]), velocity_vec(10, [1e-3, 0., -1])
+    p1 = np.concatenate((3 * v1, v1))[np.newaxis, :]
+    p2 = np.concatenate((3 * v2, v2))[np.newaxis, :]
+    cases = [([p1.copy(), p2.copy()], [0, 0, 0])]
+    p1[0, 0] += 1
+    p2[0, 0] += 1
+    cases.append(([p1.copy(), p2.copy()], [1, 0, 0]))
+    for p in (p1, p2):
+        p[0, 1] += 1
+        p[0, 2] += 1
+    cases.append(([p1.copy(), p2.copy()], [1, 1, 1]))
+    w1, w2, w3 = (velocity_vec_spherical(1, 0, 0), velocity_vec_spherical(5, 1 / 30, 1 / 30),
+                  velocity_vec_spherical(10, 1 / 30, np.pi / 2))
+    cases.append(([np.concatenate((w, w))[np.newaxis, :] for w in (w1, w2, w3)], [0, 0, 0]))
+    return cases
+
+
+def test_focus_known_answers():
+    """The oracle's focus_position against the reference's focus tests."""
+    for beams, expected in _focus_beams():
+        assert np.allclose(focus_position(beams), expected)
+
+
 def test_oracle_vs_reference_build(port, ref):
     """The restatement against the reference compiled from its sources."""
     from traceon_b200.geometry import einzel_lens
@@ -188,3 +215,31 @@ def test_diagonal_converged_vs_shipped_call(port, ref):
     r = np.abs(acc - shipped) / np.abs(acc)
     assert np.median(r) < 1e-13
     assert r.max() < 1e-4
+
+
+def _coil_rings(seed, n=20):
+    """Synthetic coil cross-section quadrature: n triangles in r in [3, 6] mm,
+    z in [-1, 1] mm, 12 points each (y = 0), weights = area / 12; currents
+    U[0.5, 5] kA-turns spread over the triangles."""
+    rng = np.random.default_rng(seed)
+    pos = np.zeros((n, 12, 3))
+    pos[:, :, 0] = rng.uniform(3e-3, 6e-3, (n, 12))
+    pos[:, :, 2] = rng.uniform(-1e-3, 1e-3, (n, 12))
+    jac = np.full((n, 12), 1e-8 / 12)
+    I = rng.uniform(500.0, 5000.0, n) / n
+    return I, jac, pos
+
+
+def test_current_rings_vs_reference_build(port, ref):
+    """current_field_radial (radial.c:55-83) and current_axial_derivatives_radial
+    (radial.c:85-103): the oracle's restatement against the reference build."""
+    I, jac, pos = _coil_rings(3)
+    rng = np.random.default_rng(4)
+    pts = np.stack([rng.uniform(0, 2e-3, 30), rng.uniform(-1e-3, 1e-3, 30), rng.uniform(-8e-3, 8e-3, 30)], 1)
+    for p in pts:
+        a, b = port.current_field_radial(p, I, jac, pos), ref.current_field_radial(p, I, jac, pos)
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
+    z = np.linspace(-8e-3, 8e-3, 41)
+    a, b = port.current_axial_derivatives_radial(z, I, jac, pos), ref.current_axial_derivatives_radial(z, I, jac, pos)
+    for c in range(b.shape[1]):
+        assert np.max(np.abs(a[:, c] - b[:, c])) <= 1e-11 * np.max(np.abs(b[:, c]))
