@@ -277,13 +277,14 @@ int tb_pack_sources(const double *charges, const double *jac, const double *pos,
  * numpy.linalg.solve (solver.py:173). */
 int tb_lu_nopiv_f64(double *A, int64_t lda, int64_t N, tb_stream_t stream);
 int tb_lu_nopiv_f32(float *A, int64_t lda, int64_t N, tb_stream_t stream);
-/* The same FP32 factorisation with the updates on the tensor cores
+/* The same FP32 factorisation in 256-column panels: each 64-column step of
+ * a panel in two launches (diagonal LU with the inverses of its triangles,
+ * then the rows below), the trailing matrix updated on the tensor cores
  * (tcgen05, 3xTF32: TF32 head/tail split of both operands, FP32 accumulation
- * in tensor memory) and 256-column panels; err (device int) is set to 1 if a
- * bounded wait inside a tensor-core kernel ran out.  With `work` (device
- * scratch of tb_lu_nopiv_f32_tc_workspace(N) bytes, or NULL) the trailing
- * updates split their operands once and stream them with bulk copies.  Used
- * by tb_solve_mixed. */
+ * in tensor memory).  work: device scratch of
+ * tb_lu_nopiv_f32_tc_workspace(N) bytes, 16-byte aligned (required).  err
+ * (device int) is set to 1 if a bounded wait inside a tensor-core kernel ran
+ * out.  Used by tb_solve_mixed. */
 int64_t tb_lu_nopiv_f32_tc_workspace(int64_t N);
 int tb_lu_nopiv_f32_tc(float *A, int64_t lda, int64_t N, void *work, int64_t work_bytes, int *err,
                        tb_stream_t stream);
@@ -403,6 +404,28 @@ typedef struct {
 int tb_trace_rk45(const double *start, const double *t0, const double *qm, int64_t n, const tb_field_t *field,
                   const tb_trace_opts_t *opts, double *rows, int64_t *nrows, int32_t *status, double *final_state,
                   double *plane, int64_t *counters, int32_t *work, tb_stream_t stream);
+
+/* Plane crossings of trajectories stored by tb_trace_rk45 (device arrays):
+ * per trajectory the crossing nearest its end, by linear interpolation, as
+ * plane_intersection (traceon/backend/tracing.c:184-223) finds it.
+ *   rows (n, max_rows, 7), nrows (n): as written by tb_trace_rk45
+ *   p0, normal: host double[3], a point of the plane and its normal (non-zero)
+ *   out (n, 7) t, x..vz at the crossing (NaN where there is none)
+ *   found (n) int32 1 / 0 (the reference's bool return) */
+int tb_plane_intersection_rows(const double *rows, const int64_t *nrows, int64_t n, int64_t max_rows,
+                               const double *p0, const double *normal, double *out, int32_t *found,
+                               tb_stream_t stream);
+
+/* Least-squares focus of a beam (focus_position, traceon/focus.py:9-42)
+ * from its final states on the device: particle i's x, y, z, vx, vy, vz at
+ * states + i * ld (ld >= 6; e.g. ld = 7 on the x column of a (n, 7) t..vz
+ * array).  out: device double[3] = (x, y, z) of the focus, NaN when the
+ * system is rank deficient (fewer than two particles, or all final
+ * directions equal).  work: device scratch of tb_focus_position_workspace()
+ * bytes. */
+int64_t tb_focus_position_workspace(void);
+int tb_focus_position(const double *states, int64_t n, int64_t ld, double *out, void *work, int64_t work_bytes,
+                      tb_stream_t stream);
 
 /* ---------------------------------------------------------------------
  * Learned field surrogate (no reference counterpart; see tb_mlp.cuh).

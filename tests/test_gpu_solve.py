@@ -83,7 +83,8 @@ def test_mixed_solve_reports_failure_and_solver_falls_back(cuda):
 
 
 @pytest.mark.parametrize('presplit', [False, True])
-@pytest.mark.parametrize('M,N,K', [(128, 256, 32), (300, 500, 256), (1000, 700, 100), (37, 9, 5)])
+@pytest.mark.parametrize('M,N,K', [(128, 256, 32), (300, 500, 256), (1000, 700, 100), (37, 9, 5),
+                                   (4100, 4000, 256)])  # the last: several tiles per CTA of the persistent kernel
 def test_gemm_tf32x3_vs_fp64(cuda, M, N, K, presplit):
     """The tensor-core update C -= A B (tcgen05, 3xTF32) against FP64 numpy,
     on strided sub-matrices with sizes that are not multiples of the 128 x 256
@@ -109,22 +110,26 @@ def test_gemm_tf32x3_vs_fp64(cuda, M, N, K, presplit):
     assert np.array_equal(out[mask], ref[mask])
 
 
-def test_lu_nopiv_tc_factors(cuda):
-    """The FP32 LU with tensor-core trailing updates (256-column panels): on a
-    BEM matrix of 700 elements (three panels, the last partial) L U
+@pytest.mark.parametrize('n', [700, 1000])
+def test_lu_nopiv_tc_factors(cuda, n):
+    """The FP32 LU of the mixed solve (256-column panels: fused panel steps,
+    tensor-core trailing updates): on BEM matrices of 700 elements (three
+    panels, the last partial, 700 = 10 x 64 + 60) and 1,000 elements, L U
     reproduces the column-equilibrated FP32 matrix to FP32 accuracy."""
     import torch
-    A, F = _matrix(cuda, 700)
+    A, F = _matrix(cuda, n)
     A_h = A.cpu().numpy()
     c = 1.0 / np.abs(A_h).max(axis=0)
     S_h = (A_h * c).astype(np.float32)
-    for presplit in (False, True):
-        S = torch.as_tensor(S_h, device='cuda')
-        cuda.dev_lu_nopiv_tc(S, presplit=presplit)
-        LU = S.cpu().numpy().astype(np.float64)
-        L = np.tril(LU, -1) + np.eye(700)
-        U = np.triu(LU)
-        assert np.abs(L @ U - S_h).max() < 2e-5 * np.abs(S_h).max()
+    S = torch.as_tensor(S_h, device='cuda')
+    cuda.dev_lu_nopiv_tc(S)
+    LU = S.cpu().numpy().astype(np.float64)
+    L = np.tril(LU, -1) + np.eye(n)
+    U = np.triu(LU)
+    assert np.abs(L @ U - S_h).max() < 2e-5 * np.abs(S_h).max()
+    err = torch.zeros(1, dtype=torch.int32, device='cuda')
+    with pytest.raises(cuda.BackendError):  # the workspace is required
+        cuda._call('tb_lu_nopiv_f32_tc', S.data_ptr(), n, n, None, 0, err.data_ptr(), cuda._stream())
 
 
 def test_mixed_solve_with_dielectric_rows(cuda, port):

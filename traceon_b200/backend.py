@@ -225,6 +225,8 @@ _DEV = {
     'tb_self_integrals_batched': (vp, C.c_int, i64, vp),
     'tb_gemm_sub_tf32x3': (vp, i64, vp, i64, vp, i64, i64, i64, i64, vp, i64, vp, vp),
     'tb_solve_mixed': (vp, i64, i64, vp, vp, i64, vp, i64, C.c_int, dbl, C.POINTER(C.c_int), C.POINTER(dbl), vp),
+    'tb_plane_intersection_rows': (vp, vp, i64, i64, C.POINTER(dbl), C.POINTER(dbl), vp, vp, vp),
+    'tb_focus_position': (vp, i64, i64, vp, vp, i64, vp),
 }
 for _name, _args in _DEV.items():
     _f = getattr(backend_lib, _name)
@@ -636,6 +638,43 @@ def dev_lu_solve(LU, perm, F):
     return X
 
 
+backend_lib.tb_focus_position_workspace.restype = i64
+backend_lib.tb_focus_position_workspace.argtypes = []
+
+
+def dev_plane_intersection_rows(rows, nrows, p0, normal):
+    """Plane crossing nearest the end of each stored trajectory (rows
+    (n, max_rows, 7), nrows (n) as written by the tracer), linear
+    interpolation as traceon/backend/tracing.c:184-223.  Returns device
+    tensors (out (n, 7) t, x..vz, NaN where none; found (n) bool)."""
+    torch = _torch()
+    n, max_rows = rows.shape[0], rows.shape[1]
+    assert rows.shape[2:] == (7,) and rows.dtype == torch.float64 and rows.is_contiguous()
+    assert nrows.shape == (n,) and nrows.dtype == torch.int64
+    out = torch.empty((n, 7), dtype=torch.float64, device=rows.device)
+    found = torch.empty(n, dtype=torch.int32, device=rows.device)
+    a = (dbl * 3)(*[float(v) for v in np.asarray(p0, dtype=np.float64).reshape(3)])
+    b = (dbl * 3)(*[float(v) for v in np.asarray(normal, dtype=np.float64).reshape(3)])
+    _call('tb_plane_intersection_rows', _ptr(rows), _ptr(nrows), n, max_rows, a, b, _ptr(out), _ptr(found), _stream())
+    return out, found.bool()
+
+
+def dev_focus_position(states):
+    """Least-squares beam focus (traceon/focus.py:9-42) from final states on
+    the device: states (n, 6) x..vz, or (n, 7) t, x..vz.  Returns a device
+    tensor (3,) = (x, y, z); NaN when rank deficient."""
+    torch = _torch()
+    assert states.dim() == 2 and states.shape[1] in (6, 7) and states.dtype == torch.float64
+    states = states.contiguous()
+    off = states.shape[1] - 6
+    out = torch.empty(3, dtype=torch.float64, device=states.device)
+    nbytes = backend_lib.tb_focus_position_workspace()
+    work = torch.empty(nbytes, dtype=torch.uint8, device=states.device)
+    _call('tb_focus_position', states.data_ptr() + 8 * off, states.shape[0], states.stride(0), _ptr(out), _ptr(work),
+          nbytes, _stream())
+    return out
+
+
 backend_lib.tb_solve_mixed_workspace.restype = i64
 backend_lib.tb_solve_mixed_workspace.argtypes = [i64, i64]
 
@@ -653,13 +692,13 @@ backend_lib.tb_gemm_tf32x3_workspace.restype = i64
 backend_lib.tb_gemm_tf32x3_workspace.argtypes = [i64, i64, i64]
 
 
-def dev_lu_nopiv_tc(A, presplit=True):
-    """In-place FP32 LU without pivoting, updates on the tensor cores
-    (3xTF32); presplit: trailing updates from pre-split operands."""
+def dev_lu_nopiv_tc(A):
+    """In-place FP32 LU without pivoting of a square FP32 device matrix:
+    256-column panels, trailing updates on the tensor cores (3xTF32)."""
     torch = _torch()
     N = A.shape[0]
     err = torch.zeros(1, dtype=torch.int32, device=A.device)
-    nbytes = backend_lib.tb_lu_nopiv_f32_tc_workspace(N) if presplit else 0
+    nbytes = backend_lib.tb_lu_nopiv_f32_tc_workspace(N)
     work = torch.empty(nbytes, dtype=torch.uint8, device=A.device) if nbytes else None
     _call('tb_lu_nopiv_f32_tc', _ptr(A), A.stride(0), N, _ptr(work), nbytes, _ptr(err), _stream())
     if int(err.item()):

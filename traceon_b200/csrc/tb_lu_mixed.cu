@@ -147,121 +147,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// ---------------------------------------------------------------- FP32 panel kernels
-// Panel kernels of lu_nopiv_f32_tc (64-wide blocks).  Each thread keeps its
-// row (or column) of the block in registers and eliminates right-looking
-// with the pivots' reciprocals, fully unrolled: no divisions and no dynamic
-// register indexing in the loop.
-
-// D (the nb x nb diagonal block at (k0, k0)) <- its LU factors in place.
-// Thread t owns column j = t % 64 of rows t / 64 + 4 s (s = 0..15) in
-// registers; at step k the owners publish column k and row k to shared
-// memory (double-buffered by the parity of k: one barrier per step) and
-// every thread updates its elements.  Fully unrolled (k and s are constants
-// in every iteration).  Rows and columns beyond nb are the identity.
-__global__ void __launch_bounds__(256) k_diag_lu_f32(float* __restrict__ A, int64_t lda, int64_t k0, int nb) {
-  __shared__ float colk[2][MX_NB], rowk[2][MX_NB];
-  const int j = threadIdx.x % MX_NB, i0 = threadIdx.x / MX_NB;
-  float v[16];
-#pragma unroll
-  for (int sI = 0; sI < 16; sI++) {
-    const int i = i0 + 4 * sI;
-    v[sI] = (i < nb && j < nb) ? A[(k0 + i) * lda + k0 + j] : (i == j ? 1.f : 0.f);
-  }
-#pragma unroll
-  for (int k = 0; k < MX_NB - 1; k++) {
-    if (k >= nb - 1) break;
-    const int buf = k & 1;
-    if (j == k) {
-#pragma unroll
-      for (int sI = 0; sI < 16; sI++) colk[buf][i0 + 4 * sI] = v[sI];
-    }
-    if (i0 == (k & 3)) rowk[buf][j] = v[k >> 2];
-    __syncthreads();
-    const float inv = 1.f / rowk[buf][k];
-    const float u = rowk[buf][j];
-#pragma unroll
-    for (int sI = 0; sI < 16; sI++) {
-      const int i = i0 + 4 * sI;
-      if (i > k) {
-        const float l = colk[buf][i] * inv;
-        if (j == k)
-          v[sI] = l;
-        else if (j > k)
-          v[sI] = fmaf(-l, u, v[sI]);
-      }
-    }
-  }
-#pragma unroll
-  for (int sI = 0; sI < 16; sI++) {
-    const int i = i0 + 4 * sI;
-    if (i < nb && j < nb) A[(k0 + i) * lda + k0 + j] = v[sI];
-  }
-}
-
-// rows r0 <= i < r1: A[i, k0:k0+nb] <- A[i, k0:k0+nb] U11^-1 (one thread per row)
-__global__ void __launch_bounds__(128)
-    k_trsm_right_f32(float* __restrict__ A, int64_t lda, int64_t r0, int64_t r1, int64_t k0, int nb) {
-  __shared__ float U[MX_NB][MX_NB];
-  __shared__ float inv[MX_NB];
-  for (int e = threadIdx.x; e < MX_NB * MX_NB; e += blockDim.x) {
-    const int m = e / MX_NB, jj = e % MX_NB;
-    U[m][jj] = (m < nb && jj < nb) ? A[(k0 + m) * lda + k0 + jj] : 0.f;
-  }
-  __syncthreads();
-  for (int m = threadIdx.x; m < MX_NB; m += blockDim.x) inv[m] = m < nb ? 1.f / U[m][m] : 1.f;
-  __syncthreads();
-  const int64_t i = r0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= r1) return;
-  float* row = A + i * lda + k0;
-  float v[MX_NB];
-#pragma unroll
-  for (int jj = 0; jj < MX_NB; jj++) v[jj] = jj < nb ? row[jj] : 0.f;
-#pragma unroll
-  for (int m = 0; m < MX_NB; m++) {
-    const float x = v[m] * inv[m];
-    v[m] = x;
-#pragma unroll
-    for (int jj = m + 1; jj < MX_NB; jj++) v[jj] = fmaf(-x, U[m][jj], v[jj]);
-  }
-#pragma unroll
-  for (int jj = 0; jj < MX_NB; jj++)
-    if (jj < nb) row[jj] = v[jj];
-}
-
-// columns c0 <= c < c1: A[k0:k0+nb, c] <- L11^-1 A[k0:k0+nb, c] (L11 unit
-// lower).  The CTA's 64 x 128 column tile passes through shared memory
-// (coalesced global access, constant-offset shared reads into registers).
-__global__ void __launch_bounds__(128)
-    k_trsm_left_f32(float* __restrict__ A, int64_t lda, int64_t c0, int64_t c1, int64_t k0, int nb) {
-  __shared__ float Lr[MX_NB][MX_NB];
-  __shared__ float T[MX_NB][128];
-  const int64_t cb = c0 + blockIdx.x * (int64_t)128;
-  const int ncol = c1 - cb < 128 ? int(c1 - cb) : 128;
-  for (int e = threadIdx.x; e < MX_NB * MX_NB; e += blockDim.x) {
-    const int ii = e / MX_NB, m = e % MX_NB;
-    Lr[ii][m] = (ii < nb && m < nb && m < ii) ? A[(k0 + ii) * lda + k0 + m] : 0.f;
-  }
-  for (int ii = 0; ii < MX_NB; ii++) T[ii][threadIdx.x] = (ii < nb && threadIdx.x < ncol) ? A[(k0 + ii) * lda + cb + threadIdx.x] : 0.f;
-  __syncthreads();
-  float v[MX_NB];
-#pragma unroll
-  for (int ii = 0; ii < MX_NB; ii++) v[ii] = T[ii][threadIdx.x];
-  // left-looking: v[ii] -= sum_{m < ii} L[ii][m] v[m] (rows of L read contiguously)
-#pragma unroll
-  for (int ii = 1; ii < MX_NB; ii++) {
-    float acc = v[ii];
-#pragma unroll
-    for (int m = 0; m < ii; m++) acc = fmaf(-Lr[ii][m], v[m], acc);
-    v[ii] = acc;
-  }
-#pragma unroll
-  for (int ii = 0; ii < MX_NB; ii++) T[ii][threadIdx.x] = v[ii];
-  __syncthreads();
-  for (int ii = 0; ii < nb; ii++)
-    if (threadIdx.x < ncol) A[(k0 + ii) * lda + cb + threadIdx.x] = T[ii][threadIdx.x];
-}
-
 // ---------------------------------------------------------------- tensor cores
 // C (M x Nc, ldc) -= A (M x K, lda) . B (K x Nc, ldb), FP32 row-major, on
 // the 5th-generation tensor cores (tcgen05.mma kind::tf32) with 3xTF32:
@@ -544,40 +429,53 @@ __global__ void __launch_bounds__(256) k_split_b(const float* __restrict__ B, in
   }
 }
 
-struct GemmPreSmem {
+// C (M x Nc) -= A B from pre-split blocks, persistent: one CTA per SM walks
+// the 128 x 256 tiles (t = blockIdx.x, + gridDim.x, ...) with two
+// accumulators in tensor memory (512 columns), so the epilogue of one tile
+// overlaps the MMAs of the next.  Warp 0 lane 0 streams the K chunks' blocks
+// into two shared-memory stages with bulk copies (waiting for a stage to be
+// released by the MMAs two chunks back), warp 1 lane 0 issues the 3 x 4 MMAs
+// of each chunk (3xTF32) into accumulator t & 1 once the epilogue has
+// released it (acc_empty), releases each stage with tcgen05.commit and
+// signals the tile's end the same way (acc_full);
+// warps 4..11 are the epilogue: warp w drains TMEM lanes 32 (w % 4).. and
+// columns 128 ((w - 4) / 4).. of the tile into C.  Before waiting for an
+// accumulator the epilogue warps prefetch their C rows into L2, so the
+// read-modify-write of C mostly hits L2.  Every wait is bounded; a role
+// whose wait runs out sets the failure flag and the others stop at their
+// next wait.
+constexpr int GQ_THREADS = 384;
+
+struct GemmPersistSmem {
   uint8_t a[2][PA_BLOCK];
   uint8_t b[2][PB_BLOCK];
-  uint64_t full[2], empty[2];
+  uint64_t full[2], empty[2], acc_full[2], acc_empty[2];
   uint32_t tmem_base;
   int fail;
 };
-constexpr int GP_SMEM_BYTES = int(sizeof(GemmPreSmem)) + 1024;
+constexpr int GQ_SMEM_BYTES = int(sizeof(GemmPersistSmem)) + 1024;
 
-// C (M x Nc) -= A B from pre-split blocks: warp 0 lane 0 streams the K
-// chunks into two shared-memory stages with bulk copies (waiting for a stage
-// to be released by the MMAs two chunks back), warp 1 lane 0 issues the 3 x 4
-// MMAs of each chunk once its copies have landed and releases the stage with
-// tcgen05.commit; then all 8 warps drain the accumulator as in
-// k_gemm_sub_tf32x3.  Every wait is bounded.
-__global__ void __launch_bounds__(GT_THREADS, 1)
-    k_gemm_sub_pre(float* __restrict__ C, int64_t ldc, const uint8_t* __restrict__ Apre,
-                   const uint8_t* __restrict__ Bpre, int64_t M, int64_t Nc, int nk, int* __restrict__ err) {
-  extern __shared__ __align__(1024) unsigned char gp_raw[];
-  const uint32_t raw = tc::smem_u32(gp_raw);
-  GemmPreSmem& sm = *reinterpret_cast<GemmPreSmem*>(gp_raw + (((raw + 1023u) & ~1023u) - raw));
+__global__ void __launch_bounds__(GQ_THREADS, 1)
+    k_gemm_sub_persist(float* __restrict__ C, int64_t ldc, const uint8_t* __restrict__ Apre,
+                       const uint8_t* __restrict__ Bpre, int64_t M, int64_t Nc, int nk, int64_t nbn, int64_t ntiles,
+                       int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char gq_raw[];
+  const uint32_t raw = tc::smem_u32(gq_raw);
+  GemmPersistSmem& sm = *reinterpret_cast<GemmPersistSmem*>(gq_raw + (((raw + 1023u) & ~1023u) - raw));
+  volatile int* fail = &sm.fail;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  const int64_t mb = blockIdx.y, nb = blockIdx.x;
-  const int64_t m0 = mb * GT_M, n0 = nb * GT_N;
   if (tid < 2) {
     tc::mbar_init(&sm.full[tid], 1);
     tc::mbar_init(&sm.empty[tid], 1);
+    tc::mbar_init(&sm.acc_full[tid], 1);
+    tc::mbar_init(&sm.acc_empty[tid], 8);  // one arrive per epilogue warp
   }
   if (tid == 0) {
     sm.fail = 0;
     tc::fence_mbar_init();
   }
   if (warp == 0) {
-    tc::tmem_alloc(&sm.tmem_base, GT_N);
+    tc::tmem_alloc(&sm.tmem_base, 2 * GT_N);
     tc::tmem_relinquish();
   }
   tc::fence_before_sync();
@@ -586,90 +484,137 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
   const uint32_t dtm = sm.tmem_base;
   constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(GT_N >> 3) << 17) |
                              (uint32_t(GT_M >> 4) << 24);
-  const uint8_t* Ab = Apre + mb * nk * (int64_t)PA_BLOCK;
-  const uint8_t* Bb = Bpre + nb * nk * (int64_t)PB_BLOCK;
+  int issued = 0;  // MMA chunks issued by this thread (warp 1 lane 0)
+  int filled = 0;  // chunks whose copies this thread started (warp 0 lane 0)
   if (warp == 0) {
     if (lane == 0) {  // producer
-      for (int kc = 0; kc < nk; kc++) {
-        const int st = kc & 1;
-        if (kc >= 2 && !tc::mbar_wait_bounded(&sm.empty[st], uint32_t((kc - 2) >> 1) & 1u, GT_WAIT_CYCLES)) {
-          sm.fail = 1;
-          break;
+      int it = 0;
+      for (int64_t t = blockIdx.x; t < ntiles && !*fail; t += gridDim.x) {
+        const uint8_t* Ab = Apre + (t / nbn) * nk * (int64_t)PA_BLOCK;
+        const uint8_t* Bb = Bpre + (t % nbn) * nk * (int64_t)PB_BLOCK;
+        for (int kc = 0; kc < nk; kc++, it++) {
+          const int st = it & 1;
+          if (it >= 2 && !tc::mbar_wait_bounded(&sm.empty[st], uint32_t((it - 2) >> 1) & 1u, GT_WAIT_CYCLES)) {
+            *fail = 1;
+            break;
+          }
+          tc::mbar_arrive_expect_tx(&sm.full[st], PA_BLOCK + PB_BLOCK);
+          const uint32_t da = tc::smem_u32(sm.a[st]), db = tc::smem_u32(sm.b[st]);
+          for (uint32_t o = 0; o < PA_BLOCK; o += 16384u)
+            tc::bulk_copy_g2s(da + o, Ab + kc * (int64_t)PA_BLOCK + o, 16384u, &sm.full[st]);
+          for (uint32_t o = 0; o < PB_BLOCK; o += 16384u)
+            tc::bulk_copy_g2s(db + o, Bb + kc * (int64_t)PB_BLOCK + o, 16384u, &sm.full[st]);
+          filled = it + 1;
         }
-        tc::mbar_arrive_expect_tx(&sm.full[st], PA_BLOCK + PB_BLOCK);
-        const uint32_t da = tc::smem_u32(sm.a[st]), db = tc::smem_u32(sm.b[st]);
-        for (uint32_t o = 0; o < PA_BLOCK; o += 16384u)
-          tc::bulk_copy_g2s(da + o, Ab + kc * (int64_t)PA_BLOCK + o, 16384u, &sm.full[st]);
-        for (uint32_t o = 0; o < PB_BLOCK; o += 16384u)
-          tc::bulk_copy_g2s(db + o, Bb + kc * (int64_t)PB_BLOCK + o, 16384u, &sm.full[st]);
       }
     }
     __syncwarp();
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
-      for (int kc = 0; kc < nk; kc++) {
-        const int st = kc & 1;
-        if (!tc::mbar_wait_bounded(&sm.full[st], uint32_t(kc >> 1) & 1u, GT_WAIT_CYCLES)) {
-          sm.fail = 1;
+      int it = 0, tl = 0;
+      for (int64_t t = blockIdx.x; t < ntiles && !*fail; t += gridDim.x, tl++) {
+        const int buf = tl & 1;
+        if (tl >= 2 && !tc::mbar_wait_bounded(&sm.acc_empty[buf], uint32_t((tl - 2) >> 1) & 1u, GT_WAIT_CYCLES)) {
+          *fail = 1;
           break;
         }
         tc::fence_after_sync();
-        const uint32_t ah = tc::smem_u32(sm.a[st]), al = ah + GT_M * 128;
-        const uint32_t bh = tc::smem_u32(sm.b[st]), bl = bh + GT_N * 128;
+        const uint32_t d = dtm + uint32_t(buf * GT_N);
+        bool ok = true;
+        for (int kc = 0; kc < nk; kc++, it++) {
+          const int st = it & 1;
+          if (!tc::mbar_wait_bounded(&sm.full[st], uint32_t(it >> 1) & 1u, GT_WAIT_CYCLES)) {
+            ok = false;
+            break;
+          }
+          tc::fence_after_sync();
+          const uint32_t ah = tc::smem_u32(sm.a[st]), al = ah + GT_M * 128;
+          const uint32_t bh = tc::smem_u32(sm.b[st]), bl = bh + GT_N * 128;
 #pragma unroll
-        for (int ks = 0; ks < GT_K / 8; ks++) {
-          const uint64_t dah = tc::desc_sw128(ah + 32 * ks), dal = tc::desc_sw128(al + 32 * ks);
-          const uint64_t dbh = tc::desc_sw128(bh + 32 * ks), dbl = tc::desc_sw128(bl + 32 * ks);
-          mma_tf32(dtm, dal, dbh, IDESC, (kc > 0 || ks > 0) ? 1u : 0u);
-          mma_tf32(dtm, dah, dbl, IDESC, 1u);
-          mma_tf32(dtm, dah, dbh, IDESC, 1u);
+          for (int ks = 0; ks < GT_K / 8; ks++) {
+            const uint64_t dah = tc::desc_sw128(ah + 32 * ks), dal = tc::desc_sw128(al + 32 * ks);
+            const uint64_t dbh = tc::desc_sw128(bh + 32 * ks), dbl = tc::desc_sw128(bl + 32 * ks);
+            mma_tf32(d, dal, dbh, IDESC, (kc > 0 || ks > 0) ? 1u : 0u);
+            mma_tf32(d, dah, dbl, IDESC, 1u);
+            mma_tf32(d, dah, dbh, IDESC, 1u);
+          }
+          tc::mma_commit(&sm.empty[st]);
+          issued = it + 1;
         }
-        tc::mma_commit(&sm.empty[st]);
+        if (!ok) {
+          *fail = 1;
+          break;
+        }
+        tc::mma_commit(&sm.acc_full[buf]);
       }
     }
     __syncwarp();
-  }
-  bool ok = tc::mbar_wait_warp(&sm.empty[(nk - 1) & 1], uint32_t((nk - 1) >> 1) & 1u, GT_WAIT_CYCLES);
-  ok = !__syncthreads_or(!ok || sm.fail);
-  if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
-  } else {
-    tc::fence_after_sync();
-    const int row = 32 * (warp % 4) + lane;
-    const int64_t gr = m0 + row;
-    const uint32_t tbase = dtm + (uint32_t(32 * (warp % 4)) << 16) + uint32_t(128 * (warp / 4));
+  } else if (warp >= 4) {  // epilogue
+    const int quarter = warp % 4, half = (warp - 4) / 4;
+    const int row = 32 * quarter + lane;
     const bool vec = (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(C) % 16 == 0);
+    int tl = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, tl++) {
+      const int buf = tl & 1;
+      const int64_t gr = (t / nbn) * GT_M + row;
+      const int64_t c0 = (t % nbn) * GT_N + 128 * half;
+      if (gr < M && c0 < Nc) {  // this thread's 128 columns of C, 4 lines of 128 bytes
+        const float* crow = C + gr * ldc + c0;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (c0 + 32 * q < Nc) asm volatile("prefetch.global.L2 [%0];" ::"l"(crow + 32 * q));
+      }
+      const bool stop = __shfl_sync(0xffffffffu, *fail, 0) != 0;  // warp-uniform
+      if (stop || !tc::mbar_wait_warp(&sm.acc_full[buf], uint32_t(tl >> 1) & 1u, GT_WAIT_CYCLES)) {
+        if (lane == 0) *fail = 1;
+        break;
+      }
+      tc::fence_after_sync();
+      const uint32_t tbase = dtm + (uint32_t(32 * quarter) << 16) + uint32_t(buf * GT_N + 128 * half);
 #pragma unroll 1
-    for (int c = 0; c < 8; c++) {
-      uint32_t v[16];
-      tc::tmem_ld16(tbase + 16 * c, v);
-      tc::tmem_wait_ld16(v);
-      const int64_t col0 = n0 + 128 * (warp / 4) + 16 * c;
-      if (gr < M && col0 < Nc) {
-        float* crow = C + gr * ldc + col0;
-        if (vec && col0 + 16 <= Nc) {
+      for (int c = 0; c < 8; c++) {
+        uint32_t v[16];
+        tc::tmem_ld16(tbase + 16 * c, v);
+        tc::tmem_wait_ld16(v);
+        const int64_t col0 = c0 + 16 * c;
+        if (gr < M && col0 < Nc) {
+          float* crow = C + gr * ldc + col0;
+          if (vec && col0 + 16 <= Nc) {
 #pragma unroll
-          for (int q = 0; q < 4; q++) {
-            float4 x = *reinterpret_cast<float4*>(crow + 4 * q);
-            x.x -= __uint_as_float(v[4 * q]);
-            x.y -= __uint_as_float(v[4 * q + 1]);
-            x.z -= __uint_as_float(v[4 * q + 2]);
-            x.w -= __uint_as_float(v[4 * q + 3]);
-            *reinterpret_cast<float4*>(crow + 4 * q) = x;
+            for (int q = 0; q < 4; q++) {
+              float4 x = *reinterpret_cast<float4*>(crow + 4 * q);
+              x.x -= __uint_as_float(v[4 * q]);
+              x.y -= __uint_as_float(v[4 * q + 1]);
+              x.z -= __uint_as_float(v[4 * q + 2]);
+              x.w -= __uint_as_float(v[4 * q + 3]);
+              *reinterpret_cast<float4*>(crow + 4 * q) = x;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++)
+              if (col0 + j < Nc) crow[j] -= __uint_as_float(v[j]);
           }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 16; j++)
-            if (col0 + j < Nc) crow[j] -= __uint_as_float(v[j]);
         }
       }
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&sm.acc_empty[buf]);
     }
   }
+  // teardown: the MMAs issued and the copies started must have completed
+  // before TMEM is freed and the CTA exits (after a failure too; all of
+  // this has already happened on the normal path)
+  if (warp == 1 && lane == 0 && issued > 0)
+    tc::mbar_wait_bounded(&sm.empty[(issued - 1) & 1], uint32_t((issued - 1) >> 1) & 1u, GT_WAIT_CYCLES);
+  if (warp == 0 && lane == 0)
+    for (int j = filled - 1; j >= 0 && j >= filled - 2; j--)
+      tc::mbar_wait_bounded(&sm.full[j & 1], uint32_t(j >> 1) & 1u, GT_WAIT_CYCLES);
   tc::fence_before_sync();
   __syncthreads();
+  if (tid == 0 && sm.fail) atomicExch(err, 1);
   if (warp == 0) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(dtm, GT_N);
+    tc::tmem_dealloc(dtm, 2 * GT_N);
   }
 }
 
@@ -687,7 +632,7 @@ static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, cons
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return CUDA_ERR;
   if (dev >= 0 && dev < 64 && !g_attr_gemm_pre[dev]) {
-    if (cudaFuncSetAttribute(k_gemm_sub_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, GP_SMEM_BYTES) !=
+    if (cudaFuncSetAttribute(k_gemm_sub_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, GQ_SMEM_BYTES) !=
         cudaSuccess)
       return CUDA_ERR;
     g_attr_gemm_pre[dev] = true;
@@ -698,48 +643,373 @@ static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, cons
   uint8_t* pb = work + mbk * nk * (int64_t)PA_BLOCK;
   k_split_a<<<dim3(unsigned(nk), unsigned(mbk)), 256, 0, s>>>(A, lda, M, K, pa);
   k_split_b<<<dim3(unsigned(nk), unsigned(nbk)), 256, 0, s>>>(B, ldb, K, Nc, pb);
-  k_gemm_sub_pre<<<dim3(unsigned(nbk), unsigned(mbk)), GT_THREADS, GP_SMEM_BYTES, s>>>(C, ldc, pa, pb, M, Nc, nk, err);
+  const int64_t ntiles = mbk * nbk;
+  const int64_t grid = ntiles < num_sms() ? ntiles : num_sms();
+  k_gemm_sub_persist<<<unsigned(grid), GQ_THREADS, GQ_SMEM_BYTES, s>>>(C, ldc, pa, pb, M, Nc, nk, nbk, ntiles, err);
   return launch_status();
 }
 
-// FP32 LU without pivoting, two-level blocked: panels of 256 columns are
-// factored with the 64-wide kernels above (diagonal block, triangular
-// solves) and tensor-core updates (K = 64) inside the panel and its row
-// block; the trailing matrix is updated once per panel on the tensor cores
-// (K = 256).  err receives 1 if a tensor-core wait ran out.
+// FP32 LU without pivoting, two-level blocked: panels of 256 columns; each
+// 64-column step of a panel is k_panel_head + k_panel_rows, the panel's
+// row block is one k_rowblock_step per step, and the trailing matrix is
+// updated once per panel on the tensor cores (K = 256, pre-split operands,
+// persistent).  work: the pre-split operand blocks of the trailing update;
+// its first LU_INV_BYTES also hold the inverses of the current panel's
+// diagonal blocks (free while the panel is factored).  err receives 1 if a
+// tensor-core wait ran out.
 constexpr int TC_PANEL = 256;
+constexpr int64_t LU_INV_BYTES = int64_t(TC_PANEL / 64) * 2 * 64 * 64 * int64_t(sizeof(float));
+// ---------------------------------------------------------------- fused panel steps
+// One 64-column step of a panel in two launches instead of four.
+//
+// k_panel_head (one CTA): LU of the 64 x 64 diagonal block, the inverses of its unit lower and upper triangles
+// (Li = L11^-1, Ui = U11^-1, written to `inv` for the next launch), and the
+// block row of U right of the block inside the panel, U12 = Li A12
+// (independent dot products).
+//
+// k_panel_rows (a CTA per 64 rows below the block): L21 = A21 Ui, then the
+// panel columns right of the block, A22 -= L21 U12 (FP32 FMA; a panel is at
+// most 256 wide, so U12 has at most 192 columns).
+//
+// Explicit inverses of the 64 x 64 diagonal triangles turn the triangular
+// solves into independent dot products; the factors only precondition the
+// FP64 refinement, whose convergence the solver checks.
+constexpr int PR_LD = MX_NB + 4;  // row stride of the transposed 64-row tiles (16-byte aligned rows)
+constexpr int PR_MAXR = TC_PANEL - MX_NB;  // columns of U12
+// T, Ui, Li, Lit (Li transposed), Xs (A12)
+constexpr int PH_SMEM = (MX_NB * (MX_NB + 1) + 2 * MX_NB * MX_NB + MX_NB * PR_LD + MX_NB * PR_MAXR) * int(sizeof(float));
+constexpr int PR_SMEM = (MX_NB * PR_LD + MX_NB * MX_NB + MX_NB * PR_MAXR) * int(sizeof(float));
+
+__global__ void __launch_bounds__(256) k_panel_head(float* __restrict__ A, int64_t lda, int64_t k0, int nb, int right,
+                                                   float* __restrict__ inv) {
+  extern __shared__ __align__(16) float ph_dyn[];
+  float(*T)[MX_NB + 1] = reinterpret_cast<float(*)[MX_NB + 1]>(ph_dyn);
+  float(*Ui)[MX_NB] = reinterpret_cast<float(*)[MX_NB]>(ph_dyn + MX_NB * (MX_NB + 1));
+  float(*Li)[MX_NB] = Ui + MX_NB;
+  float(*Lit)[PR_LD] = reinterpret_cast<float(*)[PR_LD]>(ph_dyn + MX_NB * (MX_NB + 1) + 2 * MX_NB * MX_NB);
+  float(*Xs)[PR_MAXR] =
+      reinterpret_cast<float(*)[PR_MAXR]>(ph_dyn + MX_NB * (MX_NB + 1) + 2 * MX_NB * MX_NB + MX_NB * PR_LD);
+  __shared__ float rpiv[MX_NB];  // reciprocal pivots, each formed once
+  const int jj = threadIdx.x % MX_NB, ig = threadIdx.x / MX_NB;
+  // LU of the diagonal block, right-looking in shared memory.  Step k
+  // updates only the trailing (nb - 1 - k)^2 block: thread (jj, ig) takes
+  // column k + 1 + jj and every 4th row from k + 1 + ig.  The multipliers
+  // are formed on the fly from the unscaled column k, which is scaled after
+  // the step's barrier (step k + 1 does not read it): one barrier per step.
+  // Thread 0 updates the next pivot (row and column k + 1 of its share) and
+  // forms its correctly rounded reciprocal for everyone.  Rows and columns
+  // beyond nb are the identity.
+#pragma unroll
+  for (int s = 0; s < 16; s++) {
+    const int i = ig + 4 * s;
+    T[i][jj] = (i < nb && jj < nb) ? A[(k0 + i) * lda + k0 + jj] : (i == jj ? 1.f : 0.f);
+  }
+  if (threadIdx.x == 0) rpiv[0] = __frcp_rn(T[0][0]);  // thread 0 loaded T[0][0]
+  __syncthreads();
+#pragma unroll 1
+  for (int k = 0; k < nb - 1; k++) {
+    const float rp = rpiv[k];
+    const int j = k + 1 + jj;
+    if (j < nb) {
+      const float u = T[k][j];
+#pragma unroll 4
+      for (int i = k + 1 + ig; i < nb; i += 4) T[i][j] = fmaf(-(T[i][k] * rp), u, T[i][j]);
+    }
+    if (threadIdx.x == 0) rpiv[k + 1] = __frcp_rn(T[k + 1][k + 1]);  // its own update of step k
+    __syncthreads();
+    if (k + 1 + threadIdx.x < nb) T[k + 1 + threadIdx.x][k] *= rp;
+  }
+  __syncthreads();
+  // inverses, one column per thread: threads 0..63 Ui, 64..127 Li (rows and
+  // columns beyond nb are the identity); two partial sums per element
+  if (threadIdx.x < MX_NB) {
+    const int k = threadIdx.x;
+#pragma unroll 1
+    for (int i = MX_NB - 1; i >= 0; i--) {
+      float s0 = (i == k) ? 1.f : 0.f, s1 = 0.f;
+      if (i <= k) {
+        int m = i + 1;
+        for (; m + 1 <= k; m += 2) {
+          s0 = fmaf(-T[i][m], Ui[m][k], s0);
+          s1 = fmaf(-T[i][m + 1], Ui[m + 1][k], s1);
+        }
+        if (m <= k) s0 = fmaf(-T[i][m], Ui[m][k], s0);
+      }
+      Ui[i][k] = i <= k ? (s0 + s1) * (i < nb ? rpiv[i] : 1.f) : 0.f;
+    }
+  } else if (threadIdx.x < 2 * MX_NB) {
+    const int k = threadIdx.x - MX_NB;
+#pragma unroll 1
+    for (int i = 0; i < MX_NB; i++) {
+      float s0 = (i == k) ? 1.f : 0.f, s1 = 0.f;
+      if (i > k) {
+        int m = k;
+        for (; m + 1 < i; m += 2) {
+          s0 = fmaf(-T[i][m], Li[m][k], s0);
+          s1 = fmaf(-T[i][m + 1], Li[m + 1][k], s1);
+        }
+        if (m < i) s0 = fmaf(-T[i][m], Li[m][k], s0);
+      }
+      Li[i][k] = i >= k ? s0 + s1 : 0.f;
+    }
+  }
+  __syncthreads();
+  // U12 = Li A12 (64 x right): thread (c, g) forms rows 16 g .. 16 g + 15 of
+  // columns c, c + 64, c + 128 as independent dot products, Li read
+  // transposed (Lit[m][i] = Li[i][m]) as 16-byte broadcasts
+  if (right > 0) {
+    for (int e = threadIdx.x; e < MX_NB * MX_NB; e += blockDim.x) Lit[e % MX_NB][e / MX_NB] = Li[e / MX_NB][e % MX_NB];
+    for (int e = threadIdx.x; e < MX_NB * right; e += blockDim.x) {
+      const int m = e / right, j = e % right;
+      Xs[m][j] = m < nb ? A[(k0 + m) * lda + k0 + nb + j] : 0.f;
+    }
+    __syncthreads();
+    const int c = threadIdx.x % MX_NB, g = threadIdx.x / MX_NB;
+    for (int j = c; j < right; j += MX_NB) {
+      float acc[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) acc[q] = 0.f;
+#pragma unroll 4
+      for (int m = 0; m < MX_NB; m++) {
+        const float w = Xs[m][j];
+        const float4* lr = reinterpret_cast<const float4*>(&Lit[m][16 * g]);
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          const float4 y = lr[v];
+          acc[4 * v] = fmaf(y.x, w, acc[4 * v]);
+          acc[4 * v + 1] = fmaf(y.y, w, acc[4 * v + 1]);
+          acc[4 * v + 2] = fmaf(y.z, w, acc[4 * v + 2]);
+          acc[4 * v + 3] = fmaf(y.w, w, acc[4 * v + 3]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        if (16 * g + q < nb) A[(k0 + 16 * g + q) * lda + k0 + nb + j] = acc[q];
+    }
+  }
+  // the factored block and the inverses
+#pragma unroll
+  for (int s = 0; s < 16; s++) {
+    const int i = ig + 4 * s;
+    if (i < nb && jj < nb) A[(k0 + i) * lda + k0 + jj] = T[i][jj];
+  }
+  for (int e = threadIdx.x; e < MX_NB * MX_NB; e += blockDim.x) {
+    inv[e] = Ui[e / MX_NB][e % MX_NB];
+    inv[MX_NB * MX_NB + e] = Li[e / MX_NB][e % MX_NB];
+  }
+}
+
+// Rows r0 <= r < r1 (a CTA per 64): L21 = A21 Ui into A[r, k0:k0+64], then
+// A[r, k0+nb : k0+nb+right] -= L21 U12.  Thread (c, g) = (t % 64, t / 64)
+// computes rows 16 g .. 16 g + 15 of the CTA's 64 for column c; the 16 row
+// values of a k index are one broadcast 64-byte read of a transposed tile.
+__global__ void __launch_bounds__(256) k_panel_rows(float* __restrict__ A, int64_t lda, int64_t k0, int nb,
+                                                   int64_t r0, int64_t r1, int right, const float* __restrict__ inv) {
+  extern __shared__ __align__(16) float pr_dyn[];
+  float(*At)[PR_LD] = reinterpret_cast<float(*)[PR_LD]>(pr_dyn);          // At[m][r]: A21, then L21
+  float(*Us)[MX_NB] = reinterpret_cast<float(*)[MX_NB]>(pr_dyn + MX_NB * PR_LD);  // Ui
+  float(*U12)[PR_MAXR] = reinterpret_cast<float(*)[PR_MAXR]>(pr_dyn + MX_NB * PR_LD + MX_NB * MX_NB);
+  const int c = threadIdx.x % MX_NB, g = threadIdx.x / MX_NB;
+  const int64_t rb = r0 + blockIdx.x * (int64_t)MX_NB;
+  const int nrow = r1 - rb < MX_NB ? int(r1 - rb) : MX_NB;
+  {  // staging; all loads of a thread issued before the shared-memory stores
+    float a[16], u[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int e = threadIdx.x + 256 * q, m = e / MX_NB, r = e % MX_NB;  // lanes over rows r
+      a[q] = (r < nrow && m < nb) ? A[(rb + r) * lda + k0 + m] : 0.f;
+      u[q] = inv[e];
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int e = threadIdx.x + 256 * q;
+      At[e / MX_NB][e % MX_NB] = a[q];
+      Us[e / MX_NB][e % MX_NB] = u[q];
+    }
+    for (int e = threadIdx.x; e < MX_NB * right; e += blockDim.x) {
+      const int m = e / right, j = e % right;
+      U12[m][j] = m < nb ? A[(k0 + m) * lda + k0 + nb + j] : 0.f;
+    }
+  }
+  __syncthreads();
+  float acc[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) acc[q] = 0.f;
+#pragma unroll 4
+  for (int m = 0; m < MX_NB; m++) {
+    const float w = Us[m][c];
+    const float4* ar = reinterpret_cast<const float4*>(&At[m][16 * g]);
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const float4 x = ar[v];
+      acc[4 * v] = fmaf(x.x, w, acc[4 * v]);
+      acc[4 * v + 1] = fmaf(x.y, w, acc[4 * v + 1]);
+      acc[4 * v + 2] = fmaf(x.z, w, acc[4 * v + 2]);
+      acc[4 * v + 3] = fmaf(x.w, w, acc[4 * v + 3]);
+    }
+  }
+  __syncthreads();  // every read of A21 is done: At becomes L21 (transposed)
+  if (c < nb) {
+    float4* lr = reinterpret_cast<float4*>(&At[c][16 * g]);
+#pragma unroll
+    for (int v = 0; v < 4; v++) lr[v] = make_float4(acc[4 * v], acc[4 * v + 1], acc[4 * v + 2], acc[4 * v + 3]);
+#pragma unroll
+    for (int q = 0; q < 16; q++)
+      if (16 * g + q < nrow) A[(rb + 16 * g + q) * lda + k0 + c] = acc[q];
+  } else {
+    float4* lr = reinterpret_cast<float4*>(&At[c][16 * g]);
+#pragma unroll
+    for (int v = 0; v < 4; v++) lr[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  if (right <= 0) return;
+  __syncthreads();
+  for (int j0 = 0; j0 < right; j0 += MX_NB) {
+    const int j = j0 + c;
+    float* out = A + (rb + 16 * g) * lda + k0 + nb + j;
+#pragma unroll
+    for (int q = 0; q < 16; q++) acc[q] = (j < right && 16 * g + q < nrow) ? out[q * lda] : 0.f;
+    if (j < right) {
+#pragma unroll 4
+      for (int m = 0; m < MX_NB; m++) {
+        const float w = U12[m][j];
+        const float4* lr = reinterpret_cast<const float4*>(&At[m][16 * g]);
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          const float4 x = lr[v];
+          acc[4 * v] = fmaf(-x.x, w, acc[4 * v]);
+          acc[4 * v + 1] = fmaf(-x.y, w, acc[4 * v + 1]);
+          acc[4 * v + 2] = fmaf(-x.z, w, acc[4 * v + 2]);
+          acc[4 * v + 3] = fmaf(-x.w, w, acc[4 * v + 3]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        if (16 * g + q < nrow) out[q * lda] = acc[q];
+    }
+  }
+}
+
+// The panel's row block right of the panel, one 64-row step per launch:
+// X = Li A[k0:k0+64, cb:cb+64] (the block row of U), then the rows of the
+// panel below the step, A[k0+nb : pe, cb:cb+64] -= L[k0+nb : pe, k0:k0+nb] X.
+// A CTA per 64 columns (thread (c, g) = column c, rows 16 g .. 16 g + 15 of
+// a 64-row group); Li comes from the step's k_panel_head.
+constexpr int RB_MAXR = TC_PANEL - MX_NB;  // panel rows below a step
+constexpr int RB_LD = RB_MAXR + 4;
+constexpr int RB_SMEM = (MX_NB * MX_NB + MX_NB * PR_LD + MX_NB * RB_LD) * int(sizeof(float));
+
+__global__ void __launch_bounds__(256) k_rowblock_step(float* __restrict__ A, int64_t lda, int64_t k0, int nb,
+                                                      int rows, int64_t c0, int64_t c1, const float* __restrict__ li) {
+  extern __shared__ __align__(16) float rb_dyn[];
+  float(*Xs)[MX_NB] = reinterpret_cast<float(*)[MX_NB]>(rb_dyn);                 // Xs[m][c]
+  float(*Lit)[PR_LD] = reinterpret_cast<float(*)[PR_LD]>(rb_dyn + MX_NB * MX_NB);  // Lit[m][i] = Li[i][m]
+  float(*Lpt)[RB_LD] = reinterpret_cast<float(*)[RB_LD]>(rb_dyn + MX_NB * MX_NB + MX_NB * PR_LD);  // Lpt[m][r]
+  const int c = threadIdx.x % MX_NB, g = threadIdx.x / MX_NB;
+  const int64_t cb = c0 + blockIdx.x * (int64_t)MX_NB;
+  const bool col_ok = cb + c < c1;
+  {
+    float x[16], l[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int m = g + 4 * q;
+      x[q] = (m < nb && col_ok) ? A[(k0 + m) * lda + cb + c] : 0.f;
+      const int e = threadIdx.x + 256 * q;  // Li row-major: e = i * 64 + m
+      l[q] = li[e];
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      Xs[g + 4 * q][c] = x[q];
+      const int e = threadIdx.x + 256 * q;
+      Lit[e % MX_NB][e / MX_NB] = l[q];
+    }
+    for (int e = threadIdx.x; e < rows * MX_NB; e += blockDim.x) {
+      const int r = e / MX_NB, m = e % MX_NB;
+      Lpt[m][r] = m < nb ? A[(k0 + nb + r) * lda + k0 + m] : 0.f;
+    }
+  }
+  __syncthreads();
+  float acc[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) acc[q] = 0.f;
+#pragma unroll 4
+  for (int m = 0; m < MX_NB; m++) {
+    const float w = Xs[m][c];
+    const float4* lr = reinterpret_cast<const float4*>(&Lit[m][16 * g]);
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const float4 y = lr[v];
+      acc[4 * v] = fmaf(y.x, w, acc[4 * v]);
+      acc[4 * v + 1] = fmaf(y.y, w, acc[4 * v + 1]);
+      acc[4 * v + 2] = fmaf(y.z, w, acc[4 * v + 2]);
+      acc[4 * v + 3] = fmaf(y.w, w, acc[4 * v + 3]);
+    }
+  }
+  __syncthreads();  // every read of the input X is done
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int i = 16 * g + q;
+    Xs[i][c] = acc[q];
+    if (i < nb && col_ok) A[(k0 + i) * lda + cb + c] = acc[q];
+  }
+  if (rows <= 0) return;
+  __syncthreads();
+  for (int r0 = 0; r0 < rows; r0 += MX_NB) {
+    float* out = A + (k0 + nb + r0 + 16 * g) * lda + cb + c;
+#pragma unroll
+    for (int q = 0; q < 16; q++) acc[q] = (col_ok && r0 + 16 * g + q < rows) ? out[q * lda] : 0.f;
+#pragma unroll 4
+    for (int m = 0; m < MX_NB; m++) {
+      const float w = Xs[m][c];
+      const float4* lr = reinterpret_cast<const float4*>(&Lpt[m][r0 + 16 * g]);
+#pragma unroll
+      for (int v = 0; v < 4; v++) {
+        const float4 y = lr[v];
+        acc[4 * v] = fmaf(-y.x, w, acc[4 * v]);
+        acc[4 * v + 1] = fmaf(-y.y, w, acc[4 * v + 1]);
+        acc[4 * v + 2] = fmaf(-y.z, w, acc[4 * v + 2]);
+        acc[4 * v + 3] = fmaf(-y.w, w, acc[4 * v + 3]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q++)
+      if (col_ok && r0 + 16 * g + q < rows) out[q * lda] = acc[q];
+  }
+}
+
+static bool g_attr_panel[64];
+
 static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* work, cudaStream_t s) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return CUDA_ERR;
+  if (dev >= 0 && dev < 64 && !g_attr_panel[dev]) {
+    if (cudaFuncSetAttribute(k_panel_head, cudaFuncAttributeMaxDynamicSharedMemorySize, PH_SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(k_panel_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(k_rowblock_step, cudaFuncAttributeMaxDynamicSharedMemorySize, RB_SMEM) != cudaSuccess)
+      return CUDA_ERR;
+    g_attr_panel[dev] = true;
+  }
+  float* inv = reinterpret_cast<float*>(work);  // per step of the panel: Ui (64 x 64), then Li
   for (int64_t p0 = 0; p0 < N; p0 += TC_PANEL) {
     const int64_t pe = p0 + TC_PANEL < N ? p0 + TC_PANEL : N;
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
       const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
-      k_diag_lu_f32<<<1, 256, 0, s>>>(A, lda, k0, nb);
-      const int64_t below = N - k0 - nb, right = pe - k0 - nb;
-      if (below > 0) k_trsm_right_f32<<<unsigned((below + 127) / 128), 128, 0, s>>>(A, lda, k0 + nb, N, k0, nb);
-      if (right > 0) {
-        k_trsm_left_f32<<<unsigned((right + 127) / 128), 128, 0, s>>>(A, lda, k0 + nb, pe, k0, nb);
-        const int st = gemm_sub_tf32x3(A + (k0 + nb) * lda + k0 + nb, lda, A + (k0 + nb) * lda + k0, lda,
-                                       A + k0 * lda + k0 + nb, lda, below, right, nb, err, s);
-        if (st != OK) return st;
-      }
+      const int right = int(pe - k0 - nb);
+      const int64_t below = N - k0 - nb;
+      float* iv = inv + ((k0 - p0) / MX_NB) * 2 * MX_NB * MX_NB;
+      k_panel_head<<<1, 256, PH_SMEM, s>>>(A, lda, k0, nb, right, iv);
+      if (below > 0)
+        k_panel_rows<<<unsigned((below + MX_NB - 1) / MX_NB), 256, PR_SMEM, s>>>(A, lda, k0, nb, k0 + nb, N, right, iv);
     }
     const int64_t rest = N - pe;
     if (rest <= 0) break;
-    // row block right of the panel: U12 = L11^-1 A12, 64 rows at a time
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
       const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
-      k_trsm_left_f32<<<unsigned((rest + 127) / 128), 128, 0, s>>>(A, lda, pe, N, k0, nb);
-      const int64_t rows = pe - k0 - nb;
-      if (rows > 0) {
-        const int st = gemm_sub_tf32x3(A + (k0 + nb) * lda + pe, lda, A + (k0 + nb) * lda + k0, lda, A + k0 * lda + pe,
-                                       lda, rows, rest, nb, err, s);
-        if (st != OK) return st;
-      }
+      const float* li = inv + ((k0 - p0) / MX_NB) * 2 * MX_NB * MX_NB + MX_NB * MX_NB;
+      k_rowblock_step<<<unsigned((rest + MX_NB - 1) / MX_NB), 256, RB_SMEM, s>>>(A, lda, k0, nb, int(pe - k0 - nb), pe,
+                                                                                N, li);
     }
-    const int st = work ? gemm_sub_pre(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest,
-                                       rest, int(pe - p0), work, err, s)
-                        : gemm_sub_tf32x3(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda,
-                                          rest, rest, int(pe - p0), err, s);
+    const int st = gemm_sub_pre(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest,
+                                int(pe - p0), work, err, s);
     if (st != OK) return st;
   }
   return launch_status();
@@ -829,12 +1099,18 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
 // CTA q owns row block b (64 rows; b = q for the forward sweep with the unit
 // lower factor, b = nblk - 1 - q for the backward sweep with the upper
 // factor), so every block it depends on belongs to a CTA launched before it.
-// It accumulates the products of its off-diagonal factor tiles with the
-// finished blocks' solutions as their flags appear, then applies the FP64
-// inverse of its diagonal block (computed once after the factorisation) and
-// publishes its block: solution to X, then the flag (release / acquire).
-// Waits are bounded: after TRSV_WAIT_CYCLES the CTA records an error and
-// writes NaN, which the refinement reports as non-convergence.
+//
+// Lookahead form.  With T the triangle, D_b = T_bb^-1 and g the block
+// published last before b (g = b - 1 forward, b + 1 backward):
+//   x_b = y_b - M_b x_g,   y_b = D_b (r_b - sum_{j != g} T_bj x_j),   M_b = D_b T_bg.
+// y_b needs only blocks published before g, so the CTA finishes it while it
+// waits; the step that gates the next block is one 64 x 64 FP64
+// matrix-vector product with the freshly published x_g.  D_b and M_b are
+// computed once per factorisation (k_diag_inverse) in FP64 from the FP32
+// factor values.  Published blocks: solution to X, then flags[b] = epoch
+// (release / acquire).  Waits are bounded: after TRSV_WAIT_CYCLES the CTA
+// records an error and writes NaN, which the refinement reports as
+// non-convergence.
 constexpr int TS_B = 64;
 constexpr long long TRSV_WAIT_CYCLES = 2000000000LL;  // ~1 s
 
@@ -847,14 +1123,34 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Dinv[blk] = inverse of the 64 x 64 diagonal block blk of the factor (unit
-// lower or upper triangle of LU), in FP64; rows / columns beyond N are the
-// identity.  One CTA of 64 threads per block, one column per thread.
+// Bounded wait of one thread for flags[j] == epoch; false (and err set) when
+// it ran out.  The sleep between polls doubles up to max_ns.
+__device__ __forceinline__ bool wait_flag(const int* flags, int j, int epoch, int* err, unsigned max_ns) {
+  const long long t0 = clock64();
+  unsigned ns = 32;
+  while (ld_acquire(flags + j) != epoch) {
+    if (clock64() - t0 > TRSV_WAIT_CYCLES) {
+      atomicExch(err, 1);
+      return false;
+    }
+    __nanosleep(ns);
+    ns = ns < max_ns ? 2 * ns : max_ns;
+  }
+  return true;
+}
+
+// For row block b of the unit lower (LOWER) or upper triangle of LU:
+// Dinv[b] = T_bb^-1 and Mla[b] = T_bb^-1 T_bg (g = b - 1 / b + 1; zero when
+// b has no such neighbour), both 64 x 64 FP64 stored column-major
+// (element (i, m) at m * 64 + i); rows / columns beyond N are the identity
+// in T_bb and zero in T_bg.  One CTA of 64 threads per block, one column per
+// thread.
 template <bool LOWER>
 __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__ LU, int64_t lda, int64_t N,
-                                                      double* __restrict__ Dinv) {
+                                                      double* __restrict__ Dinv, double* __restrict__ Mla) {
   __shared__ float T[TS_B][TS_B];    // the factor block (FP32 values, exact)
   __shared__ double Xc[TS_B][TS_B];  // Xc[row][col]; thread k owns column k
+  const int nblk = int((N + TS_B - 1) / TS_B);
   const int64_t b0 = (int64_t)blockIdx.x * TS_B;
   const int nb = N - b0 < TS_B ? int(N - b0) : TS_B;
   for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) {
@@ -882,132 +1178,191 @@ __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__
     }
   }
   __syncthreads();
-  // stored column-major: D[m * 64 + i] = (T^-1)[i][m]
   double* D = Dinv + (int64_t)blockIdx.x * TS_B * TS_B;
   for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) D[e] = Xc[e % TS_B][e / TS_B];
+  // the lookahead product with the neighbour block of the same block row
+  const int g = LOWER ? int(blockIdx.x) - 1 : int(blockIdx.x) + 1;
+  double* Mo = Mla + (int64_t)blockIdx.x * TS_B * TS_B;
+  if (g < 0 || g >= nblk) {
+    for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) Mo[e] = 0.0;
+    return;
+  }
+  const int64_t g0 = (int64_t)g * TS_B;
+  for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) {
+    const int i = e / TS_B, j = e % TS_B;
+    T[i][j] = (i < nb && g0 + j < N) ? LU[(b0 + i) * lda + g0 + j] : 0.f;
+  }
+  __syncthreads();
+  for (int i = 0; i < TS_B; i++) {
+    double v0 = 0.0, v1 = 0.0;
+#pragma unroll 8
+    for (int m = 0; m < TS_B; m += 2) {
+      v0 = fma(Xc[i][m], double(T[m][k]), v0);
+      v1 = fma(Xc[i][m + 1], double(T[m + 1][k]), v1);
+    }
+    Mo[(int64_t)k * TS_B + i] = v0 + v1;
+  }
 }
 
 // X (nrhs x N, row r at X + r N) <- T^-1 X with T the unit lower (LOWER) or
-// upper triangle of LU.  256 threads (8 warps).  Every finished block's tile
-// is shared by all 8 warps (warp w: columns 8w .. 8w + 7, lane: rows lane and
-// lane + 32): per tile one bounded wait for the block's flag, one staging of
-// its solution in shared memory, and 16 factor values per lane prefetched
-// into registers before the wait -- so the step that gates publication (the
-// tile of the block just before) costs one short pass, not a full tile on
-// one warp.  Partial sums meet in shared memory, then the FP64 inverse of
-// the diagonal block (staged before any waiting) is applied.
+// upper triangle of LU, in the lookahead form above.  256 threads: thread
+// (i, grp) = (tid % 64, tid / 64) accumulates row i of the block over
+// columns 16 grp .. 16 grp + 15 of every tile before the gate (16 factor
+// values prefetched into registers one tile ahead, NR right-hand sides in
+// registers; the four column groups meet in shared memory once, in a fixed
+// order), and owns right-hand sides NR/4 grp .. NR/4 grp + NR/4 - 1 of row i
+// in the two matrix-vector products.  Dynamic shared memory: D_b, M_b
+// (64 KB) and the column groups' partial sums (NR * 2 KB).
 // flags[blk] == epoch marks a published block.
+template <int NR>
+constexpr int sweep_dyn_bytes() {
+  return 2 * TS_B * TS_B * int(sizeof(double)) + 4 * NR * TS_B * int(sizeof(double));
+}
+
 template <bool LOWER, int NR>
-__global__ void __launch_bounds__(256) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
-                                                   const double* __restrict__ Dinv, double* __restrict__ X, int nrhs,
-                                                   int* __restrict__ flags, int epoch, int* __restrict__ err) {
-  extern __shared__ __align__(16) double sw_dyn[];  // the block's diagonal inverse, 64 x 64 (column-major)
-  __shared__ double accs[TS_B][NR];
-  __shared__ double rs[NR][TS_B];
-  __shared__ double xs[NR][TS_B];
+__global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
+                                                   const double* __restrict__ Dinv, const double* __restrict__ Mla,
+                                                   double* __restrict__ X, int nrhs, int* __restrict__ flags,
+                                                   int epoch, int* __restrict__ err) {
+  extern __shared__ __align__(16) double sw_dyn[];
+  double* Ds = sw_dyn;                    // D_b, column-major
+  double* Ms = sw_dyn + TS_B * TS_B;      // M_b, column-major
+  double* part = Ms + TS_B * TS_B;        // part[(grp * NR + r) * 64 + i]
+  __shared__ __align__(16) double xs[NR][TS_B];  // a published block's solution
+  __shared__ double rs[NR][TS_B];                // this block's right-hand side
   __shared__ int s_fail;
+  constexpr int RPT = NR / 4;  // right-hand sides per thread in the products
   const int nblk = int((N + TS_B - 1) / TS_B);
   const int q = blockIdx.x;
   const int b = LOWER ? q : nblk - 1 - q;
   const int64_t b0 = (int64_t)b * TS_B;
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  // everything that does not depend on other blocks first: the diagonal
-  // inverse and this block's right-hand side
-  const double* Dg = Dinv + (int64_t)b * TS_B * TS_B;
-  for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) sw_dyn[e] = Dg[e];
-  for (int e = threadIdx.x; e < TS_B * NR; e += blockDim.x) accs[e / NR][e % NR] = 0.0;
+  const int i = threadIdx.x % TS_B, grp = threadIdx.x / TS_B;
+  // everything that does not depend on other blocks first
+  {
+    const double* Dg = Dinv + (int64_t)b * TS_B * TS_B;
+    const double* Mg = Mla + (int64_t)b * TS_B * TS_B;
+    for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) {
+      Ds[e] = Dg[e];
+      Ms[e] = Mg[e];
+    }
+  }
   for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
     const int r = e / TS_B, c = e % TS_B;
     rs[r][c] = (r < nrhs && b0 + c < N) ? X[(int64_t)r * N + b0 + c] : 0.0;
   }
   if (threadIdx.x == 0) s_fail = 0;
   __syncthreads();
-  double acc[2][NR];
+  double acc[NR];
 #pragma unroll
-  for (int h = 0; h < 2; h++)
-#pragma unroll
-    for (int r = 0; r < NR; r++) acc[h][r] = 0.0;
-  // this lane's factor values of a tile: rows b0 + lane + 32 h, columns j0 + 8 warp + c
-  float lv[2][8];
+  for (int r = 0; r < NR; r++) acc[r] = 0.0;
+  const int64_t row = b0 + i;
+  const bool vec4 = (lda % 4) == 0 && (reinterpret_cast<uintptr_t>(LU) % 16) == 0;
+  float lv[16];  // row i, columns 16 grp .. 16 grp + 15 of the next tile
   auto load_lu = [&](int j) {
-    const int64_t j0 = (int64_t)j * TS_B + 8 * warp;
+    const int64_t j0 = (int64_t)j * TS_B + 16 * grp;
+    if (vec4 && row < N && j0 + 16 <= N) {
+      const float4* p = reinterpret_cast<const float4*>(LU + row * lda + j0);
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int64_t row = b0 + lane + 32 * h;
+      for (int v = 0; v < 4; v++) {
+        const float4 f = __ldg(p + v);
+        lv[4 * v] = f.x;
+        lv[4 * v + 1] = f.y;
+        lv[4 * v + 2] = f.z;
+        lv[4 * v + 3] = f.w;
+      }
+    } else {
 #pragma unroll
-      for (int c = 0; c < 8; c++) lv[h][c] = (row < N && j0 + c < N) ? LU[row * lda + j0 + c] : 0.f;
+      for (int c = 0; c < 16; c++) lv[c] = (row < N && j0 + c < N) ? LU[row * lda + j0 + c] : 0.f;
     }
   };
-  if (q > 0) load_lu(LOWER ? 0 : nblk - 1);
-  for (int t = 0; t < q; t++) {
-    const int j = LOWER ? t : nblk - 1 - t;  // finished blocks in publication order
-    const int64_t j0 = (int64_t)j * TS_B;
-    if (threadIdx.x == 0) {
-      const long long t0 = clock64();
-      unsigned ns = 32;  // back off so that hundreds of waiting CTAs do not flood L2
-      while (ld_acquire(flags + j) != epoch) {
-        if (clock64() - t0 > TRSV_WAIT_CYCLES) {
-          s_fail = 1;
-          atomicExch(err, 1);
-          break;
-        }
-        __nanosleep(ns);
-        ns = ns < 256 ? 2 * ns : 256;
-      }
-    }
-    __syncthreads();
-    if (s_fail) break;
+  auto load_x = [&](int64_t j0) {  // published by another CTA: read via L2
     for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
-      const int r = e / TS_B, c = e % TS_B;  // published by another CTA: read via L2
+      const int r = e / TS_B, c = e % TS_B;
       xs[r][c] = (r < nrhs && j0 + c < N) ? __ldcg(X + (int64_t)r * N + j0 + c) : 0.0;
     }
+  };
+  const int nacc = q > 0 ? q - 1 : 0;  // tiles accumulated before the gate
+  if (nacc > 0) load_lu(LOWER ? 0 : nblk - 1);
+  for (int t = 0; t < nacc; t++) {
+    const int j = LOWER ? t : nblk - 1 - t;  // finished blocks in publication order
+    if (threadIdx.x == 0 && !wait_flag(flags, j, epoch, err, 256)) s_fail = 1;
+    __syncthreads();  // also: every thread is done with the previous tile's xs
+    if (s_fail) break;
+    load_x((int64_t)j * TS_B);
     __syncthreads();
-    float lc[2][8];
+    float lc[16];
 #pragma unroll
-    for (int h = 0; h < 2; h++)
+    for (int c = 0; c < 16; c++) lc[c] = lv[c];
+    if (t + 1 < nacc) load_lu(LOWER ? t + 1 : nblk - 2 - t);
 #pragma unroll
-      for (int c = 0; c < 8; c++) lc[h][c] = lv[h][c];
-    if (t + 1 < q) load_lu(LOWER ? t + 1 : nblk - 2 - t);
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
+    for (int c = 0; c < 16; c += 2) {
 #pragma unroll
       for (int r = 0; r < NR; r++) {
-        const double x = xs[r][8 * warp + c];
-#pragma unroll
-        for (int h = 0; h < 2; h++) acc[h][r] = fma(double(lc[h][c]), x, acc[h][r]);
+        const double2 x = *reinterpret_cast<const double2*>(&xs[r][16 * grp + c]);
+        acc[r] = fma(double(lc[c]), x.x, acc[r]);
+        acc[r] = fma(double(lc[c + 1]), x.y, acc[r]);
       }
     }
-    __syncthreads();  // xs is rewritten by the next tile
   }
 #pragma unroll
-  for (int h = 0; h < 2; h++)
-#pragma unroll
-    for (int r = 0; r < NR; r++)
-      if (r < nrhs) atomicAdd(&accs[lane + 32 * h][r], acc[h][r]);
+  for (int r = 0; r < NR; r++) part[(grp * NR + r) * TS_B + i] = acc[r];
   __syncthreads();
-  // right-hand side minus the accumulated products, then the diagonal inverse
-  const int i = threadIdx.x % TS_B, rg = threadIdx.x / TS_B;
-  for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
-    const int r = e / TS_B, c = e % TS_B;
-    rs[r][c] -= accs[c][r];
+  // y_b = D_b (r_b - sum): this thread's right-hand sides of row i
+#pragma unroll
+  for (int u = 0; u < RPT; u++) {
+    const int r = RPT * grp + u;
+    double v = rs[r][i];
+#pragma unroll
+    for (int h = 0; h < 4; h++) v -= part[(h * NR + r) * TS_B + i];
+    rs[r][i] = v;
   }
   __syncthreads();
-  const double* D = sw_dyn;
-  constexpr int RPT = NR / 4;  // right-hand sides per thread
-  double out[RPT];
+  double y[RPT];
+  {
+    double y0[RPT], y1[RPT];
 #pragma unroll
-  for (int u = 0; u < RPT; u++) out[u] = 0.0;
-#pragma unroll 8
-  for (int m = 0; m < TS_B; m++) {
-    const double d = D[m * TS_B + i];
+    for (int u = 0; u < RPT; u++) y0[u] = y1[u] = 0.0;
+#pragma unroll 4
+    for (int m = 0; m < TS_B; m += 2) {
+      const double d0 = Ds[m * TS_B + i], d1 = Ds[(m + 1) * TS_B + i];
 #pragma unroll
-    for (int u = 0; u < RPT; u++) out[u] = fma(d, rs[RPT * rg + u][m], out[u]);
+      for (int u = 0; u < RPT; u++) {
+        y0[u] = fma(d0, rs[RPT * grp + u][m], y0[u]);
+        y1[u] = fma(d1, rs[RPT * grp + u][m + 1], y1[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < RPT; u++) y[u] = y0[u] + y1[u];
+  }
+  // the gate: x_b = y_b - M_b x_g
+  if (q > 0) {
+    const int g = LOWER ? b - 1 : b + 1;
+    if (threadIdx.x == 0 && !s_fail && !wait_flag(flags, g, epoch, err, 64)) s_fail = 1;
+    __syncthreads();
+    if (!s_fail) {
+      load_x((int64_t)g * TS_B);
+      __syncthreads();
+      double z0[RPT], z1[RPT];
+#pragma unroll
+      for (int u = 0; u < RPT; u++) z0[u] = z1[u] = 0.0;
+#pragma unroll 4
+      for (int m = 0; m < TS_B; m += 2) {
+        const double m0 = Ms[m * TS_B + i], m1 = Ms[(m + 1) * TS_B + i];
+#pragma unroll
+        for (int u = 0; u < RPT; u++) {
+          z0[u] = fma(m0, xs[RPT * grp + u][m], z0[u]);
+          z1[u] = fma(m1, xs[RPT * grp + u][m + 1], z1[u]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < RPT; u++) y[u] -= z0[u] + z1[u];
+    }
   }
   const double nan = __longlong_as_double(0x7ff8000000000000LL);
 #pragma unroll
   for (int u = 0; u < RPT; u++) {
-    const int r = RPT * rg + u;
-    if (r < nrhs && b0 + i < N) X[(int64_t)r * N + b0 + i] = s_fail ? nan : out[u];
+    const int r = RPT * grp + u;
+    if (r < nrhs && row < N) X[(int64_t)r * N + row] = s_fail ? nan : y[u];
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1016,22 +1371,38 @@ __global__ void __launch_bounds__(256) k_trsv_sweep(const float* __restrict__ LU
   }
 }
 
-// X[r, j] += c[j] D[r, j]; also the largest |c D| / |X| over all entries
-// (bits of a non-negative double compare like integers).
+// X[r, j] += c[j] D[r, j]; also, per right-hand side r, the largest
+// |c D| (maxes[2 r]) and |X| (maxes[2 r + 1]) -- non-negative doubles order
+// like their bit patterns.  Grid (blocks, nrhs): one warp-reduced atomic per
+// warp and quantity.
 __global__ void k_apply_correction(double* __restrict__ X, const double* __restrict__ D, const double* __restrict__ c,
-                                   int64_t N, int nrhs, unsigned long long* __restrict__ maxes) {
-  // maxes[2 r] = max_j |correction|, maxes[2 r + 1] = max_j |x| of right-hand side r
-  // (non-negative doubles order like their bit patterns)
-  int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (g >= N * nrhs) return;
-  int64_t j = g % N, r = g / N;
-  double d = c[j] * D[g];
-  double x = X[g] + d;
-  X[g] = x;
-  double ad = fabs(d), ax = fabs(x);
-  if (!(ad == ad) || !(ax == ax)) ad = 1e300;
-  atomicMax(&maxes[2 * r], (unsigned long long)__double_as_longlong(ad));
-  atomicMax(&maxes[2 * r + 1], (unsigned long long)__double_as_longlong(ax));
+                                   int64_t N, unsigned long long* __restrict__ maxes) {
+  const int r = blockIdx.y;
+  unsigned long long md = 0, mx = 0;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < N; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = (int64_t)r * N + j;
+    const double d = c[j] * D[g];
+    const double x = X[g] + d;
+    X[g] = x;
+    double ad = fabs(d);
+    const double ax = fabs(x);
+    if (!(ad == ad) || !(ax == ax)) ad = 1e300;
+    const unsigned long long bd = (unsigned long long)__double_as_longlong(ad);
+    const unsigned long long bx = (unsigned long long)__double_as_longlong(ax);
+    md = bd > md ? bd : md;
+    mx = bx > mx ? bx : mx;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long od = __shfl_xor_sync(0xffffffffu, md, o);
+    const unsigned long long ox = __shfl_xor_sync(0xffffffffu, mx, o);
+    md = od > md ? od : md;
+    mx = ox > mx ? ox : mx;
+  }
+  if (threadIdx.x % 32 == 0) {
+    atomicMax(&maxes[2 * r], md);
+    atomicMax(&maxes[2 * r + 1], mx);
+  }
 }
 
 template <class T>
@@ -1077,14 +1448,16 @@ extern "C" int64_t tb_gemm_tf32x3_workspace(int64_t M, int64_t N, int64_t K) {
 
 extern "C" int64_t tb_lu_nopiv_f32_tc_workspace(int64_t N) {
   if (N <= 0) return 0;
-  return gemm_pre_bytes(N, N, TC_PANEL);
+  const int64_t g = gemm_pre_bytes(N, N, TC_PANEL);
+  return g > LU_INV_BYTES ? g : LU_INV_BYTES;
 }
 
 extern "C" int tb_lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, void* work, int64_t work_bytes, int* err,
                                   tb_stream_t stream) {
   if (N < 0 || lda < N || (N > 0 && (!A || !err)) || N > 0x7fffffff) return BAD_ARG;
   if (N == 0) return OK;
-  if (work && work_bytes < tb_lu_nopiv_f32_tc_workspace(N)) return BAD_ARG;
+  if (!work || work_bytes < tb_lu_nopiv_f32_tc_workspace(N) || reinterpret_cast<uintptr_t>(work) % 16 != 0)
+    return BAD_ARG;
   return lu_nopiv_f32_tc(A, lda, N, err, static_cast<uint8_t*>(work), (cudaStream_t)stream);
 }
 
@@ -1106,10 +1479,11 @@ extern "C" int64_t tb_solve_mixed_workspace(int64_t N, int64_t nrhs) {
   if (N <= 0 || nrhs <= 0) return 0;
   const int64_t nblk = (N + TS_B - 1) / TS_B;
   // FP32 factors, column scales, correction / residual block, 2 * nrhs
-  // maxima, inverses of the diagonal blocks of both factors, sweep flags and
-  // the error word
+  // maxima, inverses of the diagonal blocks of both factors and their
+  // lookahead products, sweep flags and the error word
   return round256(N * N * 4) + round256(N * 8) + round256(nrhs * N * 8) + 256 +
-         2 * round256(nblk * TS_B * TS_B * 8) + round256(nblk * 4) + 256 + round256(gemm_pre_bytes(N, N, TC_PANEL));
+         4 * round256(nblk * TS_B * TS_B * 8) + round256(nblk * 4) + 256 +
+         round256(tb_lu_nopiv_f32_tc_workspace(N));
 }
 
 extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const double* F, double* X, int64_t nrhs,
@@ -1133,6 +1507,10 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   w += round256(nblk * TS_B * TS_B * 8);
   double* dinv_u = reinterpret_cast<double*>(w);
   w += round256(nblk * TS_B * TS_B * 8);
+  double* mla_l = reinterpret_cast<double*>(w);
+  w += round256(nblk * TS_B * TS_B * 8);
+  double* mla_u = reinterpret_cast<double*>(w);
+  w += round256(nblk * TS_B * TS_B * 8);
   int* flags = reinterpret_cast<int*>(w);
   w += round256(nblk * 4);
   int* err = reinterpret_cast<int*>(w);
@@ -1144,15 +1522,15 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   if (cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) return CUDA_ERR;
   int st = lu_nopiv_f32_tc(S, N, N, err, gemm_work, s);
   if (st != OK) return st;
-  k_diag_inverse<true><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_l);
-  k_diag_inverse<false><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_u);
+  k_diag_inverse<true><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_l, mla_l);
+  k_diag_inverse<false><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_u, mla_u);
   if (cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s) != cudaSuccess) return CUDA_ERR;
-  constexpr int SW_DYN = TS_B * TS_B * int(sizeof(double));  // 32 KB: the diagonal inverse
-  if (cudaFuncSetAttribute(k_trsv_sweep<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_DYN) != cudaSuccess ||
-      cudaFuncSetAttribute(k_trsv_sweep<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_DYN) != cudaSuccess ||
-      cudaFuncSetAttribute(k_trsv_sweep<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_DYN) !=
+  constexpr int SW8 = sweep_dyn_bytes<8>(), SW16 = sweep_dyn_bytes<16>();
+  if (cudaFuncSetAttribute(k_trsv_sweep<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW16) !=
           cudaSuccess ||
-      cudaFuncSetAttribute(k_trsv_sweep<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_DYN) !=
+      cudaFuncSetAttribute(k_trsv_sweep<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW16) !=
           cudaSuccess)
     return CUDA_ERR;
   int epoch = 0;
@@ -1167,14 +1545,17 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
     else
       k_residual<2><<<unsigned((N + 15) / 16), 256, 0, s>>>(A, lda, X, F, D, N, nr);
     if (nr <= 8) {
-      k_trsv_sweep<true, 8><<<unsigned(nblk), 256, SW_DYN, s>>>(S, N, N, dinv_l, D, nr, flags, ++epoch, err);
-      k_trsv_sweep<false, 8><<<unsigned(nblk), 256, SW_DYN, s>>>(S, N, N, dinv_u, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<true, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<false, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err);
     } else {
-      k_trsv_sweep<true, 16><<<unsigned(nblk), 256, SW_DYN, s>>>(S, N, N, dinv_l, D, nr, flags, ++epoch, err);
-      k_trsv_sweep<false, 16><<<unsigned(nblk), 256, SW_DYN, s>>>(S, N, N, dinv_u, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<true, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<false, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err);
     }
     if (cudaMemsetAsync(maxes, 0, sizeof(unsigned long long) * 2 * nr, s) != cudaSuccess) return CUDA_ERR;
-    k_apply_correction<<<unsigned((N * nrhs + 255) / 256), 256, 0, s>>>(X, D, c, N, nr, maxes);
+    {
+      const int64_t bx = (N + 255) / 256;
+      k_apply_correction<<<dim3(unsigned(bx < 256 ? bx : 256), unsigned(nr)), 256, 0, s>>>(X, D, c, N, maxes);
+    }
     unsigned long long bits[2 * MX_MAX_RHS];
     if (cudaMemcpyAsync(bits, maxes, sizeof(unsigned long long) * 2 * nr, cudaMemcpyDeviceToHost, s) != cudaSuccess)
       return CUDA_ERR;

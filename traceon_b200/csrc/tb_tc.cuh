@@ -92,6 +92,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t tx
                : "memory");
 }
 
+// Plain arrive (count 1) on `bar`.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Asynchronous bulk copy global -> this CTA's shared memory (no multicast),
 // completing `bytes` of transactions on `bar`.  Both addresses 16-byte
 // aligned, bytes a multiple of 16.

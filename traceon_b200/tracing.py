@@ -58,6 +58,36 @@ class TraceResult:
         self.rows = rows              # (n, max_rows, 7) or None
         self.nrows = nrows            # (n,) int64 or None
 
+    def plane_intersection(self, p0, normal):
+        """Crossing of every stored trajectory with the plane through p0
+        with normal `normal`, nearest the trajectory's end, by linear
+        interpolation (traceon/tracing.py:247-272 for one trajectory), on the
+        device.  Needs a trace with max_rows > 0.  Returns device tensors
+        (out (n, 7) t, x..vz, NaN where none; found (n) bool)."""
+        if self.rows is None:
+            raise ValueError('plane_intersection needs stored trajectories (trace with max_rows > 0)')
+        return B.dev_plane_intersection_rows(self.rows, self.nrows, p0, normal)
+
+    def xy_plane_intersection(self, z):
+        return self.plane_intersection([0, 0, z], [0, 0, 1])
+
+    def xz_plane_intersection(self, y):
+        return self.plane_intersection([0, y, 0], [0, 1, 0])
+
+    def yz_plane_intersection(self, x):
+        return self.plane_intersection([x, 0, 0], [1, 0, 0])
+
+    def axis_intersection(self):
+        """z of each trajectory's crossing of x = 0 (traceon/tracing.py:317-335),
+        a device tensor (n,); NaN where there is none."""
+        return self.yz_plane_intersection(0.0)[0][:, 3]
+
+    def focus_position(self, plane=False):
+        """Least-squares focus of the traced beam from its final states
+        (traceon/focus.py:9-42), or from the exit-plane crossings when
+        `plane`: a device tensor (3,) = (x, y, z)."""
+        return B.dev_focus_position(self.plane if plane else self.final)
+
 
 class Tracer:
     """General tracer (traceon/tracing.py:104-245) on the GPU."""
