@@ -54,6 +54,22 @@ def test_solvers_agree_with_lapack(cuda, n):
     assert _close(X.cpu().numpy(), X_ref) < 1e-10
 
 
+@pytest.mark.parametrize('nrhs', [1, 9, 16])
+def test_mixed_solve_right_hand_side_counts(cuda, nrhs):
+    """1, 9 and 16 (the maximum) right-hand sides against LAPACK on a
+    1,100-element matrix (the last sweep block partial); 17 are refused."""
+    import torch
+    A, F = _matrix(cuda, 1100)
+    rng = np.random.default_rng(nrhs)
+    F = np.vstack([F, rng.normal(size=(16, 1100))])[:nrhs]
+    X_ref = np.linalg.solve(A.cpu().numpy(), F.T).T
+    X, iters, rel = cuda.dev_solve_mixed(A, torch.as_tensor(F, device='cuda'))
+    assert iters <= 8 and rel <= 1e-12
+    assert _close(X.cpu().numpy(), X_ref) < 1e-10
+    with pytest.raises(cuda.BackendError):
+        cuda.dev_solve_mixed(A, torch.as_tensor(np.vstack([F] * 17)[:17], device='cuda'))
+
+
 def test_mixed_solve_reports_failure_and_solver_falls_back(cuda):
     """A system that needs pivoting (zero diagonal): the unpivoted mixed
     solve reports failure, and the solver then uses the pivoted FP64 LU."""

@@ -1096,7 +1096,7 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
 
 // ---------------------------------------------------------------- sweeps
 // One launch per triangular sweep of the refinement's correction equation.
-// CTA q owns row block b (64 rows; b = q for the forward sweep with the unit
+// CTA q owns row block b (128 rows; b = q for the forward sweep with the unit
 // lower factor, b = nblk - 1 - q for the backward sweep with the upper
 // factor), so every block it depends on belongs to a CTA launched before it.
 //
@@ -1104,14 +1104,16 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
 // published last before b (g = b - 1 forward, b + 1 backward):
 //   x_b = y_b - M_b x_g,   y_b = D_b (r_b - sum_{j != g} T_bj x_j),   M_b = D_b T_bg.
 // y_b needs only blocks published before g, so the CTA finishes it while it
-// waits; the step that gates the next block is one 64 x 64 FP64
+// waits; the step that gates the next block is one 128 x 128 FP64
 // matrix-vector product with the freshly published x_g.  D_b and M_b are
 // computed once per factorisation (k_diag_inverse) in FP64 from the FP32
 // factor values.  Published blocks: solution to X, then flags[b] = epoch
 // (release / acquire).  Waits are bounded: after TRSV_WAIT_CYCLES the CTA
 // records an error and writes NaN, which the refinement reports as
 // non-convergence.
-constexpr int TS_B = 64;
+constexpr int TS_B = 128;
+constexpr int SW_THREADS = 512;
+constexpr int SW_NR = 8;  // right-hand sides per sweep launch
 constexpr long long TRSV_WAIT_CYCLES = 2000000000LL;  // ~1 s
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -1141,15 +1143,18 @@ __device__ __forceinline__ bool wait_flag(const int* flags, int j, int epoch, in
 
 // For row block b of the unit lower (LOWER) or upper triangle of LU:
 // Dinv[b] = T_bb^-1 and Mla[b] = T_bb^-1 T_bg (g = b - 1 / b + 1; zero when
-// b has no such neighbour), both 64 x 64 FP64 stored column-major
-// (element (i, m) at m * 64 + i); rows / columns beyond N are the identity
-// in T_bb and zero in T_bg.  One CTA of 64 threads per block, one column per
-// thread.
+// b has no such neighbour), both 128 x 128 FP64 stored column-major
+// (element (i, m) at m * 128 + i); rows / columns beyond N are the identity
+// in T_bb and zero in T_bg.  One CTA of 128 threads per block, one column
+// per thread; dynamic shared memory DI_SMEM.
+constexpr int DI_SMEM = TS_B * TS_B * int(sizeof(float) + sizeof(double));
+
 template <bool LOWER>
 __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__ LU, int64_t lda, int64_t N,
                                                       double* __restrict__ Dinv, double* __restrict__ Mla) {
-  __shared__ float T[TS_B][TS_B];    // the factor block (FP32 values, exact)
-  __shared__ double Xc[TS_B][TS_B];  // Xc[row][col]; thread k owns column k
+  extern __shared__ __align__(16) unsigned char di_dyn[];
+  double(*Xc)[TS_B] = reinterpret_cast<double(*)[TS_B]>(di_dyn);  // Xc[row][col]; thread k owns column k
+  float(*T)[TS_B] = reinterpret_cast<float(*)[TS_B]>(di_dyn + TS_B * TS_B * sizeof(double));  // the factor block
   const int nblk = int((N + TS_B - 1) / TS_B);
   const int64_t b0 = (int64_t)blockIdx.x * TS_B;
   const int nb = N - b0 < TS_B ? int(N - b0) : TS_B;
@@ -1166,15 +1171,25 @@ __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__
   const int k = threadIdx.x;  // column k of the inverse: T x = e_k
   if (LOWER) {
     for (int i = 0; i < TS_B; i++) {
-      double v = (i == k) ? 1.0 : 0.0;
-      for (int m = 0; m < i; m++) v = fma(-double(T[i][m]), Xc[m][k], v);
-      Xc[i][k] = v;
+      double v0 = (i == k) ? 1.0 : 0.0, v1 = 0.0;
+      int m = 0;
+      for (; m + 1 < i; m += 2) {
+        v0 = fma(-double(T[i][m]), Xc[m][k], v0);
+        v1 = fma(-double(T[i][m + 1]), Xc[m + 1][k], v1);
+      }
+      if (m < i) v0 = fma(-double(T[i][m]), Xc[m][k], v0);
+      Xc[i][k] = v0 + v1;
     }
   } else {
     for (int i = TS_B - 1; i >= 0; i--) {
-      double v = (i == k) ? 1.0 : 0.0;
-      for (int m = i + 1; m < TS_B; m++) v = fma(-double(T[i][m]), Xc[m][k], v);
-      Xc[i][k] = v / double(T[i][i]);
+      double v0 = (i == k) ? 1.0 : 0.0, v1 = 0.0;
+      int m = i + 1;
+      for (; m + 1 < TS_B; m += 2) {
+        v0 = fma(-double(T[i][m]), Xc[m][k], v0);
+        v1 = fma(-double(T[i][m + 1]), Xc[m + 1][k], v1);
+      }
+      if (m < TS_B) v0 = fma(-double(T[i][m]), Xc[m][k], v0);
+      Xc[i][k] = (v0 + v1) / double(T[i][i]);
     }
   }
   __syncthreads();
@@ -1204,66 +1219,58 @@ __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__
   }
 }
 
-// X (nrhs x N, row r at X + r N) <- T^-1 X with T the unit lower (LOWER) or
-// upper triangle of LU, in the lookahead form above.  256 threads: thread
-// (i, grp) = (tid % 64, tid / 64) accumulates row i of the block over
-// columns 16 grp .. 16 grp + 15 of every tile before the gate (16 factor
-// values prefetched into registers one tile ahead, NR right-hand sides in
-// registers; the four column groups meet in shared memory once, in a fixed
-// order), and owns right-hand sides NR/4 grp .. NR/4 grp + NR/4 - 1 of row i
-// in the two matrix-vector products.  Dynamic shared memory: D_b, M_b
-// (64 KB) and the column groups' partial sums (NR * 2 KB).
-// flags[blk] == epoch marks a published block.
-template <int NR>
-constexpr int sweep_dyn_bytes() {
-  return 2 * TS_B * TS_B * int(sizeof(double)) + 4 * NR * TS_B * int(sizeof(double));
-}
+// X (nrhs x N, row r at X + r N, nrhs <= 8) <- T^-1 X with T the unit lower
+// (LOWER) or upper triangle of LU, in the lookahead form above.  512
+// threads: thread (i, grp) = (tid % 128, tid / 128) accumulates row i of the
+// block over columns 32 grp .. 32 grp + 31 of every tile before the gate (32
+// factor values prefetched into registers one tile ahead, 8 right-hand
+// sides in registers; the four column groups meet in shared memory once, in
+// a fixed order), and owns right-hand sides 2 grp, 2 grp + 1 of row i in the
+// two matrix-vector products (D_b read through L2 while the CTA waits, M_b
+// staged in shared memory).  One CTA per SM.
+constexpr int SW_SMEM = TS_B * TS_B * int(sizeof(double)) + 4 * SW_NR * TS_B * int(sizeof(double));
 
-template <bool LOWER, int NR>
-__global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
-                                                   const double* __restrict__ Dinv, const double* __restrict__ Mla,
-                                                   double* __restrict__ X, int nrhs, int* __restrict__ flags,
-                                                   int epoch, int* __restrict__ err) {
+template <bool LOWER>
+__global__ void __launch_bounds__(SW_THREADS, 1) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
+                                                             const double* __restrict__ Dinv,
+                                                             const double* __restrict__ Mla, double* __restrict__ X,
+                                                             int nrhs, int* __restrict__ flags, int epoch,
+                                                             int* __restrict__ err) {
   extern __shared__ __align__(16) double sw_dyn[];
-  double* Ds = sw_dyn;                    // D_b, column-major
-  double* Ms = sw_dyn + TS_B * TS_B;      // M_b, column-major
-  double* part = Ms + TS_B * TS_B;        // part[(grp * NR + r) * 64 + i]
-  __shared__ __align__(16) double xs[NR][TS_B];  // a published block's solution
-  __shared__ double rs[NR][TS_B];                // this block's right-hand side
+  double* Ms = sw_dyn;                // M_b, column-major
+  double* part = Ms + TS_B * TS_B;    // part[(grp * SW_NR + r) * 128 + i]
+  __shared__ __align__(16) double xs[SW_NR][TS_B];  // a published block's solution
+  __shared__ double rs[SW_NR][TS_B];                // this block's right-hand side
   __shared__ int s_fail;
-  constexpr int RPT = NR / 4;  // right-hand sides per thread in the products
+  constexpr int RPT = SW_NR / 4;  // right-hand sides per thread in the products
   const int nblk = int((N + TS_B - 1) / TS_B);
   const int q = blockIdx.x;
   const int b = LOWER ? q : nblk - 1 - q;
   const int64_t b0 = (int64_t)b * TS_B;
   const int i = threadIdx.x % TS_B, grp = threadIdx.x / TS_B;
-  // everything that does not depend on other blocks first
+  const double* Dg = Dinv + (int64_t)b * TS_B * TS_B;
   {
-    const double* Dg = Dinv + (int64_t)b * TS_B * TS_B;
     const double* Mg = Mla + (int64_t)b * TS_B * TS_B;
-    for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) {
-      Ds[e] = Dg[e];
-      Ms[e] = Mg[e];
-    }
+    for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) Ms[e] = Mg[e];
   }
-  for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
+  for (int e = threadIdx.x; e < SW_NR * TS_B; e += blockDim.x) {
     const int r = e / TS_B, c = e % TS_B;
     rs[r][c] = (r < nrhs && b0 + c < N) ? X[(int64_t)r * N + b0 + c] : 0.0;
   }
   if (threadIdx.x == 0) s_fail = 0;
   __syncthreads();
-  double acc[NR];
+  double acc[SW_NR];
 #pragma unroll
-  for (int r = 0; r < NR; r++) acc[r] = 0.0;
+  for (int r = 0; r < SW_NR; r++) acc[r] = 0.0;
   const int64_t row = b0 + i;
   const bool vec4 = (lda % 4) == 0 && (reinterpret_cast<uintptr_t>(LU) % 16) == 0;
-  float lv[16];  // row i, columns 16 grp .. 16 grp + 15 of the next tile
+  float lv[32];  // row i, columns 32 grp .. 32 grp + 31 of the next tile
   auto load_lu = [&](int j) {
-    const int64_t j0 = (int64_t)j * TS_B + 16 * grp;
-    if (vec4 && row < N && j0 + 16 <= N) {
+    const int64_t j0 = (int64_t)j * TS_B + 32 * grp;
+    if (vec4 && row < N && j0 + 32 <= N) {
       const float4* p = reinterpret_cast<const float4*>(LU + row * lda + j0);
 #pragma unroll
-      for (int v = 0; v < 4; v++) {
+      for (int v = 0; v < 8; v++) {
         const float4 f = __ldg(p + v);
         lv[4 * v] = f.x;
         lv[4 * v + 1] = f.y;
@@ -1272,11 +1279,11 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
       }
     } else {
 #pragma unroll
-      for (int c = 0; c < 16; c++) lv[c] = (row < N && j0 + c < N) ? LU[row * lda + j0 + c] : 0.f;
+      for (int c = 0; c < 32; c++) lv[c] = (row < N && j0 + c < N) ? LU[row * lda + j0 + c] : 0.f;
     }
   };
   auto load_x = [&](int64_t j0) {  // published by another CTA: read via L2
-    for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
+    for (int e = threadIdx.x; e < SW_NR * TS_B; e += blockDim.x) {
       const int r = e / TS_B, c = e % TS_B;
       xs[r][c] = (r < nrhs && j0 + c < N) ? __ldcg(X + (int64_t)r * N + j0 + c) : 0.0;
     }
@@ -1290,22 +1297,22 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
     if (s_fail) break;
     load_x((int64_t)j * TS_B);
     __syncthreads();
-    float lc[16];
+    float lc[32];
 #pragma unroll
-    for (int c = 0; c < 16; c++) lc[c] = lv[c];
+    for (int c = 0; c < 32; c++) lc[c] = lv[c];
     if (t + 1 < nacc) load_lu(LOWER ? t + 1 : nblk - 2 - t);
 #pragma unroll
-    for (int c = 0; c < 16; c += 2) {
+    for (int c = 0; c < 32; c += 2) {
 #pragma unroll
-      for (int r = 0; r < NR; r++) {
-        const double2 x = *reinterpret_cast<const double2*>(&xs[r][16 * grp + c]);
+      for (int r = 0; r < SW_NR; r++) {
+        const double2 x = *reinterpret_cast<const double2*>(&xs[r][32 * grp + c]);
         acc[r] = fma(double(lc[c]), x.x, acc[r]);
         acc[r] = fma(double(lc[c + 1]), x.y, acc[r]);
       }
     }
   }
 #pragma unroll
-  for (int r = 0; r < NR; r++) part[(grp * NR + r) * TS_B + i] = acc[r];
+  for (int r = 0; r < SW_NR; r++) part[(grp * SW_NR + r) * TS_B + i] = acc[r];
   __syncthreads();
   // y_b = D_b (r_b - sum): this thread's right-hand sides of row i
 #pragma unroll
@@ -1313,7 +1320,7 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
     const int r = RPT * grp + u;
     double v = rs[r][i];
 #pragma unroll
-    for (int h = 0; h < 4; h++) v -= part[(h * NR + r) * TS_B + i];
+    for (int h = 0; h < 4; h++) v -= part[(h * SW_NR + r) * TS_B + i];
     rs[r][i] = v;
   }
   __syncthreads();
@@ -1324,7 +1331,7 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
     for (int u = 0; u < RPT; u++) y0[u] = y1[u] = 0.0;
 #pragma unroll 4
     for (int m = 0; m < TS_B; m += 2) {
-      const double d0 = Ds[m * TS_B + i], d1 = Ds[(m + 1) * TS_B + i];
+      const double d0 = __ldg(Dg + m * TS_B + i), d1 = __ldg(Dg + (m + 1) * TS_B + i);
 #pragma unroll
       for (int u = 0; u < RPT; u++) {
         y0[u] = fma(d0, rs[RPT * grp + u][m], y0[u]);
@@ -1522,34 +1529,35 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   if (cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) return CUDA_ERR;
   int st = lu_nopiv_f32_tc(S, N, N, err, gemm_work, s);
   if (st != OK) return st;
-  k_diag_inverse<true><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_l, mla_l);
-  k_diag_inverse<false><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_u, mla_u);
-  if (cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s) != cudaSuccess) return CUDA_ERR;
-  constexpr int SW8 = sweep_dyn_bytes<8>(), SW16 = sweep_dyn_bytes<16>();
-  if (cudaFuncSetAttribute(k_trsv_sweep<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
-      cudaFuncSetAttribute(k_trsv_sweep<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
-      cudaFuncSetAttribute(k_trsv_sweep<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW16) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(k_trsv_sweep<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW16) !=
-          cudaSuccess)
+  if (cudaFuncSetAttribute(k_trsv_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_SMEM) != cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_SMEM) != cudaSuccess ||
+      cudaFuncSetAttribute(k_diag_inverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, DI_SMEM) != cudaSuccess ||
+      cudaFuncSetAttribute(k_diag_inverse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, DI_SMEM) != cudaSuccess)
     return CUDA_ERR;
+  k_diag_inverse<true><<<unsigned(nblk), TS_B, DI_SMEM, s>>>(S, N, N, dinv_l, mla_l);
+  k_diag_inverse<false><<<unsigned(nblk), TS_B, DI_SMEM, s>>>(S, N, N, dinv_u, mla_u);
+  if (cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s) != cudaSuccess) return CUDA_ERR;
   int epoch = 0;
   if (cudaMemsetAsync(X, 0, sizeof(double) * N * nrhs, s) != cudaSuccess) return CUDA_ERR;
   const int nr = int(nrhs);
   int it = 0;
   double rel = 1e300;
   for (it = 1; it <= max_iter; it++) {
-    // D = F - A X (FP64), then D <- (L U)^-1 D with the FP32 factors
-    if (nr <= 8)
+    // D = F - A X (FP64; F itself while X is still zero), then
+    // D <- (L U)^-1 D with the FP32 factors
+    if (it == 1) {
+      if (cudaMemcpyAsync(D, F, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return CUDA_ERR;
+    } else if (nr <= 8) {
       k_residual<4><<<unsigned((N + 31) / 32), 256, 0, s>>>(A, lda, X, F, D, N, nr);
-    else
-      k_residual<2><<<unsigned((N + 15) / 16), 256, 0, s>>>(A, lda, X, F, D, N, nr);
-    if (nr <= 8) {
-      k_trsv_sweep<true, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err);
-      k_trsv_sweep<false, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err);
     } else {
-      k_trsv_sweep<true, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err);
-      k_trsv_sweep<false, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err);
+      k_residual<2><<<unsigned((N + 15) / 16), 256, 0, s>>>(A, lda, X, F, D, N, nr);
+    }
+    for (int r0 = 0; r0 < nr; r0 += SW_NR) {  // 8 right-hand sides per sweep
+      const int ng = nr - r0 < SW_NR ? nr - r0 : SW_NR;
+      double* Dg = D + (int64_t)r0 * N;
+      k_trsv_sweep<true><<<unsigned(nblk), SW_THREADS, SW_SMEM, s>>>(S, N, N, dinv_l, mla_l, Dg, ng, flags, ++epoch, err);
+      k_trsv_sweep<false><<<unsigned(nblk), SW_THREADS, SW_SMEM, s>>>(S, N, N, dinv_u, mla_u, Dg, ng, flags, ++epoch, err);
     }
     if (cudaMemsetAsync(maxes, 0, sizeof(unsigned long long) * 2 * nr, s) != cudaSuccess) return CUDA_ERR;
     {
