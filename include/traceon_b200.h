@@ -277,11 +277,10 @@ int tb_pack_sources(const double *charges, const double *jac, const double *pos,
  * numpy.linalg.solve (solver.py:173). */
 int tb_lu_nopiv_f64(double *A, int64_t lda, int64_t N, tb_stream_t stream);
 int tb_lu_nopiv_f32(float *A, int64_t lda, int64_t N, tb_stream_t stream);
-/* The same FP32 factorisation in 256-column panels: each 64-column step of
- * a panel in two launches (diagonal LU with the inverses of its triangles,
- * then the rows below), the trailing matrix updated on the tensor cores
- * (tcgen05, 3xTF32: TF32 head/tail split of both operands, FP32 accumulation
- * in tensor memory).  work: device scratch of
+/* The same FP32 factorisation in 256-column panels with the updates on the
+ * tensor cores (tcgen05, 3xTF32: TF32 head/tail split of both operands,
+ * FP32 accumulation in tensor memory); the trailing matrix is updated once
+ * per panel from operands pre-split into `work`.  work: device scratch of
  * tb_lu_nopiv_f32_tc_workspace(N) bytes, 16-byte aligned (required).  err
  * (device int) is set to 1 if a bounded wait inside a tensor-core kernel ran
  * out.  Used by tb_solve_mixed. */

@@ -128,8 +128,8 @@ def test_gemm_tf32x3_vs_fp64(cuda, M, N, K, presplit):
 
 @pytest.mark.parametrize('n', [700, 1000])
 def test_lu_nopiv_tc_factors(cuda, n):
-    """The FP32 LU of the mixed solve (256-column panels: fused panel steps,
-    tensor-core trailing updates): on BEM matrices of 700 elements (three
+    """The FP32 LU of the mixed solve (256-column panels, tensor-core
+    updates): on BEM matrices of 700 elements (three
     panels, the last partial, 700 = 10 x 64 + 60) and 1,000 elements, L U
     reproduces the column-equilibrated FP32 matrix to FP32 accuracy."""
     import torch

@@ -147,6 +147,186 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------- FP32 panel kernels
+// Panel kernels of lu_nopiv_f32_tc (64-wide blocks).
+
+// D (the nb x nb diagonal block at (k0, k0)) <- its LU factors in place.
+// Thread t owns column j = t % 64 of rows t / 64 + 4 s (s = 0..15) in
+// registers; at step k the owners publish column k and row k to shared
+// memory (double-buffered by the parity of k: one barrier per step) and
+// every thread updates its elements with the pivot's reciprocal.  Fully
+// unrolled (k and s are constants in every iteration, so no dynamic
+// register indexing).  Rows and columns beyond nb are the identity.
+__global__ void __launch_bounds__(256) k_diag_lu_f32(float* __restrict__ A, int64_t lda, int64_t k0, int nb) {
+  __shared__ float colk[2][MX_NB], rowk[2][MX_NB];
+  const int j = threadIdx.x % MX_NB, i0 = threadIdx.x / MX_NB;
+  float v[16];
+#pragma unroll
+  for (int sI = 0; sI < 16; sI++) {
+    const int i = i0 + 4 * sI;
+    v[sI] = (i < nb && j < nb) ? A[(k0 + i) * lda + k0 + j] : (i == j ? 1.f : 0.f);
+  }
+#pragma unroll
+  for (int k = 0; k < MX_NB - 1; k++) {
+    if (k >= nb - 1) break;
+    const int buf = k & 1;
+    if (j == k) {
+#pragma unroll
+      for (int sI = 0; sI < 16; sI++) colk[buf][i0 + 4 * sI] = v[sI];
+    }
+    if (i0 == (k & 3)) rowk[buf][j] = v[k >> 2];
+    __syncthreads();
+    const float inv = 1.f / rowk[buf][k];
+    const float u = rowk[buf][j];
+#pragma unroll
+    for (int sI = 0; sI < 16; sI++) {
+      const int i = i0 + 4 * sI;
+      if (i > k) {
+        const float l = colk[buf][i] * inv;
+        if (j == k)
+          v[sI] = l;
+        else if (j > k)
+          v[sI] = fmaf(-l, u, v[sI]);
+      }
+    }
+  }
+#pragma unroll
+  for (int sI = 0; sI < 16; sI++) {
+    const int i = i0 + 4 * sI;
+    if (i < nb && j < nb) A[(k0 + i) * lda + k0 + j] = v[sI];
+  }
+}
+
+// Forward substitution on the 64-long vectors V[.][t] (one per thread, in
+// shared memory, V[m][t] = element m): x_i = (v_i - sum_{p < i} C[p][i] x_p)
+// times C[i][i] when DIAG (the caller stores the reciprocal pivots on the
+// diagonal of C), unit diagonal otherwise.  Blocked by 8: the 8 unknowns of
+// a block stay in registers while every finished unknown p < block is
+// applied to all 8 (two 16-byte broadcast reads of C per p), then the block
+// is solved in registers.
+constexpr int TRSM_COLS = 128;
+template <bool DIAG>
+__device__ __forceinline__ void solve_vectors(float (*V)[TRSM_COLS], const float (*C)[MX_NB], int t) {
+#pragma unroll 1
+  for (int b0 = 0; b0 < MX_NB; b0 += 8) {
+    float x[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) x[c] = V[b0 + c][t];
+#pragma unroll 4
+    for (int p = 0; p < b0; p++) {
+      const float xp = V[p][t];
+      const float4 c0 = *reinterpret_cast<const float4*>(&C[p][b0]);
+      const float4 c1 = *reinterpret_cast<const float4*>(&C[p][b0 + 4]);
+      x[0] = fmaf(-c0.x, xp, x[0]);
+      x[1] = fmaf(-c0.y, xp, x[1]);
+      x[2] = fmaf(-c0.z, xp, x[2]);
+      x[3] = fmaf(-c0.w, xp, x[3]);
+      x[4] = fmaf(-c1.x, xp, x[4]);
+      x[5] = fmaf(-c1.y, xp, x[5]);
+      x[6] = fmaf(-c1.z, xp, x[6]);
+      x[7] = fmaf(-c1.w, xp, x[7]);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+#pragma unroll
+      for (int q = 0; q < c; q++) x[c] = fmaf(-C[b0 + q][b0 + c], x[q], x[c]);
+      if (DIAG) x[c] *= C[b0 + c][b0 + c];
+      V[b0 + c][t] = x[c];
+    }
+  }
+}
+
+// rows r0 <= i < r1: A[i, k0:k0+nb] <- A[i, k0:k0+nb] U11^-1.  x U = a is
+// x_m = (a_m - sum_{p < m} x_p U[p][m]) / U[m][m]: solve_vectors with
+// C = U (row-major, as stored; reciprocal pivots on its diagonal).  128 rows
+// per CTA (thread = row), staged through shared memory (48 KB in all); all
+// loads of a thread are issued before the first use (one memory latency).
+__global__ void __launch_bounds__(TRSM_COLS)
+    k_trsm_right_f32(float* __restrict__ A, int64_t lda, int64_t r0, int64_t r1, int64_t k0, int nb) {
+  __shared__ __align__(16) float U[MX_NB][MX_NB];
+  __shared__ float V[MX_NB][TRSM_COLS];  // V[m][r]: element m of row r of the CTA
+  const int64_t rb = r0 + blockIdx.x * (int64_t)TRSM_COLS;
+  const int nrow = r1 - rb < TRSM_COLS ? int(r1 - rb) : TRSM_COLS;
+  const int r = threadIdx.x;  // lanes over rows: conflict-free shared stores
+  const bool vec = nb == MX_NB && lda % 4 == 0 && k0 % 4 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0;
+  float* arow = A + (rb + r) * lda + k0;
+  {
+    float a[MX_NB];
+    if (vec && r < nrow) {
+#pragma unroll
+      for (int q = 0; q < MX_NB / 4; q++) {
+        const float4 f = *reinterpret_cast<const float4*>(arow + 4 * q);
+        a[4 * q] = f.x;
+        a[4 * q + 1] = f.y;
+        a[4 * q + 2] = f.z;
+        a[4 * q + 3] = f.w;
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < MX_NB; m++) a[m] = (r < nrow && m < nb) ? arow[m] : 0.f;
+    }
+    float u[MX_NB * MX_NB / TRSM_COLS];
+#pragma unroll
+    for (int q = 0; q < MX_NB * MX_NB / TRSM_COLS; q++) {
+      const int e = threadIdx.x + TRSM_COLS * q, m = e / MX_NB, jj = e % MX_NB;
+      u[q] = (m < nb && jj < nb) ? A[(k0 + m) * lda + k0 + jj] : 0.f;
+    }
+#pragma unroll
+    for (int m = 0; m < MX_NB; m++) V[m][r] = a[m];
+#pragma unroll
+    for (int q = 0; q < MX_NB * MX_NB / TRSM_COLS; q++) {
+      const int e = threadIdx.x + TRSM_COLS * q, m = e / MX_NB, jj = e % MX_NB;
+      U[m][jj] = m == jj ? (m < nb ? __frcp_rn(u[q]) : 1.f) : u[q];
+    }
+  }
+  __syncthreads();
+  solve_vectors<true>(V, U, r);
+  if (r < nrow) {
+    if (vec) {
+#pragma unroll
+      for (int q = 0; q < MX_NB / 4; q++)
+        *reinterpret_cast<float4*>(arow + 4 * q) =
+            make_float4(V[4 * q][r], V[4 * q + 1][r], V[4 * q + 2][r], V[4 * q + 3][r]);
+    } else {
+      for (int m = 0; m < nb; m++) arow[m] = V[m][r];
+    }
+  }
+}
+
+// columns c0 <= c < c1: A[k0:k0+nb, c] <- L11^-1 A[k0:k0+nb, c] (L11 unit
+// lower): x_i = a_i - sum_{m < i} L[i][m] x_m, solve_vectors with
+// C[m][i] = L[i][m] (L transposed into shared memory).  128 columns per CTA;
+// all loads of a thread are issued before the first use.
+__global__ void __launch_bounds__(TRSM_COLS)
+    k_trsm_left_f32(float* __restrict__ A, int64_t lda, int64_t c0, int64_t c1, int64_t k0, int nb) {
+  __shared__ __align__(16) float Lt[MX_NB][MX_NB];
+  __shared__ float V[MX_NB][TRSM_COLS];  // V[i][c]: row i of column c of the CTA
+  const int64_t cb = c0 + blockIdx.x * (int64_t)TRSM_COLS;
+  const int ncol = c1 - cb < TRSM_COLS ? int(c1 - cb) : TRSM_COLS;
+  {
+    float a[MX_NB], l[MX_NB * MX_NB / TRSM_COLS];
+#pragma unroll
+    for (int ii = 0; ii < MX_NB; ii++)
+      a[ii] = (ii < nb && threadIdx.x < ncol) ? A[(k0 + ii) * lda + cb + threadIdx.x] : 0.f;
+#pragma unroll
+    for (int q = 0; q < MX_NB * MX_NB / TRSM_COLS; q++) {
+      const int e = threadIdx.x + TRSM_COLS * q, m = e / MX_NB, ii = e % MX_NB;  // lanes over ii
+      l[q] = (ii < nb && m < nb && m < ii) ? A[(k0 + ii) * lda + k0 + m] : 0.f;
+    }
+#pragma unroll
+    for (int ii = 0; ii < MX_NB; ii++) V[ii][threadIdx.x] = a[ii];
+#pragma unroll
+    for (int q = 0; q < MX_NB * MX_NB / TRSM_COLS; q++) {
+      const int e = threadIdx.x + TRSM_COLS * q;
+      Lt[e / MX_NB][e % MX_NB] = l[q];
+    }
+  }
+  __syncthreads();
+  solve_vectors<false>(V, Lt, threadIdx.x);
+  for (int ii = 0; ii < nb; ii++)
+    if (threadIdx.x < ncol) A[(k0 + ii) * lda + cb + threadIdx.x] = V[ii][threadIdx.x];
+}
+
 // ---------------------------------------------------------------- tensor cores
 // C (M x Nc, ldc) -= A (M x K, lda) . B (K x Nc, ldb), FP32 row-major, on
 // the 5th-generation tensor cores (tcgen05.mma kind::tf32) with 3xTF32:
@@ -649,364 +829,43 @@ static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, cons
   return launch_status();
 }
 
-// FP32 LU without pivoting, two-level blocked: panels of 256 columns; each
-// 64-column step of a panel is k_panel_head + k_panel_rows, the panel's
-// row block is one k_rowblock_step per step, and the trailing matrix is
-// updated once per panel on the tensor cores (K = 256, pre-split operands,
-// persistent).  work: the pre-split operand blocks of the trailing update;
-// its first LU_INV_BYTES also hold the inverses of the current panel's
-// diagonal blocks (free while the panel is factored).  err receives 1 if a
-// tensor-core wait ran out.
+// FP32 LU without pivoting, two-level blocked: panels of 256 columns are
+// factored with the 64-wide kernels above (diagonal block, triangular
+// solves) and tensor-core updates (K = 64) inside the panel and its row
+// block; the trailing matrix is updated once per panel by the persistent
+// tensor-core GEMM (K = 256) from operands pre-split into `work`.  err
+// receives 1 if a tensor-core wait ran out.
 constexpr int TC_PANEL = 256;
-constexpr int64_t LU_INV_BYTES = int64_t(TC_PANEL / 64) * 2 * 64 * 64 * int64_t(sizeof(float));
-// ---------------------------------------------------------------- fused panel steps
-// One 64-column step of a panel in two launches instead of four.
-//
-// k_panel_head (one CTA): LU of the 64 x 64 diagonal block, the inverses of its unit lower and upper triangles
-// (Li = L11^-1, Ui = U11^-1, written to `inv` for the next launch), and the
-// block row of U right of the block inside the panel, U12 = Li A12
-// (independent dot products).
-//
-// k_panel_rows (a CTA per 64 rows below the block): L21 = A21 Ui, then the
-// panel columns right of the block, A22 -= L21 U12 (FP32 FMA; a panel is at
-// most 256 wide, so U12 has at most 192 columns).
-//
-// Explicit inverses of the 64 x 64 diagonal triangles turn the triangular
-// solves into independent dot products; the factors only precondition the
-// FP64 refinement, whose convergence the solver checks.
-constexpr int PR_LD = MX_NB + 4;  // row stride of the transposed 64-row tiles (16-byte aligned rows)
-constexpr int PR_MAXR = TC_PANEL - MX_NB;  // columns of U12
-// T, Ui, Li, Lit (Li transposed), Xs (A12)
-constexpr int PH_SMEM = (MX_NB * (MX_NB + 1) + 2 * MX_NB * MX_NB + MX_NB * PR_LD + MX_NB * PR_MAXR) * int(sizeof(float));
-constexpr int PR_SMEM = (MX_NB * PR_LD + MX_NB * MX_NB + MX_NB * PR_MAXR) * int(sizeof(float));
-
-__global__ void __launch_bounds__(256) k_panel_head(float* __restrict__ A, int64_t lda, int64_t k0, int nb, int right,
-                                                   float* __restrict__ inv) {
-  extern __shared__ __align__(16) float ph_dyn[];
-  float(*T)[MX_NB + 1] = reinterpret_cast<float(*)[MX_NB + 1]>(ph_dyn);
-  float(*Ui)[MX_NB] = reinterpret_cast<float(*)[MX_NB]>(ph_dyn + MX_NB * (MX_NB + 1));
-  float(*Li)[MX_NB] = Ui + MX_NB;
-  float(*Lit)[PR_LD] = reinterpret_cast<float(*)[PR_LD]>(ph_dyn + MX_NB * (MX_NB + 1) + 2 * MX_NB * MX_NB);
-  float(*Xs)[PR_MAXR] =
-      reinterpret_cast<float(*)[PR_MAXR]>(ph_dyn + MX_NB * (MX_NB + 1) + 2 * MX_NB * MX_NB + MX_NB * PR_LD);
-  __shared__ float rpiv[MX_NB];  // reciprocal pivots, each formed once
-  const int jj = threadIdx.x % MX_NB, ig = threadIdx.x / MX_NB;
-  // LU of the diagonal block, right-looking in shared memory.  Step k
-  // updates only the trailing (nb - 1 - k)^2 block: thread (jj, ig) takes
-  // column k + 1 + jj and every 4th row from k + 1 + ig.  The multipliers
-  // are formed on the fly from the unscaled column k, which is scaled after
-  // the step's barrier (step k + 1 does not read it): one barrier per step.
-  // Thread 0 updates the next pivot (row and column k + 1 of its share) and
-  // forms its correctly rounded reciprocal for everyone.  Rows and columns
-  // beyond nb are the identity.
-#pragma unroll
-  for (int s = 0; s < 16; s++) {
-    const int i = ig + 4 * s;
-    T[i][jj] = (i < nb && jj < nb) ? A[(k0 + i) * lda + k0 + jj] : (i == jj ? 1.f : 0.f);
-  }
-  if (threadIdx.x == 0) rpiv[0] = __frcp_rn(T[0][0]);  // thread 0 loaded T[0][0]
-  __syncthreads();
-#pragma unroll 1
-  for (int k = 0; k < nb - 1; k++) {
-    const float rp = rpiv[k];
-    const int j = k + 1 + jj;
-    if (j < nb) {
-      const float u = T[k][j];
-#pragma unroll 4
-      for (int i = k + 1 + ig; i < nb; i += 4) T[i][j] = fmaf(-(T[i][k] * rp), u, T[i][j]);
-    }
-    if (threadIdx.x == 0) rpiv[k + 1] = __frcp_rn(T[k + 1][k + 1]);  // its own update of step k
-    __syncthreads();
-    if (k + 1 + threadIdx.x < nb) T[k + 1 + threadIdx.x][k] *= rp;
-  }
-  __syncthreads();
-  // inverses, one column per thread: threads 0..63 Ui, 64..127 Li (rows and
-  // columns beyond nb are the identity); two partial sums per element
-  if (threadIdx.x < MX_NB) {
-    const int k = threadIdx.x;
-#pragma unroll 1
-    for (int i = MX_NB - 1; i >= 0; i--) {
-      float s0 = (i == k) ? 1.f : 0.f, s1 = 0.f;
-      if (i <= k) {
-        int m = i + 1;
-        for (; m + 1 <= k; m += 2) {
-          s0 = fmaf(-T[i][m], Ui[m][k], s0);
-          s1 = fmaf(-T[i][m + 1], Ui[m + 1][k], s1);
-        }
-        if (m <= k) s0 = fmaf(-T[i][m], Ui[m][k], s0);
-      }
-      Ui[i][k] = i <= k ? (s0 + s1) * (i < nb ? rpiv[i] : 1.f) : 0.f;
-    }
-  } else if (threadIdx.x < 2 * MX_NB) {
-    const int k = threadIdx.x - MX_NB;
-#pragma unroll 1
-    for (int i = 0; i < MX_NB; i++) {
-      float s0 = (i == k) ? 1.f : 0.f, s1 = 0.f;
-      if (i > k) {
-        int m = k;
-        for (; m + 1 < i; m += 2) {
-          s0 = fmaf(-T[i][m], Li[m][k], s0);
-          s1 = fmaf(-T[i][m + 1], Li[m + 1][k], s1);
-        }
-        if (m < i) s0 = fmaf(-T[i][m], Li[m][k], s0);
-      }
-      Li[i][k] = i >= k ? s0 + s1 : 0.f;
-    }
-  }
-  __syncthreads();
-  // U12 = Li A12 (64 x right): thread (c, g) forms rows 16 g .. 16 g + 15 of
-  // columns c, c + 64, c + 128 as independent dot products, Li read
-  // transposed (Lit[m][i] = Li[i][m]) as 16-byte broadcasts
-  if (right > 0) {
-    for (int e = threadIdx.x; e < MX_NB * MX_NB; e += blockDim.x) Lit[e % MX_NB][e / MX_NB] = Li[e / MX_NB][e % MX_NB];
-    for (int e = threadIdx.x; e < MX_NB * right; e += blockDim.x) {
-      const int m = e / right, j = e % right;
-      Xs[m][j] = m < nb ? A[(k0 + m) * lda + k0 + nb + j] : 0.f;
-    }
-    __syncthreads();
-    const int c = threadIdx.x % MX_NB, g = threadIdx.x / MX_NB;
-    for (int j = c; j < right; j += MX_NB) {
-      float acc[16];
-#pragma unroll
-      for (int q = 0; q < 16; q++) acc[q] = 0.f;
-#pragma unroll 4
-      for (int m = 0; m < MX_NB; m++) {
-        const float w = Xs[m][j];
-        const float4* lr = reinterpret_cast<const float4*>(&Lit[m][16 * g]);
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-          const float4 y = lr[v];
-          acc[4 * v] = fmaf(y.x, w, acc[4 * v]);
-          acc[4 * v + 1] = fmaf(y.y, w, acc[4 * v + 1]);
-          acc[4 * v + 2] = fmaf(y.z, w, acc[4 * v + 2]);
-          acc[4 * v + 3] = fmaf(y.w, w, acc[4 * v + 3]);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < 16; q++)
-        if (16 * g + q < nb) A[(k0 + 16 * g + q) * lda + k0 + nb + j] = acc[q];
-    }
-  }
-  // the factored block and the inverses
-#pragma unroll
-  for (int s = 0; s < 16; s++) {
-    const int i = ig + 4 * s;
-    if (i < nb && jj < nb) A[(k0 + i) * lda + k0 + jj] = T[i][jj];
-  }
-  for (int e = threadIdx.x; e < MX_NB * MX_NB; e += blockDim.x) {
-    inv[e] = Ui[e / MX_NB][e % MX_NB];
-    inv[MX_NB * MX_NB + e] = Li[e / MX_NB][e % MX_NB];
-  }
-}
-
-// Rows r0 <= r < r1 (a CTA per 64): L21 = A21 Ui into A[r, k0:k0+64], then
-// A[r, k0+nb : k0+nb+right] -= L21 U12.  Thread (c, g) = (t % 64, t / 64)
-// computes rows 16 g .. 16 g + 15 of the CTA's 64 for column c; the 16 row
-// values of a k index are one broadcast 64-byte read of a transposed tile.
-__global__ void __launch_bounds__(256) k_panel_rows(float* __restrict__ A, int64_t lda, int64_t k0, int nb,
-                                                   int64_t r0, int64_t r1, int right, const float* __restrict__ inv) {
-  extern __shared__ __align__(16) float pr_dyn[];
-  float(*At)[PR_LD] = reinterpret_cast<float(*)[PR_LD]>(pr_dyn);          // At[m][r]: A21, then L21
-  float(*Us)[MX_NB] = reinterpret_cast<float(*)[MX_NB]>(pr_dyn + MX_NB * PR_LD);  // Ui
-  float(*U12)[PR_MAXR] = reinterpret_cast<float(*)[PR_MAXR]>(pr_dyn + MX_NB * PR_LD + MX_NB * MX_NB);
-  const int c = threadIdx.x % MX_NB, g = threadIdx.x / MX_NB;
-  const int64_t rb = r0 + blockIdx.x * (int64_t)MX_NB;
-  const int nrow = r1 - rb < MX_NB ? int(r1 - rb) : MX_NB;
-  {  // staging; all loads of a thread issued before the shared-memory stores
-    float a[16], u[16];
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const int e = threadIdx.x + 256 * q, m = e / MX_NB, r = e % MX_NB;  // lanes over rows r
-      a[q] = (r < nrow && m < nb) ? A[(rb + r) * lda + k0 + m] : 0.f;
-      u[q] = inv[e];
-    }
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const int e = threadIdx.x + 256 * q;
-      At[e / MX_NB][e % MX_NB] = a[q];
-      Us[e / MX_NB][e % MX_NB] = u[q];
-    }
-    for (int e = threadIdx.x; e < MX_NB * right; e += blockDim.x) {
-      const int m = e / right, j = e % right;
-      U12[m][j] = m < nb ? A[(k0 + m) * lda + k0 + nb + j] : 0.f;
-    }
-  }
-  __syncthreads();
-  float acc[16];
-#pragma unroll
-  for (int q = 0; q < 16; q++) acc[q] = 0.f;
-#pragma unroll 4
-  for (int m = 0; m < MX_NB; m++) {
-    const float w = Us[m][c];
-    const float4* ar = reinterpret_cast<const float4*>(&At[m][16 * g]);
-#pragma unroll
-    for (int v = 0; v < 4; v++) {
-      const float4 x = ar[v];
-      acc[4 * v] = fmaf(x.x, w, acc[4 * v]);
-      acc[4 * v + 1] = fmaf(x.y, w, acc[4 * v + 1]);
-      acc[4 * v + 2] = fmaf(x.z, w, acc[4 * v + 2]);
-      acc[4 * v + 3] = fmaf(x.w, w, acc[4 * v + 3]);
-    }
-  }
-  __syncthreads();  // every read of A21 is done: At becomes L21 (transposed)
-  if (c < nb) {
-    float4* lr = reinterpret_cast<float4*>(&At[c][16 * g]);
-#pragma unroll
-    for (int v = 0; v < 4; v++) lr[v] = make_float4(acc[4 * v], acc[4 * v + 1], acc[4 * v + 2], acc[4 * v + 3]);
-#pragma unroll
-    for (int q = 0; q < 16; q++)
-      if (16 * g + q < nrow) A[(rb + 16 * g + q) * lda + k0 + c] = acc[q];
-  } else {
-    float4* lr = reinterpret_cast<float4*>(&At[c][16 * g]);
-#pragma unroll
-    for (int v = 0; v < 4; v++) lr[v] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  if (right <= 0) return;
-  __syncthreads();
-  for (int j0 = 0; j0 < right; j0 += MX_NB) {
-    const int j = j0 + c;
-    float* out = A + (rb + 16 * g) * lda + k0 + nb + j;
-#pragma unroll
-    for (int q = 0; q < 16; q++) acc[q] = (j < right && 16 * g + q < nrow) ? out[q * lda] : 0.f;
-    if (j < right) {
-#pragma unroll 4
-      for (int m = 0; m < MX_NB; m++) {
-        const float w = U12[m][j];
-        const float4* lr = reinterpret_cast<const float4*>(&At[m][16 * g]);
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-          const float4 x = lr[v];
-          acc[4 * v] = fmaf(-x.x, w, acc[4 * v]);
-          acc[4 * v + 1] = fmaf(-x.y, w, acc[4 * v + 1]);
-          acc[4 * v + 2] = fmaf(-x.z, w, acc[4 * v + 2]);
-          acc[4 * v + 3] = fmaf(-x.w, w, acc[4 * v + 3]);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < 16; q++)
-        if (16 * g + q < nrow) out[q * lda] = acc[q];
-    }
-  }
-}
-
-// The panel's row block right of the panel, one 64-row step per launch:
-// X = Li A[k0:k0+64, cb:cb+64] (the block row of U), then the rows of the
-// panel below the step, A[k0+nb : pe, cb:cb+64] -= L[k0+nb : pe, k0:k0+nb] X.
-// A CTA per 64 columns (thread (c, g) = column c, rows 16 g .. 16 g + 15 of
-// a 64-row group); Li comes from the step's k_panel_head.
-constexpr int RB_MAXR = TC_PANEL - MX_NB;  // panel rows below a step
-constexpr int RB_LD = RB_MAXR + 4;
-constexpr int RB_SMEM = (MX_NB * MX_NB + MX_NB * PR_LD + MX_NB * RB_LD) * int(sizeof(float));
-
-__global__ void __launch_bounds__(256) k_rowblock_step(float* __restrict__ A, int64_t lda, int64_t k0, int nb,
-                                                      int rows, int64_t c0, int64_t c1, const float* __restrict__ li) {
-  extern __shared__ __align__(16) float rb_dyn[];
-  float(*Xs)[MX_NB] = reinterpret_cast<float(*)[MX_NB]>(rb_dyn);                 // Xs[m][c]
-  float(*Lit)[PR_LD] = reinterpret_cast<float(*)[PR_LD]>(rb_dyn + MX_NB * MX_NB);  // Lit[m][i] = Li[i][m]
-  float(*Lpt)[RB_LD] = reinterpret_cast<float(*)[RB_LD]>(rb_dyn + MX_NB * MX_NB + MX_NB * PR_LD);  // Lpt[m][r]
-  const int c = threadIdx.x % MX_NB, g = threadIdx.x / MX_NB;
-  const int64_t cb = c0 + blockIdx.x * (int64_t)MX_NB;
-  const bool col_ok = cb + c < c1;
-  {
-    float x[16], l[16];
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const int m = g + 4 * q;
-      x[q] = (m < nb && col_ok) ? A[(k0 + m) * lda + cb + c] : 0.f;
-      const int e = threadIdx.x + 256 * q;  // Li row-major: e = i * 64 + m
-      l[q] = li[e];
-    }
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-      Xs[g + 4 * q][c] = x[q];
-      const int e = threadIdx.x + 256 * q;
-      Lit[e % MX_NB][e / MX_NB] = l[q];
-    }
-    for (int e = threadIdx.x; e < rows * MX_NB; e += blockDim.x) {
-      const int r = e / MX_NB, m = e % MX_NB;
-      Lpt[m][r] = m < nb ? A[(k0 + nb + r) * lda + k0 + m] : 0.f;
-    }
-  }
-  __syncthreads();
-  float acc[16];
-#pragma unroll
-  for (int q = 0; q < 16; q++) acc[q] = 0.f;
-#pragma unroll 4
-  for (int m = 0; m < MX_NB; m++) {
-    const float w = Xs[m][c];
-    const float4* lr = reinterpret_cast<const float4*>(&Lit[m][16 * g]);
-#pragma unroll
-    for (int v = 0; v < 4; v++) {
-      const float4 y = lr[v];
-      acc[4 * v] = fmaf(y.x, w, acc[4 * v]);
-      acc[4 * v + 1] = fmaf(y.y, w, acc[4 * v + 1]);
-      acc[4 * v + 2] = fmaf(y.z, w, acc[4 * v + 2]);
-      acc[4 * v + 3] = fmaf(y.w, w, acc[4 * v + 3]);
-    }
-  }
-  __syncthreads();  // every read of the input X is done
-#pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const int i = 16 * g + q;
-    Xs[i][c] = acc[q];
-    if (i < nb && col_ok) A[(k0 + i) * lda + cb + c] = acc[q];
-  }
-  if (rows <= 0) return;
-  __syncthreads();
-  for (int r0 = 0; r0 < rows; r0 += MX_NB) {
-    float* out = A + (k0 + nb + r0 + 16 * g) * lda + cb + c;
-#pragma unroll
-    for (int q = 0; q < 16; q++) acc[q] = (col_ok && r0 + 16 * g + q < rows) ? out[q * lda] : 0.f;
-#pragma unroll 4
-    for (int m = 0; m < MX_NB; m++) {
-      const float w = Xs[m][c];
-      const float4* lr = reinterpret_cast<const float4*>(&Lpt[m][r0 + 16 * g]);
-#pragma unroll
-      for (int v = 0; v < 4; v++) {
-        const float4 y = lr[v];
-        acc[4 * v] = fmaf(-y.x, w, acc[4 * v]);
-        acc[4 * v + 1] = fmaf(-y.y, w, acc[4 * v + 1]);
-        acc[4 * v + 2] = fmaf(-y.z, w, acc[4 * v + 2]);
-        acc[4 * v + 3] = fmaf(-y.w, w, acc[4 * v + 3]);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 16; q++)
-      if (col_ok && r0 + 16 * g + q < rows) out[q * lda] = acc[q];
-  }
-}
-
-static bool g_attr_panel[64];
-
 static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* work, cudaStream_t s) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return CUDA_ERR;
-  if (dev >= 0 && dev < 64 && !g_attr_panel[dev]) {
-    if (cudaFuncSetAttribute(k_panel_head, cudaFuncAttributeMaxDynamicSharedMemorySize, PH_SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(k_panel_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(k_rowblock_step, cudaFuncAttributeMaxDynamicSharedMemorySize, RB_SMEM) != cudaSuccess)
-      return CUDA_ERR;
-    g_attr_panel[dev] = true;
-  }
-  float* inv = reinterpret_cast<float*>(work);  // per step of the panel: Ui (64 x 64), then Li
   for (int64_t p0 = 0; p0 < N; p0 += TC_PANEL) {
     const int64_t pe = p0 + TC_PANEL < N ? p0 + TC_PANEL : N;
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
       const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
-      const int right = int(pe - k0 - nb);
-      const int64_t below = N - k0 - nb;
-      float* iv = inv + ((k0 - p0) / MX_NB) * 2 * MX_NB * MX_NB;
-      k_panel_head<<<1, 256, PH_SMEM, s>>>(A, lda, k0, nb, right, iv);
+      k_diag_lu_f32<<<1, 256, 0, s>>>(A, lda, k0, nb);
+      const int64_t below = N - k0 - nb, right = pe - k0 - nb;
       if (below > 0)
-        k_panel_rows<<<unsigned((below + MX_NB - 1) / MX_NB), 256, PR_SMEM, s>>>(A, lda, k0, nb, k0 + nb, N, right, iv);
+        k_trsm_right_f32<<<unsigned((below + TRSM_COLS - 1) / TRSM_COLS), TRSM_COLS, 0, s>>>(A, lda, k0 + nb, N, k0,
+                                                                                            nb);
+      if (right > 0) {
+        k_trsm_left_f32<<<unsigned((right + TRSM_COLS - 1) / TRSM_COLS), TRSM_COLS, 0, s>>>(A, lda, k0 + nb, pe, k0,
+                                                                                           nb);
+        const int st = gemm_sub_tf32x3(A + (k0 + nb) * lda + k0 + nb, lda, A + (k0 + nb) * lda + k0, lda,
+                                       A + k0 * lda + k0 + nb, lda, below, right, nb, err, s);
+        if (st != OK) return st;
+      }
     }
     const int64_t rest = N - pe;
     if (rest <= 0) break;
+    // row block right of the panel: U12 = L11^-1 A12, 64 rows at a time
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
       const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
-      const float* li = inv + ((k0 - p0) / MX_NB) * 2 * MX_NB * MX_NB + MX_NB * MX_NB;
-      k_rowblock_step<<<unsigned((rest + MX_NB - 1) / MX_NB), 256, RB_SMEM, s>>>(A, lda, k0, nb, int(pe - k0 - nb), pe,
-                                                                                N, li);
+      k_trsm_left_f32<<<unsigned((rest + TRSM_COLS - 1) / TRSM_COLS), TRSM_COLS, 0, s>>>(A, lda, pe, N, k0, nb);
+      const int64_t rows = pe - k0 - nb;
+      if (rows > 0) {
+        const int st = gemm_sub_tf32x3(A + (k0 + nb) * lda + pe, lda, A + (k0 + nb) * lda + k0, lda, A + k0 * lda + pe,
+                                       lda, rows, rest, nb, err, s);
+        if (st != OK) return st;
+      }
     }
     const int st = gemm_sub_pre(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest,
                                 int(pe - p0), work, err, s);
@@ -1096,7 +955,7 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
 
 // ---------------------------------------------------------------- sweeps
 // One launch per triangular sweep of the refinement's correction equation.
-// CTA q owns row block b (128 rows; b = q for the forward sweep with the unit
+// CTA q owns row block b (64 rows; b = q for the forward sweep with the unit
 // lower factor, b = nblk - 1 - q for the backward sweep with the upper
 // factor), so every block it depends on belongs to a CTA launched before it.
 //
@@ -1104,16 +963,14 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
 // published last before b (g = b - 1 forward, b + 1 backward):
 //   x_b = y_b - M_b x_g,   y_b = D_b (r_b - sum_{j != g} T_bj x_j),   M_b = D_b T_bg.
 // y_b needs only blocks published before g, so the CTA finishes it while it
-// waits; the step that gates the next block is one 128 x 128 FP64
+// waits; the step that gates the next block is one 64 x 64 FP64
 // matrix-vector product with the freshly published x_g.  D_b and M_b are
 // computed once per factorisation (k_diag_inverse) in FP64 from the FP32
 // factor values.  Published blocks: solution to X, then flags[b] = epoch
 // (release / acquire).  Waits are bounded: after TRSV_WAIT_CYCLES the CTA
 // records an error and writes NaN, which the refinement reports as
 // non-convergence.
-constexpr int TS_B = 128;
-constexpr int SW_THREADS = 512;
-constexpr int SW_NR = 8;  // right-hand sides per sweep launch
+constexpr int TS_B = 64;
 constexpr long long TRSV_WAIT_CYCLES = 2000000000LL;  // ~1 s
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -1143,18 +1000,15 @@ __device__ __forceinline__ bool wait_flag(const int* flags, int j, int epoch, in
 
 // For row block b of the unit lower (LOWER) or upper triangle of LU:
 // Dinv[b] = T_bb^-1 and Mla[b] = T_bb^-1 T_bg (g = b - 1 / b + 1; zero when
-// b has no such neighbour), both 128 x 128 FP64 stored column-major
-// (element (i, m) at m * 128 + i); rows / columns beyond N are the identity
-// in T_bb and zero in T_bg.  One CTA of 128 threads per block, one column
-// per thread; dynamic shared memory DI_SMEM.
-constexpr int DI_SMEM = TS_B * TS_B * int(sizeof(float) + sizeof(double));
-
+// b has no such neighbour), both 64 x 64 FP64 stored column-major
+// (element (i, m) at m * 64 + i); rows / columns beyond N are the identity
+// in T_bb and zero in T_bg.  One CTA of 64 threads per block, one column per
+// thread.
 template <bool LOWER>
 __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__ LU, int64_t lda, int64_t N,
                                                       double* __restrict__ Dinv, double* __restrict__ Mla) {
-  extern __shared__ __align__(16) unsigned char di_dyn[];
-  double(*Xc)[TS_B] = reinterpret_cast<double(*)[TS_B]>(di_dyn);  // Xc[row][col]; thread k owns column k
-  float(*T)[TS_B] = reinterpret_cast<float(*)[TS_B]>(di_dyn + TS_B * TS_B * sizeof(double));  // the factor block
+  __shared__ float T[TS_B][TS_B];    // the factor block (FP32 values, exact)
+  __shared__ double Xc[TS_B][TS_B];  // Xc[row][col]; thread k owns column k
   const int nblk = int((N + TS_B - 1) / TS_B);
   const int64_t b0 = (int64_t)blockIdx.x * TS_B;
   const int nb = N - b0 < TS_B ? int(N - b0) : TS_B;
@@ -1171,25 +1025,15 @@ __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__
   const int k = threadIdx.x;  // column k of the inverse: T x = e_k
   if (LOWER) {
     for (int i = 0; i < TS_B; i++) {
-      double v0 = (i == k) ? 1.0 : 0.0, v1 = 0.0;
-      int m = 0;
-      for (; m + 1 < i; m += 2) {
-        v0 = fma(-double(T[i][m]), Xc[m][k], v0);
-        v1 = fma(-double(T[i][m + 1]), Xc[m + 1][k], v1);
-      }
-      if (m < i) v0 = fma(-double(T[i][m]), Xc[m][k], v0);
-      Xc[i][k] = v0 + v1;
+      double v = (i == k) ? 1.0 : 0.0;
+      for (int m = 0; m < i; m++) v = fma(-double(T[i][m]), Xc[m][k], v);
+      Xc[i][k] = v;
     }
   } else {
     for (int i = TS_B - 1; i >= 0; i--) {
-      double v0 = (i == k) ? 1.0 : 0.0, v1 = 0.0;
-      int m = i + 1;
-      for (; m + 1 < TS_B; m += 2) {
-        v0 = fma(-double(T[i][m]), Xc[m][k], v0);
-        v1 = fma(-double(T[i][m + 1]), Xc[m + 1][k], v1);
-      }
-      if (m < TS_B) v0 = fma(-double(T[i][m]), Xc[m][k], v0);
-      Xc[i][k] = (v0 + v1) / double(T[i][i]);
+      double v = (i == k) ? 1.0 : 0.0;
+      for (int m = i + 1; m < TS_B; m++) v = fma(-double(T[i][m]), Xc[m][k], v);
+      Xc[i][k] = v / double(T[i][i]);
     }
   }
   __syncthreads();
@@ -1219,58 +1063,66 @@ __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__
   }
 }
 
-// X (nrhs x N, row r at X + r N, nrhs <= 8) <- T^-1 X with T the unit lower
-// (LOWER) or upper triangle of LU, in the lookahead form above.  512
-// threads: thread (i, grp) = (tid % 128, tid / 128) accumulates row i of the
-// block over columns 32 grp .. 32 grp + 31 of every tile before the gate (32
-// factor values prefetched into registers one tile ahead, 8 right-hand
-// sides in registers; the four column groups meet in shared memory once, in
-// a fixed order), and owns right-hand sides 2 grp, 2 grp + 1 of row i in the
-// two matrix-vector products (D_b read through L2 while the CTA waits, M_b
-// staged in shared memory).  One CTA per SM.
-constexpr int SW_SMEM = TS_B * TS_B * int(sizeof(double)) + 4 * SW_NR * TS_B * int(sizeof(double));
+// X (nrhs x N, row r at X + r N) <- T^-1 X with T the unit lower (LOWER) or
+// upper triangle of LU, in the lookahead form above.  256 threads: thread
+// (i, grp) = (tid % 64, tid / 64) accumulates row i of the block over
+// columns 16 grp .. 16 grp + 15 of every tile before the gate (16 factor
+// values prefetched into registers one tile ahead, NR right-hand sides in
+// registers; the four column groups meet in shared memory once, in a fixed
+// order), and owns right-hand sides NR/4 grp .. NR/4 grp + NR/4 - 1 of row i
+// in the two matrix-vector products.  Dynamic shared memory: D_b, M_b
+// (64 KB) and the column groups' partial sums (NR * 2 KB).
+// flags[blk] == epoch marks a published block.
+template <int NR>
+constexpr int sweep_dyn_bytes() {
+  return 2 * TS_B * TS_B * int(sizeof(double)) + 4 * NR * TS_B * int(sizeof(double));
+}
 
-template <bool LOWER>
-__global__ void __launch_bounds__(SW_THREADS, 1) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
-                                                             const double* __restrict__ Dinv,
-                                                             const double* __restrict__ Mla, double* __restrict__ X,
-                                                             int nrhs, int* __restrict__ flags, int epoch,
-                                                             int* __restrict__ err) {
+template <bool LOWER, int NR>
+__global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
+                                                   const double* __restrict__ Dinv, const double* __restrict__ Mla,
+                                                   double* __restrict__ X, int nrhs, int* __restrict__ flags,
+                                                   int epoch, int* __restrict__ err) {
   extern __shared__ __align__(16) double sw_dyn[];
-  double* Ms = sw_dyn;                // M_b, column-major
-  double* part = Ms + TS_B * TS_B;    // part[(grp * SW_NR + r) * 128 + i]
-  __shared__ __align__(16) double xs[SW_NR][TS_B];  // a published block's solution
-  __shared__ double rs[SW_NR][TS_B];                // this block's right-hand side
+  double* Ds = sw_dyn;                    // D_b, column-major
+  double* Ms = sw_dyn + TS_B * TS_B;      // M_b, column-major
+  double* part = Ms + TS_B * TS_B;        // part[(grp * NR + r) * 64 + i]
+  __shared__ __align__(16) double xs[NR][TS_B];  // a published block's solution
+  __shared__ double rs[NR][TS_B];                // this block's right-hand side
   __shared__ int s_fail;
-  constexpr int RPT = SW_NR / 4;  // right-hand sides per thread in the products
+  constexpr int RPT = NR / 4;  // right-hand sides per thread in the products
   const int nblk = int((N + TS_B - 1) / TS_B);
   const int q = blockIdx.x;
   const int b = LOWER ? q : nblk - 1 - q;
   const int64_t b0 = (int64_t)b * TS_B;
   const int i = threadIdx.x % TS_B, grp = threadIdx.x / TS_B;
-  const double* Dg = Dinv + (int64_t)b * TS_B * TS_B;
+  // everything that does not depend on other blocks first
   {
+    const double* Dg = Dinv + (int64_t)b * TS_B * TS_B;
     const double* Mg = Mla + (int64_t)b * TS_B * TS_B;
-    for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) Ms[e] = Mg[e];
+    for (int e = threadIdx.x; e < TS_B * TS_B; e += blockDim.x) {
+      Ds[e] = Dg[e];
+      Ms[e] = Mg[e];
+    }
   }
-  for (int e = threadIdx.x; e < SW_NR * TS_B; e += blockDim.x) {
+  for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
     const int r = e / TS_B, c = e % TS_B;
     rs[r][c] = (r < nrhs && b0 + c < N) ? X[(int64_t)r * N + b0 + c] : 0.0;
   }
   if (threadIdx.x == 0) s_fail = 0;
   __syncthreads();
-  double acc[SW_NR];
+  double acc[NR];
 #pragma unroll
-  for (int r = 0; r < SW_NR; r++) acc[r] = 0.0;
+  for (int r = 0; r < NR; r++) acc[r] = 0.0;
   const int64_t row = b0 + i;
   const bool vec4 = (lda % 4) == 0 && (reinterpret_cast<uintptr_t>(LU) % 16) == 0;
-  float lv[32];  // row i, columns 32 grp .. 32 grp + 31 of the next tile
+  float lv[16];  // row i, columns 16 grp .. 16 grp + 15 of the next tile
   auto load_lu = [&](int j) {
-    const int64_t j0 = (int64_t)j * TS_B + 32 * grp;
-    if (vec4 && row < N && j0 + 32 <= N) {
+    const int64_t j0 = (int64_t)j * TS_B + 16 * grp;
+    if (vec4 && row < N && j0 + 16 <= N) {
       const float4* p = reinterpret_cast<const float4*>(LU + row * lda + j0);
 #pragma unroll
-      for (int v = 0; v < 8; v++) {
+      for (int v = 0; v < 4; v++) {
         const float4 f = __ldg(p + v);
         lv[4 * v] = f.x;
         lv[4 * v + 1] = f.y;
@@ -1279,11 +1131,11 @@ __global__ void __launch_bounds__(SW_THREADS, 1) k_trsv_sweep(const float* __res
       }
     } else {
 #pragma unroll
-      for (int c = 0; c < 32; c++) lv[c] = (row < N && j0 + c < N) ? LU[row * lda + j0 + c] : 0.f;
+      for (int c = 0; c < 16; c++) lv[c] = (row < N && j0 + c < N) ? LU[row * lda + j0 + c] : 0.f;
     }
   };
   auto load_x = [&](int64_t j0) {  // published by another CTA: read via L2
-    for (int e = threadIdx.x; e < SW_NR * TS_B; e += blockDim.x) {
+    for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
       const int r = e / TS_B, c = e % TS_B;
       xs[r][c] = (r < nrhs && j0 + c < N) ? __ldcg(X + (int64_t)r * N + j0 + c) : 0.0;
     }
@@ -1297,22 +1149,22 @@ __global__ void __launch_bounds__(SW_THREADS, 1) k_trsv_sweep(const float* __res
     if (s_fail) break;
     load_x((int64_t)j * TS_B);
     __syncthreads();
-    float lc[32];
+    float lc[16];
 #pragma unroll
-    for (int c = 0; c < 32; c++) lc[c] = lv[c];
+    for (int c = 0; c < 16; c++) lc[c] = lv[c];
     if (t + 1 < nacc) load_lu(LOWER ? t + 1 : nblk - 2 - t);
 #pragma unroll
-    for (int c = 0; c < 32; c += 2) {
+    for (int c = 0; c < 16; c += 2) {
 #pragma unroll
-      for (int r = 0; r < SW_NR; r++) {
-        const double2 x = *reinterpret_cast<const double2*>(&xs[r][32 * grp + c]);
+      for (int r = 0; r < NR; r++) {
+        const double2 x = *reinterpret_cast<const double2*>(&xs[r][16 * grp + c]);
         acc[r] = fma(double(lc[c]), x.x, acc[r]);
         acc[r] = fma(double(lc[c + 1]), x.y, acc[r]);
       }
     }
   }
 #pragma unroll
-  for (int r = 0; r < SW_NR; r++) part[(grp * SW_NR + r) * TS_B + i] = acc[r];
+  for (int r = 0; r < NR; r++) part[(grp * NR + r) * TS_B + i] = acc[r];
   __syncthreads();
   // y_b = D_b (r_b - sum): this thread's right-hand sides of row i
 #pragma unroll
@@ -1320,7 +1172,7 @@ __global__ void __launch_bounds__(SW_THREADS, 1) k_trsv_sweep(const float* __res
     const int r = RPT * grp + u;
     double v = rs[r][i];
 #pragma unroll
-    for (int h = 0; h < 4; h++) v -= part[(h * SW_NR + r) * TS_B + i];
+    for (int h = 0; h < 4; h++) v -= part[(h * NR + r) * TS_B + i];
     rs[r][i] = v;
   }
   __syncthreads();
@@ -1331,7 +1183,7 @@ __global__ void __launch_bounds__(SW_THREADS, 1) k_trsv_sweep(const float* __res
     for (int u = 0; u < RPT; u++) y0[u] = y1[u] = 0.0;
 #pragma unroll 4
     for (int m = 0; m < TS_B; m += 2) {
-      const double d0 = __ldg(Dg + m * TS_B + i), d1 = __ldg(Dg + (m + 1) * TS_B + i);
+      const double d0 = Ds[m * TS_B + i], d1 = Ds[(m + 1) * TS_B + i];
 #pragma unroll
       for (int u = 0; u < RPT; u++) {
         y0[u] = fma(d0, rs[RPT * grp + u][m], y0[u]);
@@ -1455,8 +1307,7 @@ extern "C" int64_t tb_gemm_tf32x3_workspace(int64_t M, int64_t N, int64_t K) {
 
 extern "C" int64_t tb_lu_nopiv_f32_tc_workspace(int64_t N) {
   if (N <= 0) return 0;
-  const int64_t g = gemm_pre_bytes(N, N, TC_PANEL);
-  return g > LU_INV_BYTES ? g : LU_INV_BYTES;
+  return gemm_pre_bytes(N, N, TC_PANEL);
 }
 
 extern "C" int tb_lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, void* work, int64_t work_bytes, int* err,
@@ -1529,14 +1380,17 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   if (cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) return CUDA_ERR;
   int st = lu_nopiv_f32_tc(S, N, N, err, gemm_work, s);
   if (st != OK) return st;
-  if (cudaFuncSetAttribute(k_trsv_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_SMEM) != cudaSuccess ||
-      cudaFuncSetAttribute(k_trsv_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW_SMEM) != cudaSuccess ||
-      cudaFuncSetAttribute(k_diag_inverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, DI_SMEM) != cudaSuccess ||
-      cudaFuncSetAttribute(k_diag_inverse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, DI_SMEM) != cudaSuccess)
-    return CUDA_ERR;
-  k_diag_inverse<true><<<unsigned(nblk), TS_B, DI_SMEM, s>>>(S, N, N, dinv_l, mla_l);
-  k_diag_inverse<false><<<unsigned(nblk), TS_B, DI_SMEM, s>>>(S, N, N, dinv_u, mla_u);
+  k_diag_inverse<true><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_l, mla_l);
+  k_diag_inverse<false><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_u, mla_u);
   if (cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s) != cudaSuccess) return CUDA_ERR;
+  constexpr int SW8 = sweep_dyn_bytes<8>(), SW16 = sweep_dyn_bytes<16>();
+  if (cudaFuncSetAttribute(k_trsv_sweep<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW16) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW16) !=
+          cudaSuccess)
+    return CUDA_ERR;
   int epoch = 0;
   if (cudaMemsetAsync(X, 0, sizeof(double) * N * nrhs, s) != cudaSuccess) return CUDA_ERR;
   const int nr = int(nrhs);
@@ -1553,11 +1407,12 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
     } else {
       k_residual<2><<<unsigned((N + 15) / 16), 256, 0, s>>>(A, lda, X, F, D, N, nr);
     }
-    for (int r0 = 0; r0 < nr; r0 += SW_NR) {  // 8 right-hand sides per sweep
-      const int ng = nr - r0 < SW_NR ? nr - r0 : SW_NR;
-      double* Dg = D + (int64_t)r0 * N;
-      k_trsv_sweep<true><<<unsigned(nblk), SW_THREADS, SW_SMEM, s>>>(S, N, N, dinv_l, mla_l, Dg, ng, flags, ++epoch, err);
-      k_trsv_sweep<false><<<unsigned(nblk), SW_THREADS, SW_SMEM, s>>>(S, N, N, dinv_u, mla_u, Dg, ng, flags, ++epoch, err);
+    if (nr <= 8) {
+      k_trsv_sweep<true, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<false, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err);
+    } else {
+      k_trsv_sweep<true, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<false, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err);
     }
     if (cudaMemsetAsync(maxes, 0, sizeof(unsigned long long) * 2 * nr, s) != cudaSuccess) return CUDA_ERR;
     {
