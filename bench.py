@@ -364,6 +364,7 @@ def read_peaks():
 
 
 MLP_FLOP_PER_EVAL = 2 * (16 * 128 + 3 * 128 * 128 + 128 * 16)  # dense BF16 flops of one network evaluation
+FALLBACK_BF16_TFLOPS = 1590.0  # dense bf16 burst of a cuBLAS GEMM on this pool's B200s, used without MEASURED_PEAKS.json
 
 
 def time_steps(fn, steps, flush):
@@ -522,13 +523,16 @@ def run_gpu(args):
         evals = np.mean(attempts) * 6
         achieved = evals * MLP_FLOP_PER_EVAL / launch_s / 1e12
         peak = peaks.get('bf16_tflops')
+        peak_source = 'MEASURED_PEAKS.json bf16_tflops (burst)'
+        if not peak:  # no measurement on this pool: the earlier burst figure of a cuBLAS bf16 GEMM here
+            peak, peak_source = FALLBACK_BF16_TFLOPS, 'fallback: 1,590 TFLOP/s bf16 burst measured earlier on this pool'
         roof = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
                 'frac': achieved / peak if peak else None,
                 'traffic': args.traffic if args.engine == 'tc' else None, 'traffic_unit': 'bytes per launch (ncu)',
                 'kernel': 'k_trace_surrogate_tc' if args.engine == 'tc' else 'k_trace_surrogate',
                 'flop_per_unit': MLP_FLOP_PER_EVAL, 'units_per_launch': evals,
                 'unit_desc': 'network evaluations (dense BF16 flops of the 16-128x4-16 MLP)',
-                'peak_source': 'MEASURED_PEAKS.json bf16_tflops (burst)'}
+                'peak_source': peak_source}
         if plain is not None:
             plain['roofline']['peak'] = fp64_peak
             plain['roofline']['frac'] = plain['roofline']['achieved'] / fp64_peak
