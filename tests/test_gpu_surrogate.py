@@ -233,6 +233,29 @@ def test_trace_session_graph_replays(cuda, trained):
     assert sess.h2d_bytes == n * 48 and sess.d2h_bytes == n * (112 + 4 + 24)
 
 
+def test_trace_session_pipelined_batches(cuda, trained):
+    """run_many: five batches of different beams with two buffer sets in
+    flight give, batch by batch, exactly the endpoints of run() on the same
+    inputs; an empty list returns an empty list."""
+    from traceon_b200 import geometry as G
+    fs, _ = _fields(trained, np.array([0.0, 1500.0, 0.0]))
+    n = 500
+    sess = fs.trace_session(n, G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=1e-10)
+    beams = [G.surrogate_beam(n, seed) for seed in range(50, 55)]
+    want = [tuple(a.copy() for a in sess.run(p0, v0)) for p0, v0 in beams]
+    got = sess.run_many(beams)
+    assert len(got) == len(beams)
+    for g, w in zip(got, want):
+        assert (w[2] == 0).all()
+        for a, b in zip(g, w):
+            assert np.array_equal(a, b)
+    assert sess.run_many([]) == []
+    # and once more, reusing both buffer sets
+    again = sess.run_many(beams[:3])
+    for g, w in zip(again, want[:3]):
+        assert np.array_equal(g[0], w[0])
+
+
 def test_surrogate_tracer_edge_cases(cuda, trained):
     """Empty batch; particles that start outside the (inclusive) bounds end at
     once with no step; an attempt cap of 1 ends every particle with

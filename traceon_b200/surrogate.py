@@ -485,13 +485,18 @@ class TraceSession:
 
     run(position, velocity) returns views of the pinned output buffers
     (plane (n,7), final (n,7), status (n,), counters (n,3)), valid until the
-    next run(); copy them to keep them.  replay_device() replays only the
-    device part (start states already in `start`), for timing."""
+    next run(); copy them to keep them.  run_many(batches) traces a sequence
+    of batches with two buffer sets in flight, so that one batch's copies and
+    host staging overlap the next batch's trace.  replay_device() replays
+    only the device part (start states already in `start`), for timing."""
 
     def __init__(self, field, n, bounds, plane_z, mass=None, charge=None, atol=1e-8, max_attempts=100_000):
         from scipy.constants import e as qe, m_e
         torch = B._torch()
         dev = B.device()
+        self._args = (bounds, plane_z, mass, charge, atol, max_attempts)
+        self._peer = None  # the second buffer set of run_many, made on first use
+        self._streams = None
         mass = m_e if mass is None else mass
         charge = -qe if charge is None else charge
         self.n = int(n)
@@ -564,6 +569,55 @@ class TraceSession:
         self.graph.replay()
         torch.cuda.current_stream().synchronize()
         return self.plane_h.numpy(), self.final_h.numpy(), self.status_h.numpy(), self.counters_h.numpy()
+
+    def run_many(self, batches, before=None):
+        """Traces batches [(position (n,3), velocity (n,3)), ...] with two
+        buffer sets (this session's and a second one, made on the first call)
+        replayed alternately on two streams: while batch i traces, batch i - 1's
+        endpoints come back and batch i + 1's start states are staged in pinned
+        memory.  Returns one (plane, final, status, counters) tuple of host
+        copies per batch, in order.  before: optional callable run on a
+        batch's stream just before its replay (cache control in measurements).
+        Work already queued on the current stream completes first; the current
+        stream waits for all batches on return."""
+        torch = B._torch()
+        if self._peer is None:
+            self._peer = TraceSession(self.field, self.n, *self._args)
+            self._streams = (torch.cuda.Stream(device=self.start.device), torch.cuda.Stream(device=self.start.device))
+        sets = (self, self._peer)
+        cur = torch.cuda.current_stream()
+        for st in self._streams:
+            st.wait_stream(cur)
+        events = [None, None]
+        out = [None] * len(batches)
+
+        def collect(i):
+            k = i % 2
+            events[k].synchronize()
+            t = sets[k]
+            out[i] = (t.plane_h.numpy().copy(), t.final_h.numpy().copy(), t.status_h.numpy().copy(),
+                      t.counters_h.numpy().copy())
+
+        for i, (position, velocity) in enumerate(batches):
+            k = i % 2
+            if i >= 2:
+                collect(i - 2)  # frees set k: its outputs are read and its staging is no longer in use
+            t = sets[k]
+            sh = t.start_h.numpy()
+            sh[:, :3] = position
+            sh[:, 3:] = velocity
+            with torch.cuda.stream(self._streams[k]):
+                if before is not None:
+                    before()
+                t.graph.replay()
+                ev = torch.cuda.Event()
+                ev.record()
+            events[k] = ev
+        for i in range(max(0, len(batches) - 2), len(batches)):
+            collect(i)
+        for st in self._streams:
+            cur.wait_stream(st)
+        return out
 
     def replay_device(self):
         self.graph_device.replay()
