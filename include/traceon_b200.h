@@ -404,6 +404,21 @@ int tb_trace_rk45(const double *start, const double *t0, const double *qm, int64
                   const tb_trace_opts_t *opts, double *rows, int64_t *nrows, int32_t *status, double *final_state,
                   double *plane, int64_t *counters, int32_t *work, tb_stream_t stream);
 
+/* Many geometries in one launch (no reference counterpart: the reference
+ * traces one field at a time).  As tb_trace_rk45 with a BEM field whose
+ * electrostatic sources are the concatenation of n_geoms geometries'
+ * sources: particle i sums only the rings src_offsets[geom[i]] ..
+ * src_offsets[geom[i] + 1] - 1 of field->elec_sources (n_elec = total).
+ *   geom (n) int32 device, ids in [0, n_geoms) (an id outside sums no rings)
+ *   src_offsets (n_geoms + 1) int64 device, non-decreasing, last <= n_elec
+ * Electrostatic sources only (n_mag = n_cur = 0, no axial table); TB_BAD_ARG
+ * otherwise. */
+int tb_trace_rk45_geometries(const double *start, const double *t0, const double *qm, const int32_t *geom,
+                             int64_t n, const tb_field_t *field, const int64_t *src_offsets, int64_t n_geoms,
+                             const tb_trace_opts_t *opts, double *rows, int64_t *nrows, int32_t *status,
+                             double *final_state, double *plane, int64_t *counters, int32_t *work,
+                             tb_stream_t stream);
+
 /* Plane crossings of trajectories stored by tb_trace_rk45 (device arrays):
  * per trajectory the crossing nearest its end, by linear interpolation, as
  * plane_intersection (traceon/backend/tracing.c:184-223) finds it.

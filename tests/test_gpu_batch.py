@@ -49,3 +49,39 @@ def test_solve_direct_batch_vs_oracle(cuda, port):
         q = np.linalg.solve(A, values)
         got = f.electrostatic_point_charges.charges
         assert np.max(np.abs(got - q)) / np.max(np.abs(q)) < 1e-10
+
+
+def test_trace_geometries_equals_single_traces(cuda):
+    """Particles of several geometries traced in one launch (each particle
+    sums only its own geometry's rings) give exactly the endpoints of tracing
+    each geometry on its own with the same team size; uneven particle counts
+    per geometry, some electrons reflected by the negative electrodes."""
+    from traceon_b200.solver import solve_direct_batch
+    from traceon_b200.excitation import Excitation, Mesh
+    from traceon_b200.geometry import random_lens
+    from traceon_b200.tracing import Tracer, trace_geometries, velocity_vec_xz_plane
+    lenses = [random_lens(s, n_range=(100, 400)) for s in (7, 8, 9)]
+    excs = []
+    for geo, volts in lenses:
+        exc = Excitation(Mesh.from_geometry(geo))
+        exc.add_voltage(**{n: float(v) for n, v in zip(geo.names, volts)})
+        excs.append(exc)
+    fields = solve_direct_batch(excs)
+    bounds = np.array([[-0.4e-3, 0.4e-3], [-0.4e-3, 0.4e-3], [-16e-3, 16e-3]])
+    rng = np.random.default_rng(5)
+    pos, vel = [], []
+    for count in (24, 17, 31):
+        r0 = rng.uniform(0, 0.1e-3, count)
+        pos.append(np.stack([r0, np.zeros(count), np.full(count, -15e-3)], 1))
+        vel.append(np.array([velocity_vec_xz_plane(1000.0, a, downward=False) for a in rng.uniform(-5e-3, 5e-3, count)]))
+    batched = trace_geometries(fields, bounds, pos, vel, 15e-3, atol=1e-9, team_warps=2)
+    for f, p, v, got in zip(fields, pos, vel, batched):
+        want = Tracer(f, bounds).trace_endpoints(p, v, 15e-3, atol=1e-9, team_warps=2)
+        for a, b in zip(got, want):
+            assert np.array_equal(np.nan_to_num(a, nan=7.0), np.nan_to_num(b, nan=7.0))
+        assert (want[2] == cuda.TRACE_EXITED).all()
+    # each particle sees its own geometry: the same start states through two
+    # geometries in one launch end differently
+    same = trace_geometries(fields[:2], bounds, [pos[0], pos[0]], [vel[0], vel[0]], 15e-3, atol=1e-9, team_warps=2)
+    assert np.array_equal(same[0][1], batched[0][1])
+    assert not np.array_equal(same[0][1], same[1][1])

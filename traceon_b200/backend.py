@@ -215,6 +215,8 @@ _DEV = {
     'tb_axial_coefficients': (vp, i64, dbl, vp, vp),
     'tb_axial_field_points': (vp, i64, vp, i64, vp, vp, vp, vp),
     'tb_trace_rk45': (vp, vp, vp, i64, C.POINTER(TbField), C.POINTER(TbTraceOpts), vp, vp, vp, vp, vp, vp, vp, vp),
+    'tb_trace_rk45_geometries': (vp, vp, vp, vp, i64, C.POINTER(TbField), vp, i64, C.POINTER(TbTraceOpts), vp, vp, vp,
+                                 vp, vp, vp, vp, vp),
     'tb_num_sms': (),
     'tb_probe_fp64_fma': (C.c_int, i64, vp, vp),
     'tb_probe_math': (vp, i64, C.c_int, vp, vp),

@@ -55,6 +55,11 @@ struct TraceParams {
   double* plane;
   int64_t* counters;
   int32_t* work;
+  // many geometries in one launch (BEM tracer): particle i sums the rings
+  // eoff[geom[i]] .. eoff[geom[i] + 1] - 1 of esrc; geom == nullptr: all of them
+  const int32_t* geom = nullptr;
+  const int64_t* eoff = nullptr;
+  int64_t ngeom = 0;
 };
 
 // Fehlberg 4(5) tableau, tracing.c:9-16
@@ -241,11 +246,12 @@ __device__ __forceinline__ void team_barrier(int team, int nthreads) {
 // BEM field of a team: the elec and mag ring sums split over the team's
 // threads, then a butterfly reduction (identical bits in every lane) and,
 // for teams of several warps, a fixed-order sum of the warp partials.
-template <int TW>
+template <int TW, bool GEOM>
 struct BemTeamField {
   const TraceParams& P;
   int team, lt;
   double (*red)[6];  // [TW][6] per team
+  int64_t e0 = 0, e1 = 0;  // GEOM: the electrostatic rings of the current particle's geometry
 
   __device__ void operator()(const double* p, double* E, double* H) {
     constexpr int T = 32 * TW;
@@ -259,7 +265,7 @@ struct BemTeamField {
     if (inside) {
       const double* er = P.esrc;
 #pragma unroll 2
-      for (int64_t j = lt; j < P.ne; j += T)
+      for (int64_t j = (GEOM ? e0 : 0) + lt; j < (GEOM ? e1 : P.ne); j += T)
         ring_field_acc<false>(r0, z0, er[j], er[P.ne + j], er[2 * P.ne + j], s[0], s[1], dummy);
       const double* mr = P.msrc;
       for (int64_t j = lt; j < P.nm; j += T)
@@ -329,8 +335,8 @@ struct TeamState {
 };
 
 // rk45_particle (above) with its state in shared memory, for the BEM teams.
-template <int TW>
-__device__ void rk45_team(const TraceParams& P, int64_t idx, BemTeamField<TW>& field, volatile TeamState* S,
+template <int TW, bool GEOM>
+__device__ void rk45_team(const TraceParams& P, int64_t idx, BemTeamField<TW, GEOM>& field, volatile TeamState* S,
                           bool writer) {
   for (int c = 0; c < 6; c++) S->y[c] = P.start[idx * 6 + c];
   S->qm = P.qm[idx];
@@ -467,7 +473,7 @@ __device__ void rk45_team(const TraceParams& P, int64_t idx, BemTeamField<TW>& f
   }
 }
 
-template <int TW>
+template <int TW, bool GEOM>
 __global__ void __launch_bounds__(TRACE_THREADS, 2) k_trace_bem(TraceParams P) {
   constexpr int T = 32 * TW;
   constexpr int TEAMS = TRACE_THREADS / T;
@@ -475,7 +481,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, 2) k_trace_bem(TraceParams P) {
   __shared__ double s_red[TEAMS][TW][6];
   __shared__ int64_t s_idx[TEAMS];
   const int team = threadIdx.x / T, lt = threadIdx.x % T;
-  BemTeamField<TW> field{P, team, lt, s_red[team]};
+  BemTeamField<TW, GEOM> field{P, team, lt, s_red[team]};
   for (;;) {
     int64_t idx;
     if (TW == 1) {
@@ -489,6 +495,12 @@ __global__ void __launch_bounds__(TRACE_THREADS, 2) k_trace_bem(TraceParams P) {
       team_barrier(team, T);
     }
     if (idx >= P.n) break;
+    if (GEOM) {  // an id outside [0, ngeom) sums no rings (the host checks ids)
+      const int g = P.geom[idx];
+      const bool ok = g >= 0 && g < P.ngeom;
+      field.e0 = ok ? P.eoff[g] : 0;
+      field.e1 = ok ? P.eoff[g + 1] : 0;
+    }
     rk45_team(P, idx, field, &s_state[team][lt / 32], lt == 0);
     __syncwarp();
   }
@@ -521,10 +533,10 @@ __global__ void __launch_bounds__(128) k_trace_axial(TraceParams P) {
   }
 }
 
-template <int TW>
+template <int TW, bool GEOM>
 static int launch_bem(const TraceParams& P, cudaStream_t s) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_bem<TW>, TRACE_THREADS, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_bem<TW, GEOM>, TRACE_THREADS, 0) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   int64_t teams_needed = P.n;
@@ -532,7 +544,7 @@ static int launch_bem(const TraceParams& P, cudaStream_t s) {
   int64_t by_work = (teams_needed + (TRACE_THREADS / (32 * TW)) - 1) / (TRACE_THREADS / (32 * TW));
   if (blocks > by_work) blocks = by_work;
   if (blocks < 1) blocks = 1;
-  k_trace_bem<TW><<<unsigned(blocks), TRACE_THREADS, 0, s>>>(P);
+  k_trace_bem<TW, GEOM><<<unsigned(blocks), TRACE_THREADS, 0, s>>>(P);
   return launch_status();
 }
 
@@ -1271,10 +1283,10 @@ extern "C" int tb_trace_surrogate(const double* start, const double* t0, const d
   return launch_status();
 }
 
-extern "C" int tb_trace_rk45(const double* start, const double* t0, const double* qm, int64_t n,
-                             const tb_field_t* field, const tb_trace_opts_t* opts, double* rows, int64_t* nrows,
-                             int32_t* status, double* final_state, double* plane, int64_t* counters, int32_t* work,
-                             tb_stream_t stream) {
+static int trace_rk45(const double* start, const double* t0, const double* qm, const int32_t* geom, int64_t n,
+                      const tb_field_t* field, const int64_t* src_offsets, int64_t n_geoms, const tb_trace_opts_t* opts,
+                      double* rows, int64_t* nrows, int32_t* status, double* final_state, double* plane,
+                      int64_t* counters, int32_t* work, tb_stream_t stream) {
   if (!field || !opts || n < 0 || !work) return BAD_ARG;
   if (n == 0) return OK;
   if (n > 0x7fffffff || !start || !qm) return BAD_ARG;
@@ -1315,6 +1327,12 @@ extern "C" int tb_trace_rk45(const double* start, const double* t0, const double
   P.plane = plane;
   P.counters = counters;
   P.work = work;
+  if (geom) {  // many geometries: BEM electrostatic sources only
+    if (axial || field->n_mag > 0 || field->n_cur > 0 || !src_offsets || n_geoms <= 0) return BAD_ARG;
+    P.geom = geom;
+    P.eoff = src_offsets;
+    P.ngeom = n_geoms;
+  }
   cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemsetAsync(work, 0, sizeof(int32_t), s) != cudaSuccess) return CUDA_ERR;
   if (axial) {
@@ -1335,12 +1353,31 @@ extern "C" int tb_trace_rk45(const double* start, const double* t0, const double
     while (tw < 8 && n * tw * 2 <= want) tw *= 2;
   }
   switch (tw) {
-    case 1: return launch_bem<1>(P, s);
-    case 2: return launch_bem<2>(P, s);
-    case 4: return launch_bem<4>(P, s);
-    case 8: return launch_bem<8>(P, s);
+    case 1: return P.geom ? launch_bem<1, true>(P, s) : launch_bem<1, false>(P, s);
+    case 2: return P.geom ? launch_bem<2, true>(P, s) : launch_bem<2, false>(P, s);
+    case 4: return P.geom ? launch_bem<4, true>(P, s) : launch_bem<4, false>(P, s);
+    case 8: return P.geom ? launch_bem<8, true>(P, s) : launch_bem<8, false>(P, s);
     default: return BAD_ARG;
   }
+}
+
+extern "C" int tb_trace_rk45(const double* start, const double* t0, const double* qm, int64_t n,
+                             const tb_field_t* field, const tb_trace_opts_t* opts, double* rows, int64_t* nrows,
+                             int32_t* status, double* final_state, double* plane, int64_t* counters, int32_t* work,
+                             tb_stream_t stream) {
+  return trace_rk45(start, t0, qm, nullptr, n, field, nullptr, 0, opts, rows, nrows, status, final_state, plane,
+                    counters, work, stream);
+}
+
+extern "C" int tb_trace_rk45_geometries(const double* start, const double* t0, const double* qm, const int32_t* geom,
+                                        int64_t n, const tb_field_t* field, const int64_t* src_offsets,
+                                        int64_t n_geoms, const tb_trace_opts_t* opts, double* rows, int64_t* nrows,
+                                        int32_t* status, double* final_state, double* plane, int64_t* counters,
+                                        int32_t* work, tb_stream_t stream) {
+  if (n > 0 && !geom) return BAD_ARG;
+  if (n == 0) return OK;
+  return trace_rk45(start, t0, qm, geom, n, field, src_offsets, n_geoms, opts, rows, nrows, status, final_state,
+                    plane, counters, work, stream);
 }
 
 extern "C" int tb_num_sms(void) { return num_sms(); }

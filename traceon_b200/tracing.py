@@ -216,6 +216,57 @@ class Tracer:
                 res.counters.cpu().numpy())
 
 
+def trace_geometries(fields, bounds, positions, velocities, plane_z, mass=m_e, charge=-e, atol=1e-8,
+                     max_attempts=DEFAULT_MAX_ATTEMPTS, team_warps=0):
+    """Endpoint tracing of particles through several geometries in one GPU
+    launch (tb_trace_rk45_geometries): fields[g] is a FieldRadialBEM
+    (electrostatic charges only, no field bounds) and positions[g],
+    velocities[g] (n_g, 3) its particles.  The reference traces one field at
+    a time.  Returns, per geometry, (plane (n_g, 7), final (n_g, 7),
+    status (n_g,), counters (n_g, 2)) like Tracer.trace_endpoints."""
+    from .field import FieldRadialBEM
+    torch = B._torch()
+    if len(fields) != len(positions) or len(fields) != len(velocities) or not fields:
+        raise ValueError('one list entry of positions and velocities per field')
+    srcs, offsets = [], [0]
+    for f in fields:
+        if not isinstance(f, FieldRadialBEM) or f.field_bounds is not None or \
+                len(f.magnetostatic_point_charges) or len(f.current_point_charges):
+            raise NotImplementedError('trace_geometries takes electrostatic FieldRadialBEM fields without bounds')
+        src = f.electrostatic_point_charges.device_sources()
+        srcs.append(src)
+        offsets.append(offsets[-1] + src.shape[1])
+    esrc = torch.cat(srcs, 1).contiguous()
+    counts = [len(np.atleast_2d(p)) for p in positions]
+    geom = np.repeat(np.arange(len(fields), dtype=np.int32), counts)
+    pos = np.concatenate([np.atleast_2d(np.asarray(p, dtype=np.float64)) for p in positions])
+    vel = np.concatenate([np.atleast_2d(np.asarray(v, dtype=np.float64)) for v in velocities])
+    n = len(pos)
+    dev = esrc.device
+    start = B.to_dev(np.concatenate([pos, vel], axis=1), torch.float64)
+    qm = torch.full((n,), float(charge) / float(mass), dtype=torch.float64, device=dev)
+    geom_t = B.to_dev(geom, torch.int32)
+    off_t = B.to_dev(np.array(offsets, dtype=np.int64), torch.int64)
+    f = B.TbField(esrc.data_ptr() if esrc.numel() else None, esrc.shape[1], None, 0, None, 0, None, None, None,
+                  None, 0)
+    o = B.TbTraceOpts()
+    for i, v in enumerate(np.asarray(bounds, dtype=np.float64).reshape(-1)):
+        o.bounds[i] = float(v)
+    o.atol, o.plane_z, o.record_plane = float(atol), float(plane_z), 1
+    o.max_attempts, o.max_rows, o.team_warps = int(max_attempts), 0, int(team_warps)
+    status = torch.empty(n, dtype=torch.int32, device=dev)
+    final = torch.empty((n, 7), dtype=torch.float64, device=dev)
+    plane = torch.empty((n, 7), dtype=torch.float64, device=dev)
+    counters = torch.empty((n, 2), dtype=torch.int64, device=dev)
+    work = torch.empty(1, dtype=torch.int32, device=dev)
+    B._call('tb_trace_rk45_geometries', start.data_ptr(), None, qm.data_ptr(), geom_t.data_ptr(), n, C.byref(f),
+            off_t.data_ptr(), len(fields), C.byref(o), None, None, status.data_ptr(), final.data_ptr(),
+            plane.data_ptr(), counters.data_ptr(), work.data_ptr(), B._stream())
+    out = [a.cpu().numpy() for a in (plane, final, status, counters)]
+    cuts = np.cumsum(counts)[:-1]
+    return [tuple(x) for x in zip(*(np.split(a, cuts) for a in out))]
+
+
 def plane_intersection(positions, p0, normal):
     """traceon/tracing.py:247-272 (linear interpolation, searched from the end)."""
     positions = np.array(positions, dtype=np.float64)
