@@ -55,7 +55,7 @@ def test_trace_geometries_equals_single_traces(cuda):
     """Particles of several geometries traced in one launch (each particle
     sums only its own geometry's rings) give exactly the endpoints of tracing
     each geometry on its own with the same team size; uneven particle counts
-    per geometry, some electrons reflected by the negative electrodes."""
+    per geometry."""
     from traceon_b200.solver import solve_direct_batch
     from traceon_b200.excitation import Excitation, Mesh
     from traceon_b200.geometry import random_lens
