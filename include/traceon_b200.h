@@ -188,6 +188,16 @@ void triangle_areas(const double *triangles, double *out, size_t N);
  * 2. Batched device entry points (device pointers, explicit stream)
  * ====================================================================== */
 
+/* Graded cubic meshes on the device (no reference counterpart: the
+ * reference's Path.mesh spaces nodes uniformly, traceon/geometry.py:39-70).
+ * Segment s of segments (S, 4) = (r0, z0, r1, z1) gets offsets[s + 1] -
+ * offsets[s] elements with Chebyshev-Lobatto nodes (dense toward both ends);
+ * vertices (N, 4, 3) in line4 order [start, end, 1/3, 2/3] of (r, 0, z),
+ * N = offsets[S], offsets[0] = 0, non-decreasing (device arrays).
+ * Coordinates carry the reference Mesh's 16-bit mantissa truncation. */
+int tb_mesh_segments(const double *segments, const int64_t *offsets, int64_t S, double *vertices, int64_t N,
+                     tb_stream_t stream);
+
 /* Replaces radial.c:224-246 for N elements on the device. */
 int tb_jacobian_buffer_radial(const double *vertices, double *jac, double *pos, int64_t N, tb_stream_t stream);
 

@@ -85,3 +85,28 @@ def test_trace_geometries_equals_single_traces(cuda):
     same = trace_geometries(fields[:2], bounds, [pos[0], pos[0]], [vel[0], vel[0]], 15e-3, atol=1e-9, team_warps=2)
     assert np.array_equal(same[0][1], batched[0][1])
     assert not np.array_equal(same[0][1], same[1][1])
+
+
+def test_graded_mesh_on_device(cuda):
+    """Graded cubic meshes generated on the GPU (tb_mesh_segments) against the
+    host mesher (geometry.polyline_elements): the einzel lens and three
+    batching lenses from their segments and element counts, and segments
+    with zero elements.  The GPU's cosine may differ from the host's in the
+    last bit, which the 16-bit mantissa truncation almost always removes: at
+    most one truncation step (2^-36 relative) anywhere."""
+    from traceon_b200 import geometry as G
+    geos = [G.einzel_lens(1000)] + [G.random_lens(s)[0] for s in range(3)]
+    for geo in geos:
+        v = geo.vertices_device().cpu().numpy()
+        assert v.shape == geo.vertices.shape
+        d = np.abs(v - geo.vertices)
+        assert d.max() <= 2.0 ** -35 * np.abs(geo.vertices).max()
+        assert (d > 0).mean() < 0.01
+        assert np.array_equal(v[:, :, 1], np.zeros_like(v[:, :, 1]))
+    seg = np.array([[1e-3, -2e-3, 1e-3, 2e-3], [1e-3, 2e-3, 2e-3, 2e-3], [2e-3, 2e-3, 2e-3, 3e-3]])
+    v = G.mesh_segments_device(seg, [5, 0, 3]).cpu().numpy()
+    host = np.concatenate([G.polyline_elements([seg[0, :2], seg[0, 2:]], [5]),
+                           G.polyline_elements([seg[2, :2], seg[2, 2:]], [3])])
+    assert np.max(np.abs(v - host)) <= 2.0 ** -35 * 3e-3
+    with pytest.raises(ValueError):
+        G.mesh_segments_device(seg, [5, 0])

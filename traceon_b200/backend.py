@@ -200,6 +200,7 @@ for _name, (_res, *_args) in backend_functions.items():
 
 _DEV = {
     'tb_jacobian_buffer_radial': (vp, vp, vp, i64, vp),
+    'tb_mesh_segments': (vp, vp, i64, vp, i64, vp),
     'tb_element_targets': (vp, vp, vp, i64, vp),
     'tb_fill_matrix_radial': (vp, i64, vp, vp, vp, vp, vp, i64, i64, i64, C.c_int, C.c_int, vp),
     'tb_self_integrals': (vp, vp, vp, vp, vp, i64, i64, vp),

@@ -16,6 +16,53 @@
 
 namespace tb {
 
+// ---------------------------------------------------------------- graded meshes
+// Cubic line elements along straight segments, graded toward both ends of
+// every segment: segment s from (r0, z0) to (r1, z1) carries off[s + 1] -
+// off[s] elements whose nodes are the Chebyshev-Lobatto points
+// t_k = (1 - cos(pi k / n)) / 2 (t_0 = 0, t_n = 1) -- the host mesher's rule
+// (geometry.graded_nodes), with its operations in the same order and without
+// fused multiply-adds.  Rows in the reference's line4 layout [start, end,
+// 1/3-point, 2/3-point] of (r, 0, z) (traceon/mesher.py:188-227), every
+// coordinate with its low 16 mantissa bits cleared: the truncation the
+// reference's Mesh merges points with (traceon/mesher.py:262-290).  One
+// thread per element; its segment by binary search of the offsets.
+__device__ __forceinline__ double snap16(double x) {
+  return __longlong_as_double(__double_as_longlong(x) & (long long)0xFFFFFFFFFFFF0000ULL);
+}
+
+__device__ __forceinline__ double cheb_node(int64_t k, int64_t n) {
+  if (k <= 0) return 0.0;
+  if (k >= n) return 1.0;
+  return __dmul_rn(0.5, __dsub_rn(1.0, cos(__ddiv_rn(__dmul_rn(PI, double(k)), double(n)))));
+}
+
+__global__ void k_mesh_segments(const double* __restrict__ seg, const int64_t* __restrict__ off, int64_t S,
+                                double* __restrict__ out, int64_t N) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int64_t lo = 0, hi = S - 1;  // the last segment with off[s] <= i
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) / 2;
+    if (off[mid] <= i)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const int64_t n = off[lo + 1] - off[lo], k = i - off[lo];
+  const double a = cheb_node(k, n), b = cheb_node(k + 1, n);
+  const double d = __dsub_rn(b, a);
+  const double t[4] = {a, b, __dadd_rn(a, __ddiv_rn(d, 3.0)), __dadd_rn(a, __ddiv_rn(__dmul_rn(2.0, d), 3.0))};
+  const double r0 = seg[4 * lo], z0 = seg[4 * lo + 1], dr = __dsub_rn(seg[4 * lo + 2], r0),
+               dz = __dsub_rn(seg[4 * lo + 3], z0);
+  double* row = out + i * 12;
+  for (int q = 0; q < 4; q++) {
+    row[3 * q] = snap16(__dadd_rn(r0, __dmul_rn(dr, t[q])));
+    row[3 * q + 1] = 0.0;
+    row[3 * q + 2] = snap16(__dadd_rn(z0, __dmul_rn(dz, t[q])));
+  }
+}
+
 // ---------------------------------------------------------------- jacobian
 __global__ void k_jacobian_buffer(const double* __restrict__ vertices, double* __restrict__ jac,
                                   double* __restrict__ pos, int64_t N) {
@@ -593,6 +640,14 @@ __global__ void k_axial_points(const double* __restrict__ points, int64_t M, con
 
 // ====================================================================== C ABI
 using namespace tb;
+
+extern "C" int tb_mesh_segments(const double* segments, const int64_t* offsets, int64_t S, double* vertices,
+                                int64_t N, tb_stream_t stream) {
+  if (S < 1 || N < 0 || !segments || !offsets || (N > 0 && !vertices)) return BAD_ARG;
+  if (N == 0) return OK;
+  k_mesh_segments<<<unsigned((N + 255) / 256), 256, 0, (cudaStream_t)stream>>>(segments, offsets, S, vertices, N);
+  return launch_status();
+}
 
 extern "C" int tb_jacobian_buffer_radial(const double* vertices, double* jac, double* pos, int64_t N,
                                          tb_stream_t stream) {

@@ -60,13 +60,35 @@ def split_counts(total: int, lengths) -> list[int]:
     return [int(x) for x in c]
 
 
+def tube_counts(r_in: float, r_out: float, z0: float, z1: float, n: int) -> list[int]:
+    """Elements on the three segments of aperture_tube (cap, tube, cap)."""
+    return split_counts(n, [r_out - r_in, z1 - z0, r_out - r_in])
+
+
 def aperture_tube(r_in: float, r_out: float, z0: float, z1: float, n: int) -> np.ndarray:
     """One einzel-lens electrode: a tube of radius r_in over [z0, z1] with
     annular end caps out to r_out, i.e. the polyline
     (r_out, z0) -> (r_in, z0) -> (r_in, z1) -> (r_out, z1)."""
     corners = [(r_out, z0), (r_in, z0), (r_in, z1), (r_out, z1)]
-    lengths = [r_out - r_in, z1 - z0, r_out - r_in]
-    return polyline_elements(corners, split_counts(n, lengths))
+    return polyline_elements(corners, tube_counts(r_in, r_out, z0, z1, n))
+
+
+def mesh_segments_device(segments, counts):
+    """Graded cubic elements of straight segments (S, 4) = (r0, z0, r1, z1)
+    with counts[s] elements each, meshed on the GPU (tb_mesh_segments); the
+    rule of polyline_elements.  Returns a (N, 4, 3) device tensor."""
+    from . import backend as B
+    torch = B._torch()
+    seg = np.ascontiguousarray(segments, dtype=np.float64).reshape(-1, 4)
+    counts = np.asarray(counts, dtype=np.int64).reshape(-1)
+    if len(counts) != len(seg) or (counts < 0).any() or not len(seg):
+        raise ValueError('one non-negative element count per segment')
+    off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    n = int(off[-1])
+    out = torch.empty((n, 4, 3), dtype=torch.float64, device=B.device())
+    seg_t, off_t = B.to_dev(seg, torch.float64), B.to_dev(off, torch.int64)
+    B._call('tb_mesh_segments', seg_t.data_ptr(), off_t.data_ptr(), len(seg), out.data_ptr(), n, B._stream())
+    return out
 
 
 class LensGeometry:
@@ -74,11 +96,20 @@ class LensGeometry:
     and the electrode names, in the element order used for the BEM matrix;
     `segments` (S, 4) lists the straight electrode segments (r0, z0, r1, z1)."""
 
-    def __init__(self, vertices, electrode_index, names, segments=None):
+    def __init__(self, vertices, electrode_index, names, segments=None, segment_counts=None):
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float64)
         self.electrode_index = np.asarray(electrode_index, dtype=np.int64)
         self.names = list(names)
         self.segments = np.zeros((0, 4)) if segments is None else np.asarray(segments, dtype=np.float64)
+        # elements per segment, when the mesh is exactly the graded mesh of `segments`
+        self.segment_counts = None if segment_counts is None else np.asarray(segment_counts, dtype=np.int64)
+
+    def vertices_device(self):
+        """The same vertices meshed on the GPU from `segments` and
+        `segment_counts` (tb_mesh_segments): a (N, 4, 3) device tensor."""
+        if self.segment_counts is None:
+            raise ValueError('this geometry does not record its segment counts')
+        return mesh_segments_device(self.segments, self.segment_counts)
 
     def __len__(self):
         return len(self.vertices)
@@ -103,15 +134,16 @@ def einzel_lens(n_elements: int = 1000, r_tube: float = 1.0 * MM, r_cap: float =
     split evenly across the electrodes and graded toward the tube edges."""
     k = len(spans)
     per = [n_elements // k + (1 if i < n_elements % k else 0) for i in range(k)]
-    verts, idx, segs = [], [], []
+    verts, idx, segs, counts = [], [], [], []
     for e, ((z0, z1), n) in enumerate(zip(spans, per)):
         v = aperture_tube(r_tube, r_cap, z0, z1, n)
         verts.append(v)
         idx.append(np.full(len(v), e))
         corners = [(r_cap, z0), (r_tube, z0), (r_tube, z1), (r_cap, z1)]
         segs += [(a[0], a[1], b[0], b[1]) for a, b in zip(corners[:-1], corners[1:])]
+        counts += tube_counts(r_tube, r_cap, z0, z1, n)
     names = ['ground_in', 'lens', 'ground_out'][:k] if k == 3 else [f'electrode{i}' for i in range(k)]
-    return LensGeometry(np.concatenate(verts), np.concatenate(idx), names, segs)
+    return LensGeometry(np.concatenate(verts), np.concatenate(idx), names, segs, counts)
 
 
 def einzel_lens_voltages(seed: int) -> np.ndarray:
@@ -169,12 +201,13 @@ def random_lens(seed: int, n_range=(500, 6000), tubes_range=(2, 5), r_range=(0.5
     # elements per electrode in proportion to its outline length
     outline = lengths + 2 * cap
     per = split_counts(n, outline) if k > 1 else [n]
-    verts, idx, segs = [], [], []
+    verts, idx, segs, counts = [], [], [], []
     for e, ((z0, z1), r, m) in enumerate(zip(spans, radii, per)):
         v = aperture_tube(r, r + cap, z0, z1, max(int(m), 6))
         verts.append(v)
         idx.append(np.full(len(v), e))
         corners = [(r + cap, z0), (r, z0), (r, z1), (r + cap, z1)]
         segs += [(a[0], a[1], b[0], b[1]) for a, b in zip(corners[:-1], corners[1:])]
-    geo = LensGeometry(np.concatenate(verts), np.concatenate(idx), [f'electrode{i}' for i in range(k)], segs)
+        counts += tube_counts(r, r + cap, z0, z1, max(int(m), 6))
+    geo = LensGeometry(np.concatenate(verts), np.concatenate(idx), [f'electrode{i}' for i in range(k)], segs, counts)
     return geo, rng.uniform(*volt_range, k)
