@@ -488,7 +488,9 @@ class TraceSession:
     next run(); copy them to keep them.  run_many(batches) traces a sequence
     of batches with two buffer sets in flight, so that one batch's copies and
     host staging overlap the next batch's trace.  replay_device() replays
-    only the device part (start states already in `start`), for timing."""
+    only the device part (start states already in `start`), for timing.
+    A session's buffers are shared by its calls: use it from one host thread
+    at a time."""
 
     def __init__(self, field, n, bounds, plane_z, mass=None, charge=None, atol=1e-8, max_attempts=100_000):
         from scipy.constants import e as qe, m_e
