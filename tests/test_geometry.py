@@ -1,0 +1,32 @@
+"""Host-side geometry bookkeeping the device mesher relies on: a lens's
+recorded segments and element counts regenerate exactly its vertices with the
+host mesher, and the element counts split as documented.  CPU only."""
+import numpy as np
+
+from traceon_b200 import geometry as G
+
+
+def _remesh(geo):
+    return np.concatenate([G.polyline_elements([s[:2], s[2:]], [c])
+                           for s, c in zip(geo.segments, geo.segment_counts)])
+
+
+def test_segments_and_counts_regenerate_the_mesh():
+    geos = [G.einzel_lens(1000), G.einzel_lens(96)] + [G.random_lens(s)[0] for s in range(4)]
+    for geo in geos:
+        assert geo.segment_counts.sum() == len(geo)
+        assert len(geo.segment_counts) == len(geo.segments)
+        assert np.array_equal(_remesh(geo), geo.vertices)
+
+
+def test_split_counts():
+    c = G.split_counts(100, [1.0, 8.0, 1.0])
+    assert sum(c) == 100 and min(c) >= 2 and c[1] > c[0] == c[2]
+    assert G.split_counts(6, [1.0, 100.0, 1.0]) == [2, 2, 2]
+
+
+def test_graded_nodes_dense_at_both_ends():
+    s = G.graded_nodes(10)
+    assert s[0] == 0.0 and s[-1] == 1.0
+    d = np.diff(s)
+    assert d[0] < d[5] and d[-1] < d[5] and np.allclose(d, d[::-1])

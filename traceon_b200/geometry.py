@@ -47,16 +47,17 @@ def snap(a: np.ndarray) -> np.ndarray:
 
 
 def split_counts(total: int, lengths) -> list[int]:
-    """Split ``total`` elements over segments proportionally to length (each
-    segment gets at least 2)."""
+    """Split ``total`` elements over segments proportionally to length; each
+    segment gets at least 2 (at least 1 when total < 2 per segment)."""
     lengths = np.asarray(lengths, dtype=np.float64)
     raw = total * lengths / lengths.sum()
-    c = np.maximum(2, np.floor(raw).astype(int))
+    floor = 2 if total >= 2 * len(lengths) else 1
+    c = np.maximum(floor, np.floor(raw).astype(int))
     while c.sum() < total:
         c[np.argmax(raw - c)] += 1
     while c.sum() > total:
-        i = np.argmax(c - raw)
-        c[i] -= 1
+        over = np.where(c > floor, c - raw, -np.inf)  # trim only above the minimum
+        c[np.argmax(over)] -= 1
     return [int(x) for x in c]
 
 
