@@ -30,3 +30,26 @@ def test_graded_nodes_dense_at_both_ends():
     assert s[0] == 0.0 and s[-1] == 1.0
     d = np.diff(s)
     assert d[0] < d[5] and d[-1] < d[5] and np.allclose(d, d[::-1])
+
+
+def test_device_entry_points_reject_bad_arguments_on_the_host():
+    """Argument checks that run before any device work (no GPU needed)."""
+    import pytest
+    from conftest import golden
+    from traceon_b200.field import EffectivePointCharges, FieldRadialBEM
+    from traceon_b200.tracing import trace_geometries
+    g = golden('lens96.npz')
+    f = FieldRadialBEM(EffectivePointCharges(g['charges'], g['jac'], g['pos']))
+    p, v = np.zeros((2, 3)), np.zeros((2, 3))
+    with pytest.raises(ValueError):
+        trace_geometries([f, f], g['bounds'], [p], [v], 0.0)
+    with pytest.raises(ValueError):
+        trace_geometries([], g['bounds'], [], [], 0.0)
+    bounded = FieldRadialBEM(EffectivePointCharges(g['charges'], g['jac'], g['pos']))
+    bounded.field_bounds = np.array([[-1e-3, 1e-3], [-1e-3, 1e-3], [-1e-2, 1e-2]])
+    with pytest.raises(NotImplementedError):
+        trace_geometries([bounded], g['bounds'], [p], [v], 0.0)
+    with pytest.raises(ValueError):
+        G.mesh_segments_device(np.zeros((2, 4)), [3])
+    with pytest.raises(ValueError):
+        G.mesh_segments_device(np.zeros((2, 4)), [3, -1])
