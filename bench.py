@@ -336,19 +336,33 @@ def precision_fields(geo, charges_t, m, seed, check=64):
 
 
 # ---------------------------------------------------------------- GPU arm
+def load_probe():
+    """libtb_probe.so (tests/probe): the FP64 FMA throughput probe, a
+    measurement helper kept out of the product library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location('tb_probe_loader', os.path.join(HERE, 'tests', 'probe', 'loader.py'))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.load()
+
+
 def measure_fp64_peak(B, torch):
+    """FP64 FMA throughput (TFLOP/s) of this GPU, measured in this run: the
+    denominator of the FP64-bound kernels' rooflines (the driver's measured
+    peaks cover HBM and bf16 only)."""
+    probe = load_probe()
     out = torch.zeros(1, dtype=torch.float64, device='cuda')
     sms = B.num_sms()
     blocks = sms * 8
     iters = 4096
     s = torch.cuda.current_stream().cuda_stream
-    B.backend_lib.tb_probe_fp64_fma(blocks, iters, out.data_ptr(), s)
+    probe.tb_probe_fp64_fma(blocks, iters, out.data_ptr(), s)
     torch.cuda.synchronize()
     best = 0.0
     for _ in range(5):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        B.backend_lib.tb_probe_fp64_fma(blocks, iters, out.data_ptr(), s)
+        probe.tb_probe_fp64_fma(blocks, iters, out.data_ptr(), s)
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)

@@ -521,16 +521,18 @@ int tb_surrogate_field_points(const double *points, int64_t M, const tb_field_t 
 /* Number of SMs of the current device (grid sizing helper). */
 int tb_num_sms(void);
 
-/* Measurement helper, no reference counterpart: `blocks` x 256 threads each
- * run `iters` x 8 dependent-free FP64 FMAs (16 flops per thread-iteration).
- * Used to measure the FP64 pipe peak that the FP64-bound kernels are
- * compared against. */
-int tb_probe_fp64_fma(int blocks, int64_t iters, double *out, tb_stream_t stream);
-
-/* Test helper, no reference counterpart: out[i] = f(x[i]) on the device for
- * the branch-free functions of the ring-pair loops (fn 0: 1/x, 1: 1/sqrt(x),
- * 2: log x) and, for comparison, the CUDA library forms (fn 10, 11, 12). */
-int tb_probe_math(const double *x, int64_t n, int fn, double *out, tb_stream_t stream);
+/* Bound, in SM clock cycles, of the progress waits inside this library's
+ * kernels: the tensor-core engines' waits for their MMA chains and copy
+ * stages, and the triangular sweeps' waits for blocks other CTAs publish.
+ * No reference counterpart (the reference has no GPU code).  A wait that
+ * runs out makes the kernel give up cleanly: the mixed solve returns
+ * TB_TIMEOUT, the surrogate tracer ends the particles in hand with
+ * TB_TRACE_ENGINE_TIMEOUT.  Work already in flight (MMAs, bulk copies) is
+ * always drained under the default bound before a CTA releases its memory.
+ * cycles >= 1 sets the bound for launches made after the call (one value
+ * per process); cycles <= 0 restores the default (2e9, about 1 s).
+ * Returns the previous bound. */
+int64_t tb_set_wait_limit(int64_t cycles);
 
 #ifdef __cplusplus
 }

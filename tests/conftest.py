@@ -33,6 +33,16 @@ def ref():
     return Oracle('ref')
 
 
+def load_probe():
+    """libtb_probe.so (tests/probe): the test and measurement helpers kept
+    out of the product library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location('tb_probe_loader', os.path.join(REPO, 'tests', 'probe', 'loader.py'))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.load()
+
+
 @pytest.fixture(scope='session')
 def cuda():
     import torch

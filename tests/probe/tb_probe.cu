@@ -1,11 +1,15 @@
-// tb_probe.cu -- FP64 pipe throughput probe used as the roofline denominator
-// of the FP64-bound kernels (the field sums of the tracer, fill and field
-// kernels).  Each thread runs 8 independent FMA chains; the result is
-// written so the work cannot be removed.
-#include "tb_common.cuh"
-#include "tb_internal.cuh"
-#include "tb_fastmath.cuh"
-#include "../../include/traceon_b200.h"
+// tb_probe.cu -- measurement and test helpers, built into libtb_probe.so
+// beside the tests (not into the product library):
+//   * an FP64 pipe throughput probe, the roofline denominator of the
+//     FP64-bound kernels (the tracer's field sums, the fill and field
+//     kernels): each thread runs 8 independent FMA chains, and the result is
+//     written so the work cannot be removed;
+//   * the device math of the ring-pair loops (tb_fastmath.cuh) evaluated on
+//     arrays, for comparison with the CUDA library functions.
+#include "../../traceon_b200/csrc/tb_common.cuh"
+#include "../../traceon_b200/csrc/tb_internal.cuh"
+#include "../../traceon_b200/csrc/tb_fastmath.cuh"
+#include "tb_probe.h"
 
 namespace tb {
 
@@ -41,14 +45,14 @@ __global__ void k_probe_math(const double* __restrict__ x, int64_t n, int fn, do
 
 }  // namespace tb
 
-extern "C" int tb_probe_math(const double* x, int64_t n, int fn, double* out, tb_stream_t stream) {
+extern "C" int tb_probe_math(const double* x, int64_t n, int fn, double* out, tb_probe_stream_t stream) {
   if (n < 0 || (n > 0 && (!x || !out))) return tb::BAD_ARG;
   if (n == 0) return tb::OK;
   tb::k_probe_math<<<unsigned((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(x, n, fn, out);
   return tb::launch_status();
 }
 
-extern "C" int tb_probe_fp64_fma(int blocks, int64_t iters, double* out, tb_stream_t stream) {
+extern "C" int tb_probe_fp64_fma(int blocks, int64_t iters, double* out, tb_probe_stream_t stream) {
   if (blocks <= 0 || iters <= 0 || !out) return tb::BAD_ARG;
   tb::k_fp64_fma<<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, 1.0, out);
   return tb::launch_status();

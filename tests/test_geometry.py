@@ -23,6 +23,15 @@ def test_split_counts():
     c = G.split_counts(100, [1.0, 8.0, 1.0])
     assert sum(c) == 100 and min(c) >= 2 and c[1] > c[0] == c[2]
     assert G.split_counts(6, [1.0, 100.0, 1.0]) == [2, 2, 2]
+    # fewer than 2 per segment: at least 1 each, and the total is kept
+    assert G.split_counts(3, [1.0, 1.0, 1.0]) == [1, 1, 1]
+    c = G.split_counts(5, [1.0, 1.0, 1.0])
+    assert sum(c) == 5 and min(c) >= 1
+    # fewer elements than segments cannot be split
+    import pytest
+    for total, lengths in ((1, [1, 1, 1]), (2, [1, 1, 1]), (0, [1, 2]), (3, [])):
+        with pytest.raises(ValueError):
+            G.split_counts(total, lengths)
 
 
 def test_graded_nodes_dense_at_both_ends():

@@ -1,5 +1,5 @@
 """Device math of the ring-pair loops against the CUDA library functions
-(tb_probe_math): the branch-free reciprocal, reciprocal square root and
+(tb_probe_math of the test library tests/probe): the branch-free reciprocal, reciprocal square root and
 logarithm of tb_fastmath.cuh stay within a few ulp over the argument ranges
 the loops produce."""
 import numpy as np
@@ -12,7 +12,8 @@ def _probe(cuda, x, fn):
     import torch
     xt = torch.as_tensor(x, device='cuda', dtype=torch.float64)
     out = torch.empty_like(xt)
-    rc = cuda.backend_lib.tb_probe_math(xt.data_ptr(), xt.numel(), fn, out.data_ptr(),
+    from conftest import load_probe
+    rc = load_probe().tb_probe_math(xt.data_ptr(), xt.numel(), fn, out.data_ptr(),
                                         torch.cuda.current_stream().cuda_stream)
     assert rc == 0
     return out.cpu().numpy()

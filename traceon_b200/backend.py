@@ -219,8 +219,6 @@ _DEV = {
     'tb_trace_rk45_geometries': (vp, vp, vp, vp, i64, C.POINTER(TbField), vp, i64, C.POINTER(TbTraceOpts), vp, vp, vp,
                                  vp, vp, vp, vp, vp),
     'tb_num_sms': (),
-    'tb_probe_fp64_fma': (C.c_int, i64, vp, vp),
-    'tb_probe_math': (vp, i64, C.c_int, vp, vp),
     'tb_lu_nopiv_f64': (vp, i64, i64, vp),
     'tb_lu_nopiv_f32': (vp, i64, i64, vp),
     'tb_lu_nopiv_f32_tc': (vp, i64, i64, vp, i64, vp, vp),
@@ -235,6 +233,15 @@ for _name, _args in _DEV.items():
     _f = getattr(backend_lib, _name)
     _f.restype = C.c_int
     _f.argtypes = list(_args)
+backend_lib.tb_set_wait_limit.restype = i64
+backend_lib.tb_set_wait_limit.argtypes = [i64]
+
+
+def set_wait_limit(cycles):
+    """Bound (SM clock cycles) of the progress waits inside the library's
+    kernels, for launches made after the call; cycles <= 0 restores the
+    default (about 1 s).  Returns the previous bound (tb_set_wait_limit)."""
+    return int(backend_lib.tb_set_wait_limit(int(cycles)))
 
 
 def _check_status():

@@ -2,9 +2,26 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include "tb_common.cuh"
 
 namespace tb {
+
+// Bounded waits inside kernels (an MMA chain's completion, a pipeline
+// stage, a flag another CTA publishes) give up after this many SM clock
+// cycles: ~1 s at 1.9 GHz, far beyond any wait of a healthy launch.
+constexpr long long DEFAULT_WAIT_CYCLES = 2000000000LL;
+// Waits that drain work already in flight before shared or tensor memory
+// is given up (after a failure too) always use the default bound.
+constexpr long long DRAIN_WAIT_CYCLES = DEFAULT_WAIT_CYCLES;
+
+// The limit of the progress waits, read on the host at every launch and
+// passed to the kernel (tb_set_wait_limit sets it; one value per process).
+inline std::atomic<long long>& wait_limit_cycles() {
+  static std::atomic<long long> v{DEFAULT_WAIT_CYCLES};
+  return v;
+}
+inline long long wait_limit() { return wait_limit_cycles().load(std::memory_order_relaxed); }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

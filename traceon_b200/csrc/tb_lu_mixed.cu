@@ -338,7 +338,6 @@ __global__ void __launch_bounds__(TRSM_COLS)
 // the staging of chunk k + 1 overlaps the MMAs of chunk k.  B is staged
 // transposed (N rows x K), so both operands are K-major.
 constexpr int GT_M = 128, GT_N = 256, GT_K = 32, GT_THREADS = 256;
-constexpr long long GT_WAIT_CYCLES = 2000000000LL;  // ~1 s
 
 struct GemmSmem {
   uint8_t a_hi[2][GT_M * 128];
@@ -436,7 +435,8 @@ __device__ __forceinline__ void gt_store(uint32_t ah, uint32_t al, uint32_t bh, 
 template <bool VEC>
 __global__ void __launch_bounds__(GT_THREADS, 1)
     k_gemm_sub_tf32x3(float* __restrict__ C, int64_t ldc, const float* __restrict__ A, int64_t lda,
-                      const float* __restrict__ B, int64_t ldb, int64_t M, int64_t Nc, int K, int* __restrict__ err) {
+                      const float* __restrict__ B, int64_t ldb, int64_t M, int64_t Nc, int K, int* __restrict__ err,
+                      long long wait_cycles) {
   extern __shared__ __align__(1024) unsigned char gt_raw[];
   const uint32_t raw = tc::smem_u32(gt_raw);
   GemmSmem& sm = *reinterpret_cast<GemmSmem*>(gt_raw + (((raw + 1023u) & ~1023u) - raw));
@@ -457,12 +457,13 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
                              (uint32_t(GT_M >> 4) << 24);
   const int nk = (K + GT_K - 1) / GT_K;
   bool ok = true;
+  int committed = 0;  // chunks whose MMAs were committed (uniform over the CTA)
   float ra[16], rb[32];
   gt_load<VEC>(A, lda, B, ldb, M, Nc, K, m0, n0, 0, ra, rb);
   for (int kc = 0; kc < nk; kc++) {
     const int b = kc & 1;
     if (kc >= 2) {  // the MMAs of chunk kc - 2 read buffer b
-      const bool w = tc::mbar_wait_warp(&sm.mbar[b], uint32_t((kc - 2) >> 1) & 1u, GT_WAIT_CYCLES);
+      const bool w = tc::mbar_wait_warp(&sm.mbar[b], uint32_t((kc - 2) >> 1) & 1u, wait_cycles);
       if (__syncthreads_or(!w)) {
         ok = false;
         break;
@@ -487,14 +488,21 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
       }
       tc::mma_commit(&sm.mbar[b]);
     }
+    committed = kc + 1;
   }
   if (ok && nk > 0) {
     const int bl = (nk - 1) & 1;
-    const bool w = tc::mbar_wait_warp(&sm.mbar[bl], uint32_t((nk - 1) >> 1) & 1u, GT_WAIT_CYCLES);
+    const bool w = tc::mbar_wait_warp(&sm.mbar[bl], uint32_t((nk - 1) >> 1) & 1u, wait_cycles);
     ok = !__syncthreads_or(!w);
   }
   if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
+    if (tid == 0) {
+      atomicExch(err, 1);
+      // the committed MMAs must have finished before TMEM is freed
+      if (committed > 0)
+        tc::mbar_wait_bounded(&sm.mbar[(committed - 1) & 1], uint32_t((committed - 1) >> 1) & 1u,
+                              DRAIN_WAIT_CYCLES);
+    }
   } else if (nk > 0) {
     tc::fence_after_sync();
     // warp w: TMEM lanes 32 (w % 4) .. (rows), columns 128 (w / 4) ..
@@ -548,9 +556,11 @@ static int gemm_sub_tf32x3(float* C, int64_t ldc, const float* A, int64_t lda, c
   const bool vec = (lda % 4 == 0) && (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0) &&
                    (reinterpret_cast<uintptr_t>(C) % 16 == 0);
   if (vec)
-    k_gemm_sub_tf32x3<true><<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err);
+    k_gemm_sub_tf32x3<true><<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err,
+                                                                    wait_limit());
   else
-    k_gemm_sub_tf32x3<false><<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err);
+    k_gemm_sub_tf32x3<false><<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err,
+                                                                     wait_limit());
   return launch_status();
 }
 
@@ -638,7 +648,7 @@ constexpr int GQ_SMEM_BYTES = int(sizeof(GemmPersistSmem)) + 1024;
 __global__ void __launch_bounds__(GQ_THREADS, 1)
     k_gemm_sub_persist(float* __restrict__ C, int64_t ldc, const uint8_t* __restrict__ Apre,
                        const uint8_t* __restrict__ Bpre, int64_t M, int64_t Nc, int nk, int64_t nbn, int64_t ntiles,
-                       int* __restrict__ err) {
+                       int* __restrict__ err, long long wait_cycles) {
   extern __shared__ __align__(1024) unsigned char gq_raw[];
   const uint32_t raw = tc::smem_u32(gq_raw);
   GemmPersistSmem& sm = *reinterpret_cast<GemmPersistSmem*>(gq_raw + (((raw + 1023u) & ~1023u) - raw));
@@ -674,7 +684,7 @@ __global__ void __launch_bounds__(GQ_THREADS, 1)
         const uint8_t* Bb = Bpre + (t % nbn) * nk * (int64_t)PB_BLOCK;
         for (int kc = 0; kc < nk; kc++, it++) {
           const int st = it & 1;
-          if (it >= 2 && !tc::mbar_wait_bounded(&sm.empty[st], uint32_t((it - 2) >> 1) & 1u, GT_WAIT_CYCLES)) {
+          if (it >= 2 && !tc::mbar_wait_bounded(&sm.empty[st], uint32_t((it - 2) >> 1) & 1u, wait_cycles)) {
             *fail = 1;
             break;
           }
@@ -694,7 +704,7 @@ __global__ void __launch_bounds__(GQ_THREADS, 1)
       int it = 0, tl = 0;
       for (int64_t t = blockIdx.x; t < ntiles && !*fail; t += gridDim.x, tl++) {
         const int buf = tl & 1;
-        if (tl >= 2 && !tc::mbar_wait_bounded(&sm.acc_empty[buf], uint32_t((tl - 2) >> 1) & 1u, GT_WAIT_CYCLES)) {
+        if (tl >= 2 && !tc::mbar_wait_bounded(&sm.acc_empty[buf], uint32_t((tl - 2) >> 1) & 1u, wait_cycles)) {
           *fail = 1;
           break;
         }
@@ -703,7 +713,7 @@ __global__ void __launch_bounds__(GQ_THREADS, 1)
         bool ok = true;
         for (int kc = 0; kc < nk; kc++, it++) {
           const int st = it & 1;
-          if (!tc::mbar_wait_bounded(&sm.full[st], uint32_t(it >> 1) & 1u, GT_WAIT_CYCLES)) {
+          if (!tc::mbar_wait_bounded(&sm.full[st], uint32_t(it >> 1) & 1u, wait_cycles)) {
             ok = false;
             break;
           }
@@ -745,7 +755,7 @@ __global__ void __launch_bounds__(GQ_THREADS, 1)
           if (c0 + 32 * q < Nc) asm volatile("prefetch.global.L2 [%0];" ::"l"(crow + 32 * q));
       }
       const bool stop = __shfl_sync(0xffffffffu, *fail, 0) != 0;  // warp-uniform
-      if (stop || !tc::mbar_wait_warp(&sm.acc_full[buf], uint32_t(tl >> 1) & 1u, GT_WAIT_CYCLES)) {
+      if (stop || !tc::mbar_wait_warp(&sm.acc_full[buf], uint32_t(tl >> 1) & 1u, wait_cycles)) {
         if (lane == 0) *fail = 1;
         break;
       }
@@ -785,10 +795,10 @@ __global__ void __launch_bounds__(GQ_THREADS, 1)
   // before TMEM is freed and the CTA exits (after a failure too; all of
   // this has already happened on the normal path)
   if (warp == 1 && lane == 0 && issued > 0)
-    tc::mbar_wait_bounded(&sm.empty[(issued - 1) & 1], uint32_t((issued - 1) >> 1) & 1u, GT_WAIT_CYCLES);
+    tc::mbar_wait_bounded(&sm.empty[(issued - 1) & 1], uint32_t((issued - 1) >> 1) & 1u, DRAIN_WAIT_CYCLES);
   if (warp == 0 && lane == 0)
     for (int j = filled - 1; j >= 0 && j >= filled - 2; j--)
-      tc::mbar_wait_bounded(&sm.full[j & 1], uint32_t(j >> 1) & 1u, GT_WAIT_CYCLES);
+      tc::mbar_wait_bounded(&sm.full[j & 1], uint32_t(j >> 1) & 1u, DRAIN_WAIT_CYCLES);
   tc::fence_before_sync();
   __syncthreads();
   if (tid == 0 && sm.fail) atomicExch(err, 1);
@@ -825,7 +835,8 @@ static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, cons
   k_split_b<<<dim3(unsigned(nk), unsigned(nbk)), 256, 0, s>>>(B, ldb, K, Nc, pb);
   const int64_t ntiles = mbk * nbk;
   const int64_t grid = ntiles < num_sms() ? ntiles : num_sms();
-  k_gemm_sub_persist<<<unsigned(grid), GQ_THREADS, GQ_SMEM_BYTES, s>>>(C, ldc, pa, pb, M, Nc, nk, nbk, ntiles, err);
+  k_gemm_sub_persist<<<unsigned(grid), GQ_THREADS, GQ_SMEM_BYTES, s>>>(C, ldc, pa, pb, M, Nc, nk, nbk, ntiles, err,
+                                                                       wait_limit());
   return launch_status();
 }
 
@@ -967,11 +978,13 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
 // matrix-vector product with the freshly published x_g.  D_b and M_b are
 // computed once per factorisation (k_diag_inverse) in FP64 from the FP32
 // factor values.  Published blocks: solution to X, then flags[b] = epoch
-// (release / acquire).  Waits are bounded: after TRSV_WAIT_CYCLES the CTA
-// records an error and writes NaN, which the refinement reports as
-// non-convergence.
+// (release / acquire).  A CTA's place in the chain is the ticket it draws
+// from a counter when it starts (not its block index), so it only ever
+// waits on CTAs that are already running, whatever order the hardware
+// starts them in.  Waits are bounded (the library's wait limit): when one
+// runs out the CTA records an error and writes NaN, and the solve returns
+// TB_TIMEOUT.
 constexpr int TS_B = 64;
-constexpr long long TRSV_WAIT_CYCLES = 2000000000LL;  // ~1 s
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -984,11 +997,12 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 
 // Bounded wait of one thread for flags[j] == epoch; false (and err set) when
 // it ran out.  The sleep between polls doubles up to max_ns.
-__device__ __forceinline__ bool wait_flag(const int* flags, int j, int epoch, int* err, unsigned max_ns) {
+__device__ __forceinline__ bool wait_flag(const int* flags, int j, int epoch, int* err, unsigned max_ns,
+                                          long long max_cycles) {
   const long long t0 = clock64();
   unsigned ns = 32;
   while (ld_acquire(flags + j) != epoch) {
-    if (clock64() - t0 > TRSV_WAIT_CYCLES) {
+    if (clock64() - t0 > max_cycles) {
       atomicExch(err, 1);
       return false;
     }
@@ -1072,7 +1086,9 @@ __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__
 // order), and owns right-hand sides NR/4 grp .. NR/4 grp + NR/4 - 1 of row i
 // in the two matrix-vector products.  Dynamic shared memory: D_b, M_b
 // (64 KB) and the column groups' partial sums (NR * 2 KB).
-// flags[blk] == epoch marks a published block.
+// flags[blk] == epoch marks a published block; flags[nblk] is the ticket
+// counter (every launch of a solve draws nblk tickets, so the launch of
+// epoch e draws (e - 1) nblk .. e nblk - 1).
 template <int NR>
 constexpr int sweep_dyn_bytes() {
   return 2 * TS_B * TS_B * int(sizeof(double)) + 4 * NR * TS_B * int(sizeof(double));
@@ -1082,17 +1098,19 @@ template <bool LOWER, int NR>
 __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
                                                    const double* __restrict__ Dinv, const double* __restrict__ Mla,
                                                    double* __restrict__ X, int nrhs, int* __restrict__ flags,
-                                                   int epoch, int* __restrict__ err) {
+                                                   int epoch, int* __restrict__ err, long long wait_cycles) {
   extern __shared__ __align__(16) double sw_dyn[];
   double* Ds = sw_dyn;                    // D_b, column-major
   double* Ms = sw_dyn + TS_B * TS_B;      // M_b, column-major
   double* part = Ms + TS_B * TS_B;        // part[(grp * NR + r) * 64 + i]
   __shared__ __align__(16) double xs[NR][TS_B];  // a published block's solution
   __shared__ double rs[NR][TS_B];                // this block's right-hand side
-  __shared__ int s_fail;
+  __shared__ int s_fail, s_ticket;
   constexpr int RPT = NR / 4;  // right-hand sides per thread in the products
   const int nblk = int((N + TS_B - 1) / TS_B);
-  const int q = blockIdx.x;
+  if (threadIdx.x == 0) s_ticket = atomicAdd(flags + nblk, 1) - (epoch - 1) * nblk;
+  __syncthreads();
+  const int q = s_ticket;  // this CTA's place in the chain
   const int b = LOWER ? q : nblk - 1 - q;
   const int64_t b0 = (int64_t)b * TS_B;
   const int i = threadIdx.x % TS_B, grp = threadIdx.x / TS_B;
@@ -1144,7 +1162,7 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
   if (nacc > 0) load_lu(LOWER ? 0 : nblk - 1);
   for (int t = 0; t < nacc; t++) {
     const int j = LOWER ? t : nblk - 1 - t;  // finished blocks in publication order
-    if (threadIdx.x == 0 && !wait_flag(flags, j, epoch, err, 256)) s_fail = 1;
+    if (threadIdx.x == 0 && !wait_flag(flags, j, epoch, err, 256, wait_cycles)) s_fail = 1;
     __syncthreads();  // also: every thread is done with the previous tile's xs
     if (s_fail) break;
     load_x((int64_t)j * TS_B);
@@ -1196,7 +1214,7 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
   // the gate: x_b = y_b - M_b x_g
   if (q > 0) {
     const int g = LOWER ? b - 1 : b + 1;
-    if (threadIdx.x == 0 && !s_fail && !wait_flag(flags, g, epoch, err, 64)) s_fail = 1;
+    if (threadIdx.x == 0 && !s_fail && !wait_flag(flags, g, epoch, err, 64, wait_cycles)) s_fail = 1;
     __syncthreads();
     if (!s_fail) {
       load_x((int64_t)g * TS_B);
@@ -1340,7 +1358,7 @@ extern "C" int64_t tb_solve_mixed_workspace(int64_t N, int64_t nrhs) {
   // maxima, inverses of the diagonal blocks of both factors and their
   // lookahead products, sweep flags and the error word
   return round256(N * N * 4) + round256(N * 8) + round256(nrhs * N * 8) + 256 +
-         4 * round256(nblk * TS_B * TS_B * 8) + round256(nblk * 4) + 256 +
+         4 * round256(nblk * TS_B * TS_B * 8) + round256((nblk + 1) * 4) + 256 +
          round256(tb_lu_nopiv_f32_tc_workspace(N));
 }
 
@@ -1369,8 +1387,8 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   w += round256(nblk * TS_B * TS_B * 8);
   double* mla_u = reinterpret_cast<double*>(w);
   w += round256(nblk * TS_B * TS_B * 8);
-  int* flags = reinterpret_cast<int*>(w);
-  w += round256(nblk * 4);
+  int* flags = reinterpret_cast<int*>(w);  // nblk publication flags + the ticket counter
+  w += round256((nblk + 1) * 4);
   int* err = reinterpret_cast<int*>(w);
   w += 256;
   uint8_t* gemm_work = reinterpret_cast<uint8_t*>(w);  // pre-split operands of the trailing updates
@@ -1382,7 +1400,7 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   if (st != OK) return st;
   k_diag_inverse<true><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_l, mla_l);
   k_diag_inverse<false><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_u, mla_u);
-  if (cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s) != cudaSuccess) return CUDA_ERR;
+  if (cudaMemsetAsync(flags, 0, sizeof(int) * (nblk + 1), s) != cudaSuccess) return CUDA_ERR;
   constexpr int SW8 = sweep_dyn_bytes<8>(), SW16 = sweep_dyn_bytes<16>();
   if (cudaFuncSetAttribute(k_trsv_sweep<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
       cudaFuncSetAttribute(k_trsv_sweep<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
@@ -1392,6 +1410,7 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
           cudaSuccess)
     return CUDA_ERR;
   int epoch = 0;
+  const long long wcyc = wait_limit();
   if (cudaMemsetAsync(X, 0, sizeof(double) * N * nrhs, s) != cudaSuccess) return CUDA_ERR;
   const int nr = int(nrhs);
   int it = 0;
@@ -1408,11 +1427,15 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
       k_residual<2><<<unsigned((N + 15) / 16), 256, 0, s>>>(A, lda, X, F, D, N, nr);
     }
     if (nr <= 8) {
-      k_trsv_sweep<true, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err);
-      k_trsv_sweep<false, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<true, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err,
+                                                                  wcyc);
+      k_trsv_sweep<false, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err,
+                                                                  wcyc);
     } else {
-      k_trsv_sweep<true, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err);
-      k_trsv_sweep<false, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err);
+      k_trsv_sweep<true, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err,
+                                                                  wcyc);
+      k_trsv_sweep<false, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err,
+                                                                  wcyc);
     }
     if (cudaMemsetAsync(maxes, 0, sizeof(unsigned long long) * 2 * nr, s) != cudaSuccess) return CUDA_ERR;
     {

@@ -60,6 +60,7 @@ struct TraceParams {
   const int32_t* geom = nullptr;
   const int64_t* eoff = nullptr;
   int64_t ngeom = 0;
+  long long wait_cycles = DEFAULT_WAIT_CYCLES;  // bound of the engine's progress waits
 };
 
 // Fehlberg 4(5) tableau, tracing.c:9-16
@@ -796,19 +797,14 @@ __device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams
     }
     if (engine_failed) {
       // the tensor-core engine gave up waiting for its MMAs (group-uniform):
-      // the particles in hand end with TRACE_ENGINE_TIMEOUT, no new ones
-      if (active) {
+      // the particles in hand end with TRACE_ENGINE_TIMEOUT at their last
+      // accepted state, and so does every particle this group still draws
+      // from the queue (untraced: start state, zero counters), so that each
+      // particle of the launch leaves with a defined status
+      while (active) {
         status = TRACE_ENGINE_TIMEOUT;
-        if (P.status) P.status[idx] = status;
-        if (P.final_state) {
-          P.final_state[idx * 7] = t;
-          for (int c = 0; c < 6; c++) P.final_state[idx * 7 + 1 + c] = y[c];
-        }
-        if (P.counters) {
-          P.counters[idx * 3] = accepted;
-          P.counters[idx * 3 + 1] = attempts;
-          P.counters[idx * 3 + 2] = fallbacks;
-        }
+        finish();
+        if (active) start();
       }
       return;
     }
@@ -927,7 +923,6 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
 constexpr int TC_GROUPS = TB_TC_GROUPS;
 constexpr int TC_THREADS = 128 * TC_GROUPS;
 constexpr uint32_t TC_TMEM_COLS = 512;              // 3 x 128 used
-constexpr long long TC_WAIT_CYCLES = 2000000000LL;  // ~1 s; an MMA chain takes microseconds
 constexpr uint32_t TC_ATOM = 128 * 128;             // bytes of a 128-row SWIZZLE_128B atom
 
 struct TcSmem {
@@ -1032,9 +1027,15 @@ struct TcEngine {
         tc_issue_layer(s, act, dtm, layer);
         tc::mma_commit(&s.mbar[g]);
       }
-      const bool ok = tc::mbar_wait_warp(&s.mbar[g], phase, TC_WAIT_CYCLES);
+      const bool ok = tc::mbar_wait_warp(&s.mbar[g], phase, P.wait_cycles);
+      if (tc::bar_any(1 + g, 128, !ok)) {
+        // the chain committed above must finish before the group gives up
+        // its tile and its tensor memory
+        tc::mbar_wait_warp(&s.mbar[g], phase, DRAIN_WAIT_CYCLES);
+        phase ^= 1u;
+        return false;
+      }
       phase ^= 1u;
-      if (tc::bar_any(1 + g, 128, !ok)) return false;
       tc::fence_after_sync();
       if (layer < 4) {
         const float* bias = layer == 0 ? s.b1 : s.bh[layer - 1];
@@ -1187,6 +1188,7 @@ static int fill_surrogate_params(const tb_field_t* field, const tb_surrogate_t* 
   if (sur->n_segments < 0 || sur->n_segments > SG_MAX_SEGS || (sur->n_segments > 0 && !sur->segments)) return BAD_ARG;
   if (!(sur->r_max > 0) || !(sur->z_half > 0) || sur->env_power < 0 || sur->env_power > 32) return BAD_ARG;
   memset(&P, 0, sizeof(P));
+  P.wait_cycles = wait_limit();
   P.esrc = field->elec_sources;
   P.ne = field->n_elec;
   P.fb = field->field_bounds;
@@ -1381,3 +1383,7 @@ extern "C" int tb_trace_rk45_geometries(const double* start, const double* t0, c
 }
 
 extern "C" int tb_num_sms(void) { return num_sms(); }
+
+extern "C" int64_t tb_set_wait_limit(int64_t cycles) {
+  return wait_limit_cycles().exchange(cycles >= 1 ? (long long)cycles : DEFAULT_WAIT_CYCLES);
+}

@@ -48,8 +48,11 @@ def snap(a: np.ndarray) -> np.ndarray:
 
 def split_counts(total: int, lengths) -> list[int]:
     """Split ``total`` elements over segments proportionally to length; each
-    segment gets at least 2 (at least 1 when total < 2 per segment)."""
+    segment gets at least 2 (at least 1 when total < 2 per segment).
+    Raises ValueError when there are fewer elements than segments."""
     lengths = np.asarray(lengths, dtype=np.float64)
+    if len(lengths) == 0 or total < len(lengths):
+        raise ValueError(f'{total} elements cannot cover {len(lengths)} segments with at least one each')
     raw = total * lengths / lengths.sum()
     floor = 2 if total >= 2 * len(lengths) else 1
     c = np.maximum(floor, np.floor(raw).astype(int))
