@@ -330,7 +330,8 @@ int tb_solve_mixed(const double *A, int64_t lda, int64_t N, const double *F, dou
  * returns TB_BAD_ARG); the array (256 KiB) is held by every GPU that loads
  * the library until the process exits.  The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture.  All calls share the array: calls that overlap
+ * before any stream capture; after a cudaDeviceReset the first call in the
+ * new context looks it up again.  All calls share the array: calls that overlap
  * on the GPU (different streams, or other threads) race and must be
  * serialised by the caller.  Calls no cudaMalloc or cudaFree. */
 int tb_lu_solve_noalloc(double *A, int64_t lda, int64_t N, const double *F, int64_t ldf, double *X, int64_t ldx,

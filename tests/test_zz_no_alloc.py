@@ -49,17 +49,30 @@ def _reference_solution(cuda, A, F):
 
 
 def test_noalloc_solve_matches_allocating_solve(cuda):
+    """Two calls in a row (a larger system, then a smaller one, so that the
+    second runs over pivots the first left in the shared array) against the
+    allocating entry points; the device's free memory (cudaMemGetInfo) is the
+    same before and after the two calls.  A first call on a throw-away system
+    loads the library's kernels beforehand, because loading a module on
+    first use takes device memory itself."""
     import torch
     solve = _lib()
     stream = torch.cuda.current_stream().cuda_stream
+    cases = []
     for n, volts in ((517, (0.0, 1500.0, 0.0)), (300, (-200.0, 900.0, 100.0))):
         A, F = _system(cuda, n, volts)
-        expected = _reference_solution(cuda, A, F)
-        LU = A.clone()
-        X = torch.empty_like(F)
+        cases.append((n, A, F, _reference_solution(cuda, A, F), A.clone(), torch.empty_like(F)))
+    n, A, F, _, _, _ = cases[1]
+    warm_lu, warm_x = A.clone(), torch.empty_like(F)
+    assert solve(warm_lu.data_ptr(), n, n, F.data_ptr(), n, warm_x.data_ptr(), n, F.shape[0], stream) == cuda.TB_OK
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for n, A, F, expected, LU, X in cases:
         rc = solve(LU.data_ptr(), n, n, F.data_ptr(), n, X.data_ptr(), n, F.shape[0], stream)
         assert rc == cuda.TB_OK
-        torch.cuda.synchronize()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    for n, A, F, expected, LU, X in cases:
         got = X.cpu().numpy()
         for k in range(F.shape[0]):
             scale = np.abs(expected[k]).max()

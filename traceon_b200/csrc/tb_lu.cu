@@ -305,14 +305,50 @@ extern "C" int tb_lu_solve_perm(const double* LU, int64_t lda, const int32_t* pe
 // or library allocations: every GPU that loads the library holds it
 // (256 KiB) until the process exits, and it bounds N to NOALLOC_MAX_N.
 // ============================================================================
+#include <cuda.h>
 #include <mutex>
 
 namespace tb {
 constexpr int64_t NOALLOC_MAX_N = 32768;
 static __device__ __align__(256) int32_t g_lu_noalloc_scratch[2 * NOALLOC_MAX_N];
 
+// Per device: the array's device address and the id of the CUDA context it
+// was looked up in.  A device's address belongs to its context: after a
+// cudaDeviceReset the next call runs in a new context and looks it up again.
+struct NoallocSlot {
+  unsigned long long ctx_id;
+  int32_t* addr;
+};
 static std::mutex g_noalloc_mutex;
-static int32_t* g_noalloc_addr[64] = {nullptr};
+static NoallocSlot g_noalloc[64] = {};
+
+// Id of the calling thread's current context, or 0 when there is none or the
+// driver cannot tell (then the address is looked up on every call).  The two
+// driver calls are fetched through the runtime, so the library does not link
+// the driver library itself.
+static unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    looked_up = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 }  // namespace tb
 
 extern "C" int tb_lu_solve_noalloc(double* A, int64_t lda, int64_t N, const double* F, int64_t ldf, double* X,
@@ -325,15 +361,19 @@ extern "C" int tb_lu_solve_noalloc(double* A, int64_t lda, int64_t N, const doub
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return tb::CUDA_ERR;
   int32_t* scratch = nullptr;
   {
-    // Once per device, with that device current: the host-side name of the
-    // array is not a device address, so look the address up.
+    // Once per device (and context), with that device current: the
+    // host-side name of the array is not a device address, so look the
+    // address up.
     std::lock_guard<std::mutex> lock(tb::g_noalloc_mutex);
-    if (!tb::g_noalloc_addr[dev]) {
+    tb::NoallocSlot& slot = tb::g_noalloc[dev];
+    const unsigned long long ctx = tb::current_context_id();
+    if (!slot.addr || ctx == 0 || slot.ctx_id != ctx) {
       void* p = nullptr;
       if (cudaGetSymbolAddress(&p, tb::g_lu_noalloc_scratch) != cudaSuccess || !p) return tb::CUDA_ERR;
-      tb::g_noalloc_addr[dev] = static_cast<int32_t*>(p);
+      slot.addr = static_cast<int32_t*>(p);
+      slot.ctx_id = tb::current_context_id();  // the lookup made the device's context current
     }
-    scratch = tb::g_noalloc_addr[dev];
+    scratch = slot.addr;
   }
   int32_t* ipiv = scratch;
   int32_t* perm = scratch + tb::NOALLOC_MAX_N;  // reset to the identity by every factorisation
