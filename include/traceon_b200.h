@@ -260,6 +260,15 @@ int tb_self_integrals(const double *vertices, const uint8_t *types, const double
  * pre-existing field and are filled by the caller.) */
 int tb_rhs_radial(const uint8_t *types, const double *values, double *F, int64_t N, tb_stream_t stream);
 
+/* The whole right-hand side of solver.py:118-150, magnetizable rows
+ * included: F = V for types 1, 2, 5; 0 for type 3; -factor(mu) H . n for
+ * type 6 (flux_density_to_charge_factor, utilities_2d.c:91-105), with
+ * normal (N, 2) from tb_element_targets and field (N, 3) the pre-existing
+ * field (H_x, H_y, H_z) at each element's collocation point (r, 0, z), e.g.
+ * from tb_current_field_points, or NULL for none. */
+int tb_rhs_radial_field(const uint8_t *types, const double *values, const double *normal, const double *field,
+                        double *F, int64_t N, tb_stream_t stream);
+
 /* Dense LU with partial pivoting in FP64, in place on A (N x N, row stride
  * lda): P A = L U.  ipiv (N) int32 receives the pivot row of each step
  * (LAPACK convention, 0-based); perm (N) int32, if not NULL, the resulting
@@ -493,10 +502,13 @@ typedef struct {
   const float *params_f32;      /* flat FP32 parameters (biases are read from here) */
   double r_max, z_c, z_half;    /* input normalisation; also the domain in r */
   double z_lo, z_hi;            /* domain in z */
-  int n_electrodes;             /* <= 5; outputs 3e..3e+2 are (phi, E_r, E_z) of electrode e at 1 V */
-  double volts[5];              /* electrode voltages */
-  float scale[16];              /* output scales */
-  int env_power;                /* correction = scale * y * rho^p (E_r: rho^(p+1)) */
+  int n_electrodes;             /* field sources: first the electrodes, outputs 3s..3s+2 = (phi, E_r, E_z)
+                                   of electrode s at 1 V ... */
+  int n_coils;                  /* ... then the current coils, (magnetostatic potential, H_r, H_z) of coil
+                                   s at 1 A-turn; 1 <= n_electrodes + n_coils <= 10 */
+  double strengths[10];         /* electrode voltages (V), then coil currents (A-turns) */
+  float scale[32];              /* output scales */
+  int env_power;                /* correction = strength * scale * y * rho^p (radial part: rho^(p+1)) */
   const double *segments;       /* (n_segments, 4) electrode segments r0, z0, r1, z1 (device) */
   int n_segments;               /* <= 64 */
   double fallback_dist;         /* exact BEM within this distance of a segment */
@@ -505,19 +517,25 @@ typedef struct {
 } tb_surrogate_t;
 
 /* RKF45 tracing (tracing.c:60-123 step control) through the surrogate field:
- * axial-series field of `field->axial_*` (the table for the actual voltages)
- * plus the network's correction, exact BEM sums of `field->elec_sources`
- * near electrodes and outside the network's domain.  Endpoint mode only
- * (no trajectories); counters (n, 3): accepted steps, attempts, field
- * evaluations that fell back to BEM. */
+ * axial-series field of `field->axial_elec` (the table for the actual
+ * voltages) plus the network's correction, exact BEM sums of
+ * `field->elec_sources` near electrodes and outside the network's domain.
+ * With a magnetic part (n_coils > 0, `field->axial_mag` -- the table for the
+ * actual currents -- or magnetostatic / current sources) the magnetic field
+ * H is built the same way and the force is q/m (E + mu0 v x H)
+ * (tracing.c:20-57, 141-163).  Endpoint mode only (no trajectories);
+ * counters (n, 3): accepted steps, attempts, field evaluations that fell
+ * back to BEM. */
 int tb_trace_surrogate(const double *start, const double *t0, const double *qm, int64_t n, const tb_field_t *field,
                        const tb_surrogate_t *sur, const tb_trace_opts_t *opts, int32_t *status, double *final_state,
                        double *plane, int64_t *counters, int32_t *work, tb_stream_t stream);
 
 /* The surrogate field E (M,3) at M points (M,3) exactly as the tracer sees
- * it (fallback included); used_bem (M) int32 flags BEM fallbacks, or NULL. */
+ * it (fallback included), and the magnetic field H (M,3) into out_h unless
+ * NULL (zero without a magnetic part); used_bem (M) int32 flags BEM
+ * fallbacks (-1: the engine's wait ran out), or NULL. */
 int tb_surrogate_field_points(const double *points, int64_t M, const tb_field_t *field, const tb_surrogate_t *sur,
-                              double *out, int32_t *used_bem, tb_stream_t stream);
+                              double *out, double *out_h, int32_t *used_bem, tb_stream_t stream);
 
 /* Number of SMs of the current device (grid sizing helper). */
 int tb_num_sms(void);

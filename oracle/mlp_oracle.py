@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import numpy as np
 
-IN, H, OUT = 16, 128, 16
+IN, H, OUT = 16, 128, 32
 LAYERS = [('W1', 'b1', IN, H), ('W2', 'b2', H, H), ('W3', 'b3', H, H), ('W4', 'b4', H, H), ('W5', 'b5', H, OUT)]
 
 
@@ -37,6 +37,16 @@ def silu(z):
     return z / (1 + np.exp(-z))
 
 
+def silu_bf16(z):
+    """The activation as the GPU evaluates it in packed BF16 arithmetic:
+    h = bf16(z / 2), t = bf16(tanh(h)), silu = bf16(h + h t) (one rounding
+    of the fused multiply-add).  Exact tanh here; the GPU's tanh.approx
+    differs from it by at most a BF16 rounding step."""
+    h = bf16(0.5 * np.asarray(z, dtype=np.float64))
+    t = bf16(np.tanh(h))
+    return bf16(h + h * t)
+
+
 def silu_grad(z):
     s = 1 / (1 + np.exp(-z))
     return s * (1 + z * (1 - s))
@@ -55,7 +65,7 @@ def unpack(params):
 
 
 def forward(params, X):
-    """X (M, 16) -> outputs (M, 16); returns (out, pre-activations, activations)."""
+    """X (M, 16) -> outputs (M, 32); returns (out, pre-activations, activations)."""
     P = unpack(params)
     a = bf16(X)
     acts, pre = [a], []
@@ -63,7 +73,7 @@ def forward(params, X):
         z = a @ bf16(P[W]).T + P[b]
         if W != 'W5':
             pre.append(z)
-            a = bf16(silu(z))
+            a = silu_bf16(z)
             acts.append(a)
         else:
             out = z

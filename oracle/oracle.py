@@ -340,30 +340,36 @@ class Oracle:
         return out
 
     # ------------------------------------------------------------ tracing
-    def trace_bem(self, p0, v0, qm, q, jac, pos, bounds, atol, field_bounds=None, max_attempts=0):
-        """One trajectory through a BEM field (elec charges only), returns
-        (times, (n,6) states).  Port: or_trace_particle_bem; ref: the
-        reference trace_particle with its field_radial_traceable callback."""
+    def trace_bem(self, p0, v0, qm, q, jac, pos, bounds, atol, field_bounds=None, max_attempts=0, mag=None,
+                  current=None):
+        """One trajectory through a BEM field, returns (times, (n,6) states):
+        electrostatic charges (q, jac, pos), and optionally magnetostatic
+        charges mag = (q, jac (N,16), pos (N,16,2)) and current rings
+        current = (I, jac (N,12), pos (N,12,3)) -- the Lorentz force of
+        tracing.c:141-163.  Port: or_trace_particle_bem; ref: the reference
+        trace_particle with its field_radial_traceable callback."""
         q, jac, pos = _c(q), _c(jac), _c(pos)
         bounds = _c(bounds).reshape(3, 2)
         times = np.zeros(TRACING_BLOCK_SIZE)
         states = np.zeros((TRACING_BLOCK_SIZE, 6))
         states[0, :3] = p0
         states[0, 3:] = v0
-        empty2 = (np.zeros(0), np.zeros((0, N_QUAD_2D)), np.zeros((0, N_QUAD_2D, 2)))
-        empty3 = (np.zeros(0), np.zeros((0, N_TRIANGLE_QUAD)), np.zeros((0, N_TRIANGLE_QUAD, 3)))
+        mg = (np.zeros(0), np.zeros((0, N_QUAD_2D)), np.zeros((0, N_QUAD_2D, 2))) if mag is None else \
+            tuple(_c(a) for a in mag)
+        cu = (np.zeros(0), np.zeros((0, N_TRIANGLE_QUAD)), np.zeros((0, N_TRIANGLE_QUAD, 3))) if current is None \
+            else tuple(_c(a) for a in current)
         fb = None if field_bounds is None else _c(field_bounds).reshape(3, 2)
         if self.is_port:
             a = _OrBemArgs(_p(q), _p(jac), _p(pos), len(q),
-                           _p(empty2[0]), _p(empty2[1]), _p(empty2[2]), 0,
-                           _p(empty3[0]), _p(empty3[1]), _p(empty3[2]), 0,
+                           _p(mg[0]), _p(mg[1]), _p(mg[2]), len(mg[0]),
+                           _p(cu[0]), _p(cu[1]), _p(cu[2]), len(cu[0]),
                            _p(fb) if fb is not None else None)
             n = self.f_trace_bem(_p(times), _p(states), qm, C.byref(a), _p(bounds), atol, TRACING_BLOCK_SIZE,
                                  max_attempts)
         else:
             e = _Charges2D(_p(q), _p(jac), _p(pos), len(q))
-            m = _Charges2D(_p(empty2[0]), _p(empty2[1]), _p(empty2[2]), 0)
-            c = _Charges2D(_p(empty3[0]), _p(empty3[1]), _p(empty3[2]), 0)
+            m = _Charges2D(_p(mg[0]), _p(mg[1]), _p(mg[2]), len(mg[0]))
+            c = _Charges2D(_p(cu[0]), _p(cu[1]), _p(cu[2]), len(cu[0]))
             a = _FieldArgs(C.cast(C.pointer(e), C.c_void_p), C.cast(C.pointer(m), C.c_void_p),
                            C.cast(C.pointer(c), C.c_void_p), _p(fb) if fb is not None else None)
             n = self.f_trace(_p(times), _p(states), qm, self.addr_field_radial_traceable, _p(bounds), atol,

@@ -65,7 +65,7 @@ def untrained_surrogate():
     from traceon_b200.surrogate import SurrogateTrainer, SurrogateModel, FieldSurrogate
     geo = G.einzel_lens(120)
     tr = SurrogateTrainer(geo, nz=401)
-    model = SurrogateModel(3, tr.r_max, tr.z_lo, tr.z_hi, np.full(16, 1e-3), tr.env_power, seed=0)
+    model = SurrogateModel(3, tr.r_max, tr.z_lo, tr.z_hi, np.full(32, 1e-3), tr.env_power, seed=0)
     return FieldSurrogate(model, tr.fields, tr.z, tr.tabs, np.array([0.0, 1000.0, 0.0]), geo.segments, engine='tc')
 
 

@@ -205,6 +205,7 @@ _DEV = {
     'tb_fill_matrix_radial': (vp, i64, vp, vp, vp, vp, vp, i64, i64, i64, C.c_int, C.c_int, vp),
     'tb_self_integrals': (vp, vp, vp, vp, vp, i64, i64, vp),
     'tb_rhs_radial': (vp, vp, vp, i64, vp),
+    'tb_rhs_radial_field': (vp, vp, vp, vp, vp, i64, vp),
     'tb_lu_factor_perm': (vp, i64, vp, vp, i64, vp),
     'tb_lu_solve_perm': (vp, i64, vp, i64, vp, i64, vp, i64, i64, vp),
     'tb_pack_sources': (vp, vp, vp, vp, i64, vp),

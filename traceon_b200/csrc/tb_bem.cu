@@ -301,6 +301,26 @@ __global__ void k_rhs(const uint8_t* __restrict__ types, const double* __restric
   F[i] = (t == VOLTAGE_FIXED || t == VOLTAGE_FUN || t == MAGNETOSTATIC_POT) ? values[i] : 0.0;
 }
 
+// The full right-hand side of solver.py:118-150: voltage rows take their
+// value, dielectric rows 0, magnetizable rows -factor(mu) H . n with H the
+// pre-existing field at the element's collocation point (field (N, 3) =
+// H_x, H_y, H_z at (r, 0, z), or none: zero field) and n its normal.
+__global__ void k_rhs_field(const uint8_t* __restrict__ types, const double* __restrict__ values,
+                            const double* __restrict__ normal, const double* __restrict__ field,
+                            double* __restrict__ F, int64_t N) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int t = types[i];
+  double f = 0.0;
+  if (t == VOLTAGE_FIXED || t == VOLTAGE_FUN || t == MAGNETOSTATIC_POT) {
+    f = values[i];
+  } else if (t == MAGNETIZABLE && field) {
+    const double hn = field[3 * i] * normal[2 * i] + field[3 * i + 2] * normal[2 * i + 1];
+    f = -flux_factor(values[i]) * hn;
+  }
+  F[i] = f;
+}
+
 // ---------------------------------------------------------------- sources
 __global__ void k_pack_sources(const double* __restrict__ q, const double* __restrict__ jac,
                                const double* __restrict__ pos, double* __restrict__ src, int64_t N) {
@@ -730,6 +750,14 @@ extern "C" int tb_rhs_radial(const uint8_t* types, const double* values, double*
   if (N < 0 || (N > 0 && (!types || !values || !F))) return BAD_ARG;
   if (N == 0) return OK;
   k_rhs<<<unsigned((N + 255) / 256), 256, 0, (cudaStream_t)stream>>>(types, values, F, N);
+  return launch_status();
+}
+
+extern "C" int tb_rhs_radial_field(const uint8_t* types, const double* values, const double* normal,
+                                   const double* field, double* F, int64_t N, tb_stream_t stream) {
+  if (N < 0 || (N > 0 && (!types || !values || !normal || !F))) return BAD_ARG;
+  if (N == 0) return OK;
+  k_rhs_field<<<unsigned((N + 255) / 256), 256, 0, (cudaStream_t)stream>>>(types, values, normal, field, F, N);
   return launch_status();
 }
 

@@ -49,10 +49,11 @@ inline int num_sms() {
 }
 
 // Axial series (radial.c:312-384): locate the interval of z on the equally
-// spaced grid zi and evaluate the 9 derivative polynomials.  Returns false
-// outside [zi[0], zi[Nz-1]].
+// spaced grid zi and evaluate the derivative polynomials first .. 8 (the
+// field needs 1 .. 8, the potential 0, 2, 4, 6, 8).  Returns false outside
+// [zi[0], zi[Nz-1]].
 __host__ __device__ inline bool axial_eval(double z, const double* zi, const double* coeff, int64_t Nz,
-                                           double* d) {
+                                           double* d, int first = 0) {
   double z0 = zi[0], zl = zi[Nz - 1];
   if (!(z0 <= z && z <= zl)) return false;
   double dz = zi[1] - zi[0];
@@ -61,7 +62,7 @@ __host__ __device__ inline bool axial_eval(double z, const double* zi, const dou
   if (idx > Nz - 2) idx = Nz - 2;
   double x = z - zi[idx];
   const double* C = coeff + idx * NDERIV * 6;
-  for (int i = 0; i < NDERIV; i++) {
+  for (int i = first; i < NDERIV; i++) {
     const double* c = C + i * 6;
     d[i] = ((((c[0] * x + c[1]) * x + c[2]) * x + c[3]) * x + c[4]) * x + c[5];
   }

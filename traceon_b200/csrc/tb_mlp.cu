@@ -111,13 +111,23 @@ __global__ void __launch_bounds__(128)
 }
 
 // ------------------------------------------------------------------ elementwise
+// One pair of adjacent elements per thread (the packed SiLU works on pairs);
+// an odd last element is paired with a zero.
 __global__ void k_bias_silu(const float* __restrict__ C, const float* __restrict__ b, float* __restrict__ Z,
                             __nv_bfloat16* __restrict__ Y, int64_t M, int N) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= M * N) return;
-  float z = C[i] + b[i % N];
-  if (Z) Z[i] = z;
-  Y[i] = __float2bfloat16(silu(z));
+  const int64_t n = M * N;
+  const int64_t i = 2 * (blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
+  if (i >= n) return;
+  const float z0 = C[i] + b[i % N];
+  const bool two = i + 1 < n;
+  const float z1 = two ? C[i + 1] + b[(i + 1) % N] : 0.f;
+  if (Z) {
+    Z[i] = z0;
+    if (two) Z[i + 1] = z1;
+  }
+  const uint32_t y = silu2_bf16(z0, z1);
+  Y[i] = __ushort_as_bfloat16((unsigned short)(y & 0xffffu));
+  if (two) Y[i + 1] = __ushort_as_bfloat16((unsigned short)(y >> 16));
 }
 
 __global__ void k_bias_out(const float* __restrict__ C, const float* __restrict__ b, float* __restrict__ Y,
@@ -241,7 +251,8 @@ extern "C" int tb_mlp_bias_silu(const float* C, const float* b, float* Z, void* 
                                 tb_stream_t stream) {
   if (M <= 0 || N <= 0 || !C || !b || !Y) return BAD_ARG;
   int64_t n = M * N;
-  k_bias_silu<<<unsigned((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(C, b, Z, static_cast<__nv_bfloat16*>(Y),
+  k_bias_silu<<<unsigned(((n + 1) / 2 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(C, b, Z,
+                                                                                     static_cast<__nv_bfloat16*>(Y),
                                                                          M, int(N));
   return launch_status();
 }

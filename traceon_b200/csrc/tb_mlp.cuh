@@ -1,6 +1,6 @@
 // tb_mlp.cuh -- the field-surrogate network: sizes, parameter layout, input
 // features, activation, and the warp-level forward pass used inside the
-// tracer.  The network is 16 features -> 4 x 128 (SiLU) -> 16 outputs, BF16
+// tracer.  The network is 16 features -> 4 x 128 (SiLU) -> 32 outputs, BF16
 // weights and activations with FP32 accumulation on the tensor cores
 // (mma.sync m16n8k16).
 #pragma once
@@ -12,8 +12,12 @@ namespace tb {
 
 constexpr int MLP_IN = 16;
 constexpr int MLP_H = 128;
-constexpr int MLP_OUT = 16;
-constexpr int MLP_MAX_ELECTRODES = 5;  // 3 outputs (phi, E_r, E_z) each, <= MLP_OUT
+constexpr int MLP_OUT = 32;
+// Field sources of a surrogate: electrodes (per unit voltage) and current
+// coils (per unit current), 3 outputs each -- (phi, E_r, E_z) of an
+// electrode, (magnetostatic potential, H_r, H_z) of a coil -- in columns
+// 3 s .. 3 s + 2 of source s (electrodes first).
+constexpr int MLP_MAX_SOURCES = MLP_OUT / 3;  // 10
 
 // Flat parameter layout: W1 (H x IN), b1 (H), W2, b2, W3, b3, W4, b4 (H x H, H),
 // W5 (OUT x H), b5 (OUT).  Weights are row-major [out][in].
@@ -34,28 +38,33 @@ struct MlpDomain {
   double r_max, z_c, z_half;
 };
 
-// SiLU through a single hardware tanh: silu(z) = z sigmoid(z) = h + h tanh(h)
-// with h = z / 2.  tanh.approx.f32 (one MUFU operation instead of the exp and
-// reciprocal of z / (1 + exp(-z))) has a maximum relative error of about
-// 2^-11, below the BF16 rounding of the activations that follows; training
-// and both tracer engines use the same function.  (A paired FP16 variant,
-// tanh.approx.f16x2, halves the MUFU operations but its conversions made the
-// tracer slower.)
+// SiLU in packed BF16 arithmetic: silu(z) = z sigmoid(z) = h + h tanh(h)
+// with h = z / 2.  A pair of halved pre-activations (h0, h1) is rounded to
+// BF16 once (cvt.rn.bf16x2.f32), one MUFU operation gives both tanh values
+// (tanh.approx.bf16x2) and one fused multiply-add (fma.rn.bf16x2) gives the
+// pair of BF16 activations the next layer reads -- half the MUFU operations
+// and about half the instructions of the FP32 form.  Training (the forward
+// pass of k_bias_silu) and both tracer engines evaluate the same function,
+// so the network is trained on the activations the tracer computes; the
+// backward pass uses the FP32 derivative of the exact SiLU.
+__device__ __forceinline__ uint32_t silu2_bf16_half(float h0, float h1) {
+  uint32_t p, t, y;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(p) : "f"(h1), "f"(h0));
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(p));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(p), "r"(t));
+  return y;
+}
+// BF16 pair {silu(z0), silu(z1)} (z0 in the low half).
+__device__ __forceinline__ uint32_t silu2_bf16(float z0, float z1) { return silu2_bf16_half(0.5f * z0, 0.5f * z1); }
 __device__ __forceinline__ float tanh_fast(float x) {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-__device__ __forceinline__ float silu(float z) {
-  const float h = 0.5f * z;
-  return fmaf(h, tanh_fast(h), h);
-}
 __device__ __forceinline__ float silu_grad(float z) {
   const float s = fmaf(0.5f, tanh_fast(0.5f * z), 0.5f);  // sigmoid(z)
   return s * fmaf(z, 1.f - s, 1.f);
 }
-// BF16 pair {silu(z0), silu(z1)} (z0 in the low half).
-__device__ __forceinline__ uint32_t silu2_bf16(float z0, float z1);
 
 // Input features of a point (r, z): polynomial terms in rho^2 and zeta (the
 // field is even in r) and five Fourier pairs in zeta, sin/cos(k pi zeta) for
@@ -95,7 +104,6 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<uint32_t*>(&v);
 }
-__device__ __forceinline__ uint32_t silu2_bf16(float z0, float z1) { return pack_bf16(silu(z0), silu(z1)); }
 
 // Shared-memory image of the network for the warp-level forward pass.
 constexpr int MLP_LD_IN = MLP_IN + 8;  // padded row strides (bf16 elements)
@@ -213,26 +221,29 @@ __device__ inline void mlp_warp_forward(const MlpSmem& s, const __nv_bfloat16 (*
 #pragma unroll
         for (int c = 0; c < 4; c++) h[kb][c] = h2[kb][c];
     }
-    // output layer: N = 16 (two n8 tiles), FP32 results
-    float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+    // output layer: N = MLP_OUT (MLP_OUT / 8 n8 tiles), FP32 results
+    constexpr int NT = MLP_OUT / 8;
+    float c[NT][4];
+#pragma unroll
+    for (int t = 0; t < NT; t++) c[t][0] = c[t][1] = c[t][2] = c[t][3] = 0.f;
 #pragma unroll
     for (int ki = 0; ki < 8; ki++) {
-      uint32_t b0[2], b1[2];
-      b0[0] = *reinterpret_cast<const uint32_t*>(&s.w5[g][16 * ki + 2 * q]);
-      b0[1] = *reinterpret_cast<const uint32_t*>(&s.w5[g][16 * ki + 8 + 2 * q]);
-      b1[0] = *reinterpret_cast<const uint32_t*>(&s.w5[8 + g][16 * ki + 2 * q]);
-      b1[1] = *reinterpret_cast<const uint32_t*>(&s.w5[8 + g][16 * ki + 8 + 2 * q]);
-      mma_bf16_16816(c0, h2[ki], b0);
-      mma_bf16_16816(c1, h2[ki], b1);
+#pragma unroll
+      for (int t = 0; t < NT; t++) {
+        uint32_t b[2];
+        b[0] = *reinterpret_cast<const uint32_t*>(&s.w5[8 * t + g][16 * ki + 2 * q]);
+        b[1] = *reinterpret_cast<const uint32_t*>(&s.w5[8 * t + g][16 * ki + 8 + 2 * q]);
+        mma_bf16_16816(c[t], h2[ki], b);
+      }
     }
-    out[r0][2 * q] = c0[0] + s.b5[2 * q];
-    out[r0][2 * q + 1] = c0[1] + s.b5[2 * q + 1];
-    out[r1][2 * q] = c0[2] + s.b5[2 * q];
-    out[r1][2 * q + 1] = c0[3] + s.b5[2 * q + 1];
-    out[r0][8 + 2 * q] = c1[0] + s.b5[8 + 2 * q];
-    out[r0][9 + 2 * q] = c1[1] + s.b5[9 + 2 * q];
-    out[r1][8 + 2 * q] = c1[2] + s.b5[8 + 2 * q];
-    out[r1][9 + 2 * q] = c1[3] + s.b5[9 + 2 * q];
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+      const int col = 8 * t + 2 * q;
+      out[r0][col] = c[t][0] + s.b5[col];
+      out[r0][col + 1] = c[t][1] + s.b5[col + 1];
+      out[r1][col] = c[t][2] + s.b5[col];
+      out[r1][col + 1] = c[t][3] + s.b5[col + 1];
+    }
   }
   __syncwarp();
 }

@@ -117,9 +117,14 @@ __device__ void hermite_crossing(double h, const double* s0, const double* s1, d
 }
 
 // The integrator.  `field(p, E, H)` must return identical bits in every
-// thread that shares a particle; `ks` is per-team scratch for the 6 stages.
-template <class FieldFn>
-__device__ void rk45_particle(const TraceParams& P, int64_t idx, FieldFn& field, double (*ks)[6], bool writer) {
+// thread that shares a particle; `ks` is per-team scratch for the 6 stages,
+// or, with REGS, unused: the stage loop is unrolled and the stage vectors
+// live in registers of the one thread that owns the particle.
+template <class FieldFn, bool REGS = false>
+__device__ void rk45_particle(const TraceParams& P, int64_t idx, FieldFn& field, double (*ks_shared)[6],
+                              bool writer) {
+  double ks_regs[REGS ? 6 : 1][6];
+  double (*ks)[6] = REGS ? ks_regs : ks_shared;
   double y[6];
   for (int c = 0; c < 6; c++) y[c] = P.start[idx * 6 + c];
   const double qm = P.qm[idx];
@@ -144,7 +149,7 @@ __device__ void rk45_particle(const TraceParams& P, int64_t idx, FieldFn& field,
       break;
     }
     attempts++;
-#pragma unroll 1
+#pragma unroll(REGS ? 6 : 1)
     for (int s = 0; s < 6; s++) {
       double ys[6];
 #pragma unroll
@@ -513,24 +518,25 @@ struct AxialField {
   __device__ void operator()(const double* p, double* E, double* H) {
     double d[NDERIV];
     double r2 = p[0] * p[0] + p[1] * p[1];
-    if (axial_eval(p[2], P.az, P.aec, P.anz, d))
+    if (axial_eval(p[2], P.az, P.aec, P.anz, d, 1))
       axial_field(d, p, r2, E);
     else
       E[0] = E[1] = E[2] = 0.0;
-    if (P.amc && axial_eval(p[2], P.az, P.amc, P.anz, d))
+    if (P.amc && axial_eval(p[2], P.az, P.amc, P.anz, d, 1))
       axial_field(d, p, r2, H);
     else
       H[0] = H[1] = H[2] = 0.0;
   }
 };
 
+// One thread per particle: the stage loop fully unrolled, so the six stage
+// vectors stay in registers (the team tracers share theirs in shared memory).
 __global__ void __launch_bounds__(128) k_trace_axial(TraceParams P) {
   AxialField field{P};
-  double ks[6][6];
   for (;;) {
     int64_t idx = atomicAdd(P.work, 1);
     if (idx >= P.n) break;
-    rk45_particle(P, idx, field, ks, true);
+    rk45_particle<AxialField, true>(P, idx, field, nullptr, true);
   }
 }
 
@@ -551,25 +557,31 @@ static int launch_bem(const TraceParams& P, cudaStream_t s) {
 
 // ============================================================================
 // Surrogate-field tracer.  The field at a point is the axial-series field
-// (radial.c:347-384) of a coefficient table for the actual voltages plus a
-// learned correction: a small MLP predicts, per electrode at 1 V, the
-// difference between the BEM field and the axial series, scaled by
-// rho^p (rho = r / r_max) so that the correction vanishes toward the axis
-// where the series is already exact; the per-electrode outputs are
-// contracted with the electrode voltages (the field is linear in them).
-// Points within `fallback_dist` of an electrode segment, or outside the
-// network's domain, fall back to the exact BEM sum.  One particle per lane;
-// the 32 lanes of a warp evaluate the network together on the tensor cores
-// at every RK stage.
+// (radial.c:347-384) of coefficient tables for the actual excitation plus a
+// learned correction: a small MLP predicts, per field source at unit
+// strength (an electrode at 1 V, a current coil at 1 A-turn), the
+// difference between the BEM field and the axial series, scaled by rho^p
+// (rho = r / r_max) so that the correction vanishes toward the axis where the
+// series is already exact; the per-source outputs are contracted with the
+// source strengths (the fields are linear in them, the magnetizable
+// material having a constant permeability).  Points within `fallback_dist`
+// of an electrode segment, or outside the network's domain, fall back to the
+// exact BEM sums.  MAG kernels add the magnetic field H (axial series of the
+// magnetostatic table + the coils' learned corrections; magnetostatic
+// charges and current rings in the fallback) and the Lorentz force
+// q/m (E + mu0 v x H) of tracing.c:20-57.
 // ============================================================================
 struct SurrogateParams {
   const __nv_bfloat16* wb;
   const float* pf;
   MlpDomain dom;
   double z_lo, z_hi;
-  int n_el;
-  double volts[MLP_MAX_ELECTRODES];
-  float scale[MLP_OUT];
+  // the network outputs contracted with the source strengths: before the
+  // envelope, the learned corrections are sum_j w[j] y[j] with
+  // wr[3 s + 1] = V_s scale[3 s + 1] and wz[3 s + 2] = V_s scale[3 s + 2] for
+  // electrode s (E_r, E_z), hr / hz the same with the currents of the coils
+  // (H_r, H_z), zero elsewhere
+  float wr[MLP_OUT], wz[MLP_OUT], hr[MLP_OUT], hz[MLP_OUT];
   int env_p;
   const double* segs;  // (nseg, 4): r0, z0, r1, z1
   int nseg;
@@ -580,44 +592,50 @@ constexpr int SG_THREADS = 512;
 constexpr int SG_WARPS = SG_THREADS / 32;
 constexpr int SG_MAX_SEGS = 64;
 
+// Electrode segment of the fallback test, staged in shared memory in FP32
+// as (r0, z0, dr, dz, 1 / |d|^2), so the distance test takes no division.
+// FP32 places the 50 um fallback boundary to within ~1e-10 m, far below
+// anything that matters for the choice between network and exact field.
+struct Seg {
+  float ar, az, ur, uz, il2;
+};
+
 struct SurrogateSmem {
   MlpSmem mlp;
   __nv_bfloat16 feat[SG_WARPS][32][MLP_LD_IN];
   float out[SG_WARPS][32][MLP_OUT];
-  double segs[SG_MAX_SEGS][5];
+  Seg segs[SG_MAX_SEGS];
 };
 
-// Electrode segments staged in shared memory as (r0, z0, dr, dz, 1 / |d|^2),
-// so the distance test takes no division.
-__device__ inline void load_segments(double (*seg)[5], const double* __restrict__ segs, int nseg) {
+__device__ inline void load_segments(Seg* seg, const double* __restrict__ segs, int nseg) {
   for (int i = threadIdx.x; i < nseg; i += blockDim.x) {
     const double ar = segs[4 * i], az = segs[4 * i + 1];
     const double ur = segs[4 * i + 2] - ar, uz = segs[4 * i + 3] - az;
     const double L2 = ur * ur + uz * uz;
-    seg[i][0] = ar;
-    seg[i][1] = az;
-    seg[i][2] = ur;
-    seg[i][3] = uz;
-    seg[i][4] = L2 > 0 ? 1.0 / L2 : 0.0;
+    seg[i] = Seg{float(ar), float(az), float(ur), float(uz), L2 > 0 ? float(1.0 / L2) : 0.f};
   }
 }
 
-__device__ __forceinline__ bool near_segments(const double (*seg)[5], int nseg, double r, double z, double d2) {
+__device__ __forceinline__ bool near_segments(const Seg* seg, int nseg, double r_d, double z_d, float d2) {
+  const float r = float(r_d), z = float(z_d);
   bool nearby = false;
   for (int i = 0; i < nseg; i++) {
-    const double ar = seg[i][0], az = seg[i][1], ur = seg[i][2], uz = seg[i][3];
-    double tt = ((r - ar) * ur + (z - az) * uz) * seg[i][4];
-    tt = fmin(fmax(tt, 0.0), 1.0);
-    const double dr = r - (ar + tt * ur), dz = z - (az + tt * uz);
-    nearby = nearby || (dr * dr + dz * dz < d2);
+    const Seg g = seg[i];
+    float tt = fmaf(r - g.ar, g.ur, (z - g.az) * g.uz) * g.il2;
+    tt = fminf(fmaxf(tt, 0.f), 1.f);
+    const float dr = r - fmaf(tt, g.ur, g.ar), dz = z - fmaf(tt, g.uz, g.az);
+    nearby = nearby || (fmaf(dr, dr, dz * dz) < d2);
   }
   return nearby;
 }
 
-// Exact BEM field of the electrostatic rings at one point, by one lane.
-// Out of line: it is the rare path of the surrogate tracer, and inlined its
-// ring kernel's registers would count against the whole tracer.
-__device__ __noinline__ void bem_point_field(const TraceParams& P, const double* p, double* E) {
+// Exact BEM field of the electrostatic rings at one point, by one lane, and
+// with MAG the magnetic field H of the magnetostatic charges and current
+// rings (field_radial_traceable, tracing.c:141-163).  Out of line: it is the
+// rare path of the surrogate tracer, and inlined its ring kernels' registers
+// would count against the whole tracer.
+template <bool MAG>
+__device__ __noinline__ void bem_point_field(const TraceParams& P, const double* p, double* E, double* H) {
   double r0 = sqrt(p[0] * p[0] + p[1] * p[1]);
   double Sr = 0, Sz = 0, dummy = 0;
   const double* er = P.esrc;
@@ -630,74 +648,118 @@ __device__ __noinline__ void bem_point_field(const TraceParams& P, const double*
     E[0] = E[1] = 0.0;
   }
   E[2] = -Sz * INV_PI;
+  if (MAG) {
+    double Mr = 0, Mz = 0, Cr = 0, Cz = 0;
+    const double* mr = P.msrc;
+    for (int64_t j = 0; j < P.nm; j++) ring_field_acc<false>(r0, p[2], mr[j], mr[P.nm + j], mr[2 * P.nm + j], Mr, Mz, dummy);
+    const double* cr = P.csrc;
+    for (int64_t j = 0; j < P.nc; j++) {
+      double hr, hz;
+      current_field_ring(r0, p[2], cr[j], cr[P.nc + j], hr, hz);
+      Cr = fma(cr[2 * P.nc + j], hr, Cr);
+      Cz = fma(cr[2 * P.nc + j], hz, Cz);
+    }
+    if (r0 >= MIN_AXIS) {
+      const double h = Mr / (2 * PI * r0) + Cr;
+      H[0] = p[0] / r0 * h;
+      H[1] = p[1] / r0 * h;
+    } else {
+      H[0] = H[1] = 0.0;
+    }
+    H[2] = -Mz * INV_PI + Cz;
+  }
 }
 
-// The field at point p from the network's outputs `y` (16 FP32 values of
-// this point): zero outside the field bounds, exact BEM near electrodes and
-// outside the network's domain, else axial series + learned correction.
-__device__ void surrogate_combine(const TraceParams& P, const SurrogateParams& S, const double (*segs)[5],
-                                  const double* p, double r2, double r, bool live, const float* y, double* E,
-                                  bool& used_bem) {
+// Axial series of one coefficient table plus the learned correction
+// (cr, cz) times the envelope env: the radial part (cr rho^(p+1)) applied
+// as x * (F_r / r).
+__device__ __forceinline__ void axial_plus_correction(const TraceParams& P, const double* table, const double* p,
+                                                      double r2, double env_r, double env, float cr, float cz,
+                                                      double* F) {
+  double d[NDERIV];
+  if (table && axial_eval(p[2], P.az, table, P.anz, d, 1))
+    axial_field(d, p, r2, F);
+  else
+    F[0] = F[1] = F[2] = 0.0;
+  const double fr = double(cr) * env_r, fz = double(cz) * env;
+  F[0] += p[0] * fr;
+  F[1] += p[1] * fr;
+  F[2] += fz;
+}
+
+// The field at point p from the contracted network outputs c (the learned
+// E_r, E_z and, with MAG, H_r, H_z corrections before the envelope): zero
+// outside the field bounds, exact BEM near electrodes and outside the
+// network's domain, else axial series + learned correction.
+template <bool MAG>
+__device__ __forceinline__ void surrogate_combine(const TraceParams& P, const SurrogateParams& S,
+                                                 const Seg* segs, const double* p, double r2, double r,
+                                                 bool live, const float* c, double* E, double* H, bool& used_bem) {
   used_bem = false;
-  if (!live) {
-    E[0] = E[1] = E[2] = 0.0;
-    return;
-  }
   const double* fb = P.fb;
-  if (fb && !(fb[0] < p[0] && p[0] < fb[1] && fb[2] < p[1] && p[1] < fb[3] && fb[4] < p[2] && p[2] < fb[5])) {
+  if (!live ||
+      (fb && !(fb[0] < p[0] && p[0] < fb[1] && fb[2] < p[1] && p[1] < fb[3] && fb[4] < p[2] && p[2] < fb[5]))) {
     E[0] = E[1] = E[2] = 0.0;
+    if (MAG) H[0] = H[1] = H[2] = 0.0;
     return;
   }
   const bool out_of_domain = r > S.dom.r_max || p[2] < S.z_lo || p[2] > S.z_hi;
-  if (out_of_domain || near_segments(segs, S.nseg, r, p[2], S.fb_dist2)) {
+  if (out_of_domain || near_segments(segs, S.nseg, r, p[2], float(S.fb_dist2))) {
     used_bem = true;
-    bem_point_field(P, p, E);
+    bem_point_field<MAG>(P, p, E, H);
     return;
   }
-  double d[NDERIV];
-  if (axial_eval(p[2], P.az, P.aec, P.anz, d))
-    axial_field(d, p, r2, E);
-  else
-    E[0] = E[1] = E[2] = 0.0;
   const double rho = r / S.dom.r_max;
   double env = 1.0;
   for (int i = 0; i < S.env_p; i++) env *= rho;
-  double fr = 0.0, fz = 0.0;
-  for (int e = 0; e < S.n_el; e++) {
-    fr += S.volts[e] * double(S.scale[3 * e + 1]) * double(y[3 * e + 1]);
-    fz += S.volts[e] * double(S.scale[3 * e + 2]) * double(y[3 * e + 2]);
+  const double env_r = env / S.dom.r_max;
+  axial_plus_correction(P, P.aec, p, r2, env_r, env, c[0], c[1], E);
+  if (MAG) axial_plus_correction(P, P.amc, p, r2, env_r, env, c[2], c[3], H);
+}
+
+// The network's outputs y at a point contracted with the source strengths
+// into c (the learned E_r, E_z and, with MAG, H_r, H_z corrections).
+template <bool MAG>
+__device__ __forceinline__ void contract_outputs(const SurrogateParams& S, const float* y, float* c) {
+  c[0] = c[1] = 0.f;
+  if (MAG) c[2] = c[3] = 0.f;
+#pragma unroll
+  for (int j = 0; j < MLP_OUT; j++) {
+    c[0] = fmaf(S.wr[j], y[j], c[0]);
+    c[1] = fmaf(S.wz[j], y[j], c[1]);
+    if (MAG) {
+      c[2] = fmaf(S.hr[j], y[j], c[2]);
+      c[3] = fmaf(S.hz[j], y[j], c[3]);
+    }
   }
-  // E_r correction = fr * rho^(p+1), applied as x * (E_r / r)
-  fr *= env / S.dom.r_max;
-  fz *= env;
-  E[0] += p[0] * fr;
-  E[1] += p[1] * fr;
-  E[2] += fz;
 }
 
 // Field at this lane's point; every lane of the warp must call it.
+template <bool MAG>
 __device__ void surrogate_field(const TraceParams& P, const SurrogateParams& S, SurrogateSmem& sm, int warp, int lane,
-                                const double* p, bool live, double* E, bool& used_bem) {
+                                const double* p, bool live, double* E, double* H, bool& used_bem) {
   const double r2 = p[0] * p[0] + p[1] * p[1], r = sqrt(r2);
   float f[MLP_IN];
   mlp_features(r, p[2], S.dom, f);
 #pragma unroll
   for (int c = 0; c < MLP_IN; c++) sm.feat[warp][lane][c] = __float2bfloat16(f[c]);
   mlp_warp_forward(sm.mlp, sm.feat[warp], sm.out[warp]);
-  surrogate_combine(P, S, sm.segs, p, r2, r, live, sm.out[warp][lane], E, used_bem);
+  float c[4];
+  contract_outputs<MAG>(S, sm.out[warp][lane], c);
+  surrogate_combine<MAG>(P, S, sm.segs, p, r2, r, live, c, E, H, used_bem);
 }
 
 // The RKF45 particle loop of the surrogate tracer, shared by both network
 // engines.  `eng.any(b)` is true if b holds on any thread that evaluates the
-// network together with this one; `eng.field(p, live, E, used_bem)` is the
-// field at p (all those threads call it together) and returns false if the
-// engine failed (uniformly across them).
-template <class Engine>
+// network together with this one; `eng.field(p, live, E, H, used_bem)` is
+// the field at p (all those threads call it together; H only with MAG) and
+// returns false if the engine failed (uniformly across them).
+template <bool MAG, class Engine>
 __device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams& S, Engine& eng) {
   bool engine_failed = false;
   double y[6];
   double t = 0, h = 0, hmax = 0, qm = 0;
-  int64_t accepted = 0, attempts = 0, fallbacks = 0;
+  int accepted = 0, attempts = 0, fallbacks = 0;  // the launch caps max_attempts below 2^31
   int status = TRACE_EXITED;
   int64_t idx = atomicAdd(P.work, 1);
   bool active = idx < P.n;
@@ -770,14 +832,22 @@ __device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams
         ys[1] = 0.0;
         ys[2] = S.dom.z_c;
       }
-      double E[3];
+      double E[3], H[MAG ? 3 : 1];
       bool used_bem;
-      if (!eng.field(ys, go, E, used_bem)) {
+      if (!eng.field(ys, go, E, H, used_bem)) {
         engine_failed = true;
         break;
       }
       if (go) {
         fallbacks += used_bem ? 1 : 0;
+        if (MAG) {  // Lorentz force: E + mu0 v x H (tracing.c:20-57)
+          const double cx = ys[4] * H[2] - ys[5] * H[1];
+          const double cy = ys[5] * H[0] - ys[3] * H[2];
+          const double cz = ys[3] * H[1] - ys[4] * H[0];
+          E[0] += MU0 * cx;
+          E[1] += MU0 * cy;
+          E[2] += MU0 * cz;
+        }
         const double k[6] = {h * ys[3], h * ys[4], h * ys[5], h * qm * E[0], h * qm * E[1], h * qm * E[2]};
         const double ch = RK_CH[s], ct = RK_CT[s];
 #pragma unroll
@@ -854,18 +924,20 @@ __device__ void surrogate_trace_loop(const TraceParams& P, const SurrogateParams
 
 // Network engine of the warp-level kernel: the 32 lanes of a warp evaluate
 // the network together with mma.sync.
+template <bool MAG>
 struct WarpEngine {
   const TraceParams& P;
   const SurrogateParams& S;
   SurrogateSmem& sm;
   int warp, lane;
   __device__ bool any(bool b) const { return __any_sync(0xffffffffu, b); }
-  __device__ bool field(const double* p, bool live, double* E, bool& used_bem) {
-    surrogate_field(P, S, sm, warp, lane, p, live, E, used_bem);
+  __device__ bool field(const double* p, bool live, double* E, double* H, bool& used_bem) {
+    surrogate_field<MAG>(P, S, sm, warp, lane, p, live, E, H, used_bem);
     return true;
   }
 };
 
+template <bool MAG>
 __global__ void __launch_bounds__(SG_THREADS, 1) k_trace_surrogate(TraceParams P, SurrogateParams S) {
   extern __shared__ __align__(16) unsigned char sg_raw[];
   SurrogateSmem& sm = *reinterpret_cast<SurrogateSmem*>(sg_raw);
@@ -874,14 +946,16 @@ __global__ void __launch_bounds__(SG_THREADS, 1) k_trace_surrogate(TraceParams P
   __syncthreads();
   const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
 
-  WarpEngine eng{P, S, sm, warp, lane};
-  surrogate_trace_loop(P, S, eng);
+  WarpEngine<MAG> eng{P, S, sm, warp, lane};
+  surrogate_trace_loop<MAG>(P, S, eng);
 }
 
-// Surrogate field at M points (one point per lane), for tests.
+// Surrogate field E (and with MAG the magnetic field H) at M points (one
+// point per lane), for tests.
+template <bool MAG>
 __global__ void __launch_bounds__(SG_THREADS, 1)
     k_surrogate_points(TraceParams P, SurrogateParams S, const double* __restrict__ pts, int64_t M,
-                       double* __restrict__ field, int32_t* __restrict__ used_bem) {
+                       double* __restrict__ field, double* __restrict__ hfield, int32_t* __restrict__ used_bem) {
   extern __shared__ __align__(16) unsigned char sg_raw[];
   SurrogateSmem& sm = *reinterpret_cast<SurrogateSmem*>(sg_raw);
   mlp_load_smem(sm.mlp, S.wb, S.pf);
@@ -894,11 +968,13 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
     double p[3] = {0.5 * S.dom.r_max, 0.0, S.dom.z_c};
     if (live)
       for (int c = 0; c < 3; c++) p[c] = pts[3 * i + c];
-    double E[3];
+    double E[3], H[3] = {0.0, 0.0, 0.0};
     bool ub;
-    surrogate_field(P, S, sm, warp, lane, p, live, E, ub);
+    surrogate_field<MAG>(P, S, sm, warp, lane, p, live, E, H, ub);
     if (live) {
       for (int c = 0; c < 3; c++) field[3 * i + c] = E[c];
+      if (hfield)
+        for (int c = 0; c < 3; c++) hfield[3 * i + c] = H[c];
       if (used_bem) used_bem[i] = ub ? 1 : 0;
     }
   }
@@ -928,10 +1004,10 @@ constexpr uint32_t TC_ATOM = 128 * 128;             // bytes of a 128-row SWIZZL
 struct TcSmem {
   uint8_t w1[TC_ATOM];                    // W1: 128 rows x K = 16 (chunks 0, 1 of each row)
   uint8_t wh[3][2][TC_ATOM];              // W2..W4: 128 rows x K = 128 (two atoms)
-  uint8_t w5[2][16 * 128];                // W5: 16 rows x K = 128
+  uint8_t w5[2][MLP_OUT * 128];           // W5: MLP_OUT rows x K = 128
   uint8_t act[TC_GROUPS][2][TC_ATOM];     // per group: activations, 128 rows x K <= 128
   float b1[MLP_H], bh[3][MLP_H], b5[MLP_OUT];
-  double segs[SG_MAX_SEGS][5];
+  Seg segs[SG_MAX_SEGS];
   uint64_t mbar[TC_GROUPS];
   uint32_t tmem_base;
 };
@@ -975,18 +1051,18 @@ __device__ void tc_load_network(TcSmem& s, const __nv_bfloat16* __restrict__ wb,
   for (int e = threadIdx.x; e < MLP_OUT; e += nt) s.b5[e] = pf[MLP_OFF_B5 + e];
 }
 
-// Issues layer `layer` (0: K = 16 -> 128, 1-3: 128 -> 128, 4: 128 -> 16) of
-// one group: A = the group's activation tile, D = its TMEM columns.
+// Issues layer `layer` (0: K = 16 -> 128, 1-3: 128 -> 128, 4: 128 -> MLP_OUT)
+// of one group: A = the group's activation tile, D = its TMEM columns.
 __device__ __forceinline__ void tc_issue_layer(const TcSmem& s, uint32_t act, uint32_t dtm, int layer) {
   constexpr uint32_t ID128 = tc::idesc_bf16_f32(128, 128);
-  constexpr uint32_t ID16 = tc::idesc_bf16_f32(128, 16);
+  constexpr uint32_t IDOUT = tc::idesc_bf16_f32(128, MLP_OUT);
   if (layer == 0) {
     tc::mma_bf16(dtm, tc::desc_sw128(act), tc::desc_sw128(tc::smem_u32(s.w1)), ID128, 0u);
     return;
   }
   const uint32_t wbase = layer < 4 ? tc::smem_u32(s.wh[layer - 1][0]) : tc::smem_u32(s.w5[0]);
-  const uint32_t watom = layer < 4 ? TC_ATOM : 16u * 128u;
-  const uint32_t id = layer < 4 ? ID128 : ID16;
+  const uint32_t watom = layer < 4 ? TC_ATOM : uint32_t(MLP_OUT) * 128u;
+  const uint32_t id = layer < 4 ? ID128 : IDOUT;
 #pragma unroll
   for (int kk = 0; kk < 8; kk++) {
     const uint32_t ka = (kk >> 2) * TC_ATOM + (kk & 3) * 32;
@@ -996,6 +1072,7 @@ __device__ __forceinline__ void tc_issue_layer(const TcSmem& s, uint32_t act, ui
 }
 
 // One group's view of the engine.
+template <bool MAG>
 struct TcEngine {
   const TraceParams& P;
   const SurrogateParams& S;
@@ -1009,9 +1086,10 @@ struct TcEngine {
 
   __device__ bool any(bool b) const { return tc::bar_any(1 + g, 128, b); }
 
-  // Network outputs y (16) for this thread's features; all 128 threads of
-  // the group call it together.  False (group-uniform) if an MMA wait ran out.
-  __device__ bool forward(const float* feat, float* y) {
+  // Network outputs for this thread's features, contracted with the source
+  // strengths into c (contract_outputs); all 128 threads of the group call
+  // it together.  False (group-uniform) if an MMA wait ran out.
+  __device__ __forceinline__ bool forward(const float* feat, float* c) {
     tc::st_shared_v4(act + tc::sw128(row, 0), pack_bf16(feat[0], feat[1]), pack_bf16(feat[2], feat[3]),
                      pack_bf16(feat[4], feat[5]), pack_bf16(feat[6], feat[7]));
     tc::st_shared_v4(act + tc::sw128(row, 1), pack_bf16(feat[8], feat[9]), pack_bf16(feat[10], feat[11]),
@@ -1053,11 +1131,9 @@ struct TcEngine {
           if (c < 7) tc::tmem_ld16(tld + 16 * (c + 1), nxt);
           uint32_t q[8];
 #pragma unroll
-          for (int j = 0; j < 8; j++) {
-            const float h0 = __uint_as_float(cur[2 * j]) + bias[16 * c + 2 * j];
-            const float h1 = __uint_as_float(cur[2 * j + 1]) + bias[16 * c + 2 * j + 1];
-            q[j] = pack_bf16(fmaf(h0, tanh_fast(h0), h0), fmaf(h1, tanh_fast(h1), h1));
-          }
+          for (int j = 0; j < 8; j++)
+            q[j] = silu2_bf16_half(__uint_as_float(cur[2 * j]) + bias[16 * c + 2 * j],
+                                   __uint_as_float(cur[2 * j + 1]) + bias[16 * c + 2 * j + 1]);
           // next layer's K = 16c .. 16c + 15: atom c / 4, chunks 2 (c % 4), 2 (c % 4) + 1
           const uint32_t base = act + (c >> 2) * TC_ATOM;
           tc::st_shared_v4(base + tc::sw128(row, 2 * (c & 3)), q[0], q[1], q[2], q[3]);
@@ -1065,26 +1141,42 @@ struct TcEngine {
           if (c < 7) tc::tmem_wait_ld16(nxt);
         }
       } else {
-        uint32_t v[16];
-        tc::tmem_ld16(tld, v);
-        tc::tmem_wait_ld16(v);
+        // the MLP_OUT outputs 16 columns at a time, contracted as they come
+        c[0] = c[1] = 0.f;
+        if (MAG) c[2] = c[3] = 0.f;
 #pragma unroll
-        for (int j = 0; j < MLP_OUT; j++) y[j] = __uint_as_float(v[j]) + s.b5[j];
+        for (int hc = 0; hc < MLP_OUT / 16; hc++) {
+          uint32_t v[16];
+          tc::tmem_ld16(tld + 16 * hc, v);
+          tc::tmem_wait_ld16(v);
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const int o = 16 * hc + j;
+            const float y = __uint_as_float(v[j]) + s.b5[o];
+            c[0] = fmaf(S.wr[o], y, c[0]);
+            c[1] = fmaf(S.wz[o], y, c[1]);
+            if (MAG) {
+              c[2] = fmaf(S.hr[o], y, c[2]);
+              c[3] = fmaf(S.hz[o], y, c[3]);
+            }
+          }
+        }
       }
     }
     return true;
   }
 
-  __device__ bool field(const double* p, bool live, double* E, bool& used_bem) {
+  __device__ __forceinline__ bool field(const double* p, bool live, double* E, double* H, bool& used_bem) {
     const double r2 = p[0] * p[0] + p[1] * p[1], r = sqrt(r2);
-    float f[MLP_IN], y[MLP_OUT];
+    float f[MLP_IN], c[4];
     mlp_features(r, p[2], S.dom, f);
-    if (!forward(f, y)) {
+    if (!forward(f, c)) {
       E[0] = E[1] = E[2] = 0.0;
+      if (MAG) H[0] = H[1] = H[2] = 0.0;
       used_bem = false;
       return false;
     }
-    surrogate_combine(P, S, s.segs, p, r2, r, live, y, E, used_bem);
+    surrogate_combine<MAG>(P, S, s.segs, p, r2, r, live, c, E, H, used_bem);
     return true;
   }
 };
@@ -1119,29 +1211,34 @@ __device__ void tc_teardown(TcSmem& s) {
   }
 }
 
-__device__ __forceinline__ TcEngine tc_engine(const TraceParams& P, const SurrogateParams& S, TcSmem& s) {
+template <bool MAG>
+__device__ __forceinline__ TcEngine<MAG> tc_engine(const TraceParams& P, const SurrogateParams& S, TcSmem& s) {
   const int g = threadIdx.x / 128, row = threadIdx.x % 128;
   const uint32_t dtm = s.tmem_base + uint32_t(128 * g);
   const uint32_t tld = dtm + (uint32_t((threadIdx.x / 32) % 4 * 32) << 16);
-  return TcEngine{P, S, s, g, row, tc::smem_u32(s.act[g][0]), dtm, tld, 0u};
+  return TcEngine<MAG>{P, S, s, g, row, tc::smem_u32(s.act[g][0]), dtm, tld, 0u};
 }
 
+template <bool MAG>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_trace_surrogate_tc(TraceParams P, SurrogateParams S) {
   extern __shared__ __align__(1024) unsigned char tc_raw[];
   TcSmem& s = tc_setup(tc_raw, S);
-  TcEngine eng = tc_engine(P, S, s);
-  surrogate_trace_loop(P, S, eng);
+  TcEngine<MAG> eng = tc_engine<MAG>(P, S, s);
+  surrogate_trace_loop<MAG>(P, S, eng);
   tc_teardown(s);
 }
 
-// Surrogate field at M points (one point per thread, 128 per group), for
-// tests; used_bem = -1 marks points whose MMA wait ran out.
+// Surrogate field E (and with MAG the magnetic field H) at M points (one
+// point per thread, 128 per group), for tests; used_bem = -1 marks points
+// whose MMA wait ran out.
+template <bool MAG>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_surrogate_points_tc(TraceParams P, SurrogateParams S, const double* __restrict__ pts, int64_t M,
-                          double* __restrict__ field, int32_t* __restrict__ used_bem) {
+                          double* __restrict__ field, double* __restrict__ hfield, int32_t* __restrict__ used_bem) {
   extern __shared__ __align__(1024) unsigned char tc_raw[];
   TcSmem& s = tc_setup(tc_raw, S);
-  TcEngine eng = tc_engine(P, S, s);
+  TcEngine<MAG> eng = tc_engine<MAG>(P, S, s);
+  const double nan = __longlong_as_double(0x7ff8000000000000LL);
   for (int64_t base = ((int64_t)blockIdx.x * TC_GROUPS + eng.g) * 128; base < M;
        base += (int64_t)gridDim.x * TC_THREADS) {
     const int64_t i = base + eng.row;
@@ -1149,11 +1246,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     double p[3] = {0.5 * S.dom.r_max, 0.0, S.dom.z_c};
     if (live)
       for (int c = 0; c < 3; c++) p[c] = pts[3 * i + c];
-    double E[3];
+    double E[3], H[3] = {0.0, 0.0, 0.0};
     bool ub;
-    const bool ok = eng.field(p, live, E, ub);
+    const bool ok = eng.field(p, live, E, H, ub);
     if (live) {
-      for (int c = 0; c < 3; c++) field[3 * i + c] = ok ? E[c] : __longlong_as_double(0x7ff8000000000000LL);
+      for (int c = 0; c < 3; c++) field[3 * i + c] = ok ? E[c] : nan;
+      if (hfield)
+        for (int c = 0; c < 3; c++) hfield[3 * i + c] = ok ? H[c] : nan;
       if (used_bem) used_bem[i] = ok ? (ub ? 1 : 0) : -1;
     }
     if (!ok) break;
@@ -1177,23 +1276,37 @@ static int set_smem_once(K* kernel, int bytes, bool (&done)[64]) {
   if (dev >= 0 && dev < 64) done[dev] = true;
   return OK;
 }
-static bool g_attr_trace_tc[64], g_attr_points_tc[64], g_attr_trace_warp[64], g_attr_points_warp[64];
+static bool g_attr_trace_tc[2][64], g_attr_points_tc[2][64], g_attr_trace_warp[2][64], g_attr_points_warp[2][64];
 
+// Kernel parameters of a surrogate launch; `mag` is set when the field has a
+// magnetic part (coils in the network, a magnetostatic axial table, or
+// magnetostatic charges / current rings for the fallback).
 static int fill_surrogate_params(const tb_field_t* field, const tb_surrogate_t* sur, TraceParams& P,
-                                 SurrogateParams& S) {
+                                 SurrogateParams& S, bool& mag) {
   if (!field->axial_z || field->axial_nz < 2 || !field->axial_elec) return BAD_ARG;
-  if (field->n_elec > 0 && !field->elec_sources) return BAD_ARG;
-  if (!sur->weights_bf16 || !sur->params_f32 || sur->n_electrodes < 1 || sur->n_electrodes > MLP_MAX_ELECTRODES)
+  if ((field->n_elec > 0 && !field->elec_sources) || (field->n_mag > 0 && !field->mag_sources) ||
+      (field->n_cur > 0 && !field->cur_sources) || field->n_elec < 0 || field->n_mag < 0 || field->n_cur < 0)
+    return BAD_ARG;
+  const int nsrc = sur->n_electrodes + sur->n_coils;
+  if (!sur->weights_bf16 || !sur->params_f32 || sur->n_electrodes < 0 || sur->n_coils < 0 || nsrc < 1 ||
+      nsrc > MLP_MAX_SOURCES)
     return BAD_ARG;
   if (sur->n_segments < 0 || sur->n_segments > SG_MAX_SEGS || (sur->n_segments > 0 && !sur->segments)) return BAD_ARG;
   if (!(sur->r_max > 0) || !(sur->z_half > 0) || sur->env_power < 0 || sur->env_power > 32) return BAD_ARG;
+  if (sur->engine != 0 && sur->engine != 1) return BAD_ARG;
+  mag = sur->n_coils > 0 || field->axial_mag != nullptr || field->n_mag > 0 || field->n_cur > 0;
   memset(&P, 0, sizeof(P));
   P.wait_cycles = wait_limit();
   P.esrc = field->elec_sources;
   P.ne = field->n_elec;
+  P.msrc = field->mag_sources;
+  P.nm = field->n_mag;
+  P.csrc = field->cur_sources;
+  P.nc = field->n_cur;
   P.fb = field->field_bounds;
   P.az = field->axial_z;
   P.aec = field->axial_elec;
+  P.amc = field->axial_mag;
   P.anz = field->axial_nz;
   memset(&S, 0, sizeof(S));
   S.wb = static_cast<const __nv_bfloat16*>(sur->weights_bf16);
@@ -1201,39 +1314,76 @@ static int fill_surrogate_params(const tb_field_t* field, const tb_surrogate_t* 
   S.dom = MlpDomain{sur->r_max, sur->z_c, sur->z_half};
   S.z_lo = sur->z_lo;
   S.z_hi = sur->z_hi;
-  S.n_el = sur->n_electrodes;
-  for (int e = 0; e < MLP_MAX_ELECTRODES; e++) S.volts[e] = sur->volts[e];
-  for (int c = 0; c < MLP_OUT; c++) S.scale[c] = sur->scale[c];
+  for (int src = 0; src < nsrc; src++) {
+    const double v = sur->strengths[src];
+    float* wr = src < sur->n_electrodes ? S.wr : S.hr;
+    float* wz = src < sur->n_electrodes ? S.wz : S.hz;
+    wr[3 * src + 1] = float(v * double(sur->scale[3 * src + 1]));
+    wz[3 * src + 2] = float(v * double(sur->scale[3 * src + 2]));
+  }
   S.env_p = sur->env_power;
   S.segs = sur->segments;
   S.nseg = sur->n_segments;
   S.fb_dist2 = sur->fallback_dist * sur->fallback_dist;
-  if (sur->engine != 0 && sur->engine != 1) return BAD_ARG;
   return OK;
 }
 
+template <bool MAG>
+static int launch_points(const TraceParams& P, const SurrogateParams& S, int engine, const double* points, int64_t M,
+                         double* out, double* out_h, int32_t* used_bem, cudaStream_t stream) {
+  if (engine == 0) {
+    if (set_smem_once(k_surrogate_points_tc<MAG>, TC_SMEM_BYTES, g_attr_points_tc[MAG]) != OK) return CUDA_ERR;
+    int64_t blocks = (M + TC_THREADS - 1) / TC_THREADS;
+    if (blocks > num_sms()) blocks = num_sms();
+    k_surrogate_points_tc<MAG><<<unsigned(blocks), TC_THREADS, TC_SMEM_BYTES, stream>>>(P, S, points, M, out, out_h,
+                                                                                      used_bem);
+    return launch_status();
+  }
+  const int smem = int(sizeof(SurrogateSmem));
+  if (set_smem_once(k_surrogate_points<MAG>, smem, g_attr_points_warp[MAG]) != OK) return CUDA_ERR;
+  int64_t blocks = (M + SG_THREADS - 1) / SG_THREADS;
+  if (blocks > 4 * num_sms()) blocks = 4 * num_sms();
+  k_surrogate_points<MAG><<<unsigned(blocks), SG_THREADS, smem, stream>>>(P, S, points, M, out, out_h, used_bem);
+  return launch_status();
+}
+
 extern "C" int tb_surrogate_field_points(const double* points, int64_t M, const tb_field_t* field,
-                                         const tb_surrogate_t* sur, double* out, int32_t* used_bem,
+                                         const tb_surrogate_t* sur, double* out, double* out_h, int32_t* used_bem,
                                          tb_stream_t stream) {
   if (!field || !sur || M < 0 || (M > 0 && (!points || !out))) return BAD_ARG;
   if (M == 0) return OK;
   TraceParams P;
   SurrogateParams S;
-  int st = fill_surrogate_params(field, sur, P, S);
+  bool mag = false;
+  int st = fill_surrogate_params(field, sur, P, S, mag);
   if (st != OK) return st;
-  if (sur->engine == 0) {
-    if (set_smem_once(k_surrogate_points_tc, TC_SMEM_BYTES, g_attr_points_tc) != OK) return CUDA_ERR;
-    int64_t blocks = (M + TC_THREADS - 1) / TC_THREADS;
-    if (blocks > num_sms()) blocks = num_sms();
-    k_surrogate_points_tc<<<unsigned(blocks), TC_THREADS, TC_SMEM_BYTES, (cudaStream_t)stream>>>(P, S, points, M, out,
-                                                                                              used_bem);
+  if (out_h && !mag) {
+    if (cudaMemsetAsync(out_h, 0, sizeof(double) * 3 * M, (cudaStream_t)stream) != cudaSuccess) return CUDA_ERR;
+    out_h = nullptr;
+  }
+  return mag ? launch_points<true>(P, S, sur->engine, points, M, out, out_h, used_bem, (cudaStream_t)stream)
+             : launch_points<false>(P, S, sur->engine, points, M, out, out_h, used_bem, (cudaStream_t)stream);
+}
+
+template <bool MAG>
+static int launch_trace(const TraceParams& P, const SurrogateParams& S, int engine, int64_t n, cudaStream_t s) {
+  if (engine == 0) {
+    // one CTA (3 groups of 128 particles) per SM; fewer only when there are
+    // fewer particles than that
+    if (set_smem_once(k_trace_surrogate_tc<MAG>, TC_SMEM_BYTES, g_attr_trace_tc[MAG]) != OK) return CUDA_ERR;
+    int64_t blocks = num_sms();
+    const int64_t by_work = (n + TC_THREADS - 1) / TC_THREADS;
+    if (blocks > by_work) blocks = by_work;
+    k_trace_surrogate_tc<MAG><<<unsigned(blocks), TC_THREADS, TC_SMEM_BYTES, s>>>(P, S);
     return launch_status();
   }
   const int smem = int(sizeof(SurrogateSmem));
-  if (set_smem_once(k_surrogate_points, smem, g_attr_points_warp) != OK) return CUDA_ERR;
-  int64_t blocks = (M + SG_THREADS - 1) / SG_THREADS;
-  if (blocks > 4 * num_sms()) blocks = 4 * num_sms();
-  k_surrogate_points<<<unsigned(blocks), SG_THREADS, smem, (cudaStream_t)stream>>>(P, S, points, M, out, used_bem);
+  if (set_smem_once(k_trace_surrogate<MAG>, smem, g_attr_trace_warp[MAG]) != OK) return CUDA_ERR;
+  // one block per SM; fewer only when there is not a warp of particles per SM
+  int64_t blocks = num_sms();
+  int64_t by_work = (n + 31) / 32;
+  if (blocks > by_work) blocks = by_work;
+  k_trace_surrogate<MAG><<<unsigned(blocks), SG_THREADS, smem, s>>>(P, S);
   return launch_status();
 }
 
@@ -1247,13 +1397,14 @@ extern "C" int tb_trace_surrogate(const double* start, const double* t0, const d
   if (opts->max_attempts <= 0 || !(opts->atol > 0)) return BAD_ARG;
   TraceParams P;
   SurrogateParams S;
-  int st = fill_surrogate_params(field, sur, P, S);
+  bool mag = false;
+  int st = fill_surrogate_params(field, sur, P, S, mag);
   if (st != OK) return st;
   for (int i = 0; i < 6; i++) P.bounds[i] = opts->bounds[i];
   P.atol = opts->atol;
   P.plane_z = opts->plane_z;
   P.record_plane = opts->record_plane;
-  P.max_attempts = opts->max_attempts;
+  P.max_attempts = opts->max_attempts < 0x7fffffff ? opts->max_attempts : 0x7fffffff;
   P.start = start;
   P.t0 = t0;
   P.qm = qm;
@@ -1265,24 +1416,7 @@ extern "C" int tb_trace_surrogate(const double* start, const double* t0, const d
   P.work = work;
   cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemsetAsync(work, 0, sizeof(int32_t), s) != cudaSuccess) return CUDA_ERR;
-  if (sur->engine == 0) {
-    // one CTA (3 groups of 128 particles) per SM; fewer only when there are
-    // fewer particles than that
-    if (set_smem_once(k_trace_surrogate_tc, TC_SMEM_BYTES, g_attr_trace_tc) != OK) return CUDA_ERR;
-    int64_t blocks = num_sms();
-    const int64_t by_work = (n + TC_THREADS - 1) / TC_THREADS;
-    if (blocks > by_work) blocks = by_work;
-    k_trace_surrogate_tc<<<unsigned(blocks), TC_THREADS, TC_SMEM_BYTES, s>>>(P, S);
-    return launch_status();
-  }
-  const int smem = int(sizeof(SurrogateSmem));
-  if (set_smem_once(k_trace_surrogate, smem, g_attr_trace_warp) != OK) return CUDA_ERR;
-  // one block per SM; fewer only when there is not a warp of particles per SM
-  int64_t blocks = num_sms();
-  int64_t by_work = (n + 31) / 32;
-  if (blocks > by_work) blocks = by_work;
-  k_trace_surrogate<<<unsigned(blocks), SG_THREADS, smem, s>>>(P, S);
-  return launch_status();
+  return mag ? launch_trace<true>(P, S, sur->engine, n, s) : launch_trace<false>(P, S, sur->engine, n, s);
 }
 
 static int trace_rk45(const double* start, const double* t0, const double* qm, const int32_t* geom, int64_t n,

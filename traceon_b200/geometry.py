@@ -174,10 +174,11 @@ def electron_beam(n: int, seed: int, energy_ev: float = 1000.0, z0: float = -9.5
     return pos, vel
 
 
-def surrogate_beam(n: int, seed: int):
+def surrogate_beam(n: int, seed: int, r_max: float = 0.2 * MM):
     """The learned-surrogate workload's beam: 1 keV +-5 % (uniform), angles
-    +-20 mrad, start radius up to 0.2 mm at z = -9.5 mm."""
-    return electron_beam(n, seed, r_max=0.2 * MM, angle_max=20e-3, energy_spread=0.05)
+    +-20 mrad, start radius up to r_max (default 0.2 mm, the plain-method
+    workload's beam) at z = -9.5 mm."""
+    return electron_beam(n, seed, r_max=r_max, angle_max=20e-3, energy_spread=0.05)
 
 
 LENS_BOUNDS = np.array([[-2 * MM, 2 * MM], [-2 * MM, 2 * MM], [-10 * MM, 10 * MM]])
@@ -215,3 +216,98 @@ def random_lens(seed: int, n_range=(500, 6000), tubes_range=(2, 5), r_range=(0.5
         counts += tube_counts(r, r + cap, z0, z1, max(int(m), 6))
     geo = LensGeometry(np.concatenate(verts), np.concatenate(idx), [f'electrode{i}' for i in range(k)], segs, counts)
     return geo, rng.uniform(*volt_range, k)
+
+
+# ---------------------------------------------------------------- combined lens
+# Outline of the iron pole piece of the combined workload's magnetic lens, in
+# (r, z) mm: a closed C-shaped yoke whose bore (r = 2.5 mm) is open over
+# |z| < 1 mm (the gap between the pole tips) and whose window r in
+# (2.8, 7) mm, |z| < 5 mm holds the coils.
+POLE_OUTLINE_MM = [(2.5, -6.0), (8.0, -6.0), (8.0, 6.0), (2.5, 6.0), (2.5, 1.0), (2.8, 1.0), (2.8, 5.0),
+                   (7.0, 5.0), (7.0, -5.0), (2.8, -5.0), (2.8, -1.0), (2.5, -1.0), (2.5, -6.0)]
+
+
+def outward_oriented(vertices: np.ndarray) -> np.ndarray:
+    """The line4 elements of one closed outline, reversed if needed so that
+    their normals point out of the enclosed body -- the test the reference
+    mesher applies by default (traceon/mesher.py:730-739, divergence
+    theorem: sum of r_mid n_r length > 0).  Reversal swaps start/end and the
+    1/3 / 2/3 points of every element and the element order."""
+    v = np.asarray(vertices, dtype=np.float64)
+    d = v[:, 1] - v[:, 0]
+    length = np.hypot(d[:, 0], d[:, 2])
+    n_r = d[:, 2] / np.where(length > 0, length, 1.0)  # normal_2d: (dz, -dr) / |d|
+    mid_r = 0.5 * (v[:, 0, 0] + v[:, 1, 0])
+    if np.sum(mid_r * n_r * length) > 0:
+        return v
+    return v[::-1][:, [1, 0, 3, 2]].copy()
+
+
+def coil_rings(r, z, current, half_width=0.1 * MM):
+    """Current rings as the reference's current quadrature (N, 12) weights and
+    (N, 12, 3) points (y = 0): each coil a square cross-section of side
+    2 half_width around (r, z) sampled at 12 points (a 4 x 3 grid) of equal
+    weight; current density x weights sums to the coil's A-turns.  Returns
+    (current densities (N,), jac (N, 12), pos (N, 12, 3))."""
+    r, z, current = (np.atleast_1d(np.asarray(a, dtype=np.float64)) for a in (r, z, current))
+    area = (2 * half_width) ** 2
+    ur = (np.arange(4) + 0.5) / 4 * 2 - 1
+    uz = (np.arange(3) + 0.5) / 3 * 2 - 1
+    gr, gz = np.meshgrid(ur, uz, indexing='ij')
+    pos = np.zeros((len(r), 12, 3))
+    pos[:, :, 0] = r[:, None] + half_width * gr.reshape(-1)[None]
+    pos[:, :, 2] = z[:, None] + half_width * gz.reshape(-1)[None]
+    jac = np.full((len(r), 12), area / 12)
+    return current / area, jac, pos
+
+
+class CombinedLens:
+    """The combined electro-magnetostatic workload: the three-tube einzel
+    lens (electrodes ground_in, lens, ground_out) inside the iron pole piece
+    `pole` of a magnetic lens, magnetised by current coils.  `geometry` holds
+    all elements (electrostatic first); coils: (r, z, A-turns) per coil."""
+
+    def __init__(self, geometry, coils):
+        self.geometry = geometry
+        self.coil_r, self.coil_z, self.coil_current = (np.asarray(a, dtype=np.float64) for a in coils)
+
+    def coil_sources(self, currents=None):
+        """(current densities, jac, pos) of the coils (at `currents`, default
+        their own A-turns)."""
+        cur = self.coil_current if currents is None else np.asarray(currents, dtype=np.float64)
+        return coil_rings(self.coil_r, self.coil_z, cur)
+
+
+def combined_lens(seed: int, n_elec: int = 16384, n_mag: int = 16384, n_coils: int = 4) -> CombinedLens:
+    """The combined workload's geometry: the einzel lens meshed to n_elec
+    elements, the pole piece outline (POLE_OUTLINE_MM) meshed to n_mag
+    elements graded toward its corners, normals out of the iron, and n_coils
+    coils with r ~ U[3, 6] mm, z ~ U[-4, 4] mm, currents ~ U[0.5, 5] kA-turns
+    from the seed."""
+    lens = einzel_lens(n_elec)
+    pts = np.array(POLE_OUTLINE_MM) * MM
+    seg = np.hypot(*(pts[1:] - pts[:-1]).T)
+    pole = outward_oriented(polyline_elements(pts, split_counts(n_mag, seg)))
+    verts = np.concatenate([lens.vertices, pole])
+    idx = np.concatenate([lens.electrode_index, np.full(len(pole), len(lens.names))])
+    segs = np.concatenate([lens.segments, np.stack([pts[:-1, 0], pts[:-1, 1], pts[1:, 0], pts[1:, 1]], 1)])
+    geo = LensGeometry(verts, idx, lens.names + ['pole'], segs)
+    rng = np.random.default_rng(seed)
+    coils = (rng.uniform(3e-3, 6e-3, n_coils), rng.uniform(-4e-3, 4e-3, n_coils),
+             rng.uniform(500.0, 5000.0, n_coils))
+    return CombinedLens(geo, coils)
+
+
+def combined_beam(n: int, seed: int, r_max: float = 0.2 * MM, angle_max: float = 10e-3):
+    """The combined workload's beam: electrons at 5 keV with a lognormal
+    energy spread of 2 % (sigma of log E = 0.02), start radius up to r_max at
+    z = -9.5 mm, angles U[-a, a] in the xz-plane."""
+    from scipy.constants import e, m_e
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(0.0, r_max, n)
+    ang = rng.uniform(-angle_max, angle_max, n)
+    energy = 5000.0 * np.exp(rng.normal(0.0, 0.02, n))
+    speed = np.sqrt(2 * energy * e / m_e)[:, None]
+    pos = np.stack([r, np.zeros(n), np.full(n, -9.5 * MM)], axis=1)
+    vel = speed * np.stack([np.sin(ang), np.zeros(n), np.cos(ang)], axis=1)
+    return pos, vel

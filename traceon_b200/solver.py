@@ -34,17 +34,58 @@ class SolverRadial:
         N = len(self.vertices)
         types = np.zeros(N, dtype=np.uint8)
         values = np.zeros(N)
+        self._dev = None
+        self._centers = None
         for n, indices in names.items():
             t, v = excitation.excitation_types[n]
             types[indices] = int(t)
             if int(t) != int(ET.VOLTAGE_FUN):
                 values[indices] = v
             else:
-                values[indices] = [v(*self.get_center_of_element(i)) for i in np.atleast_1d(indices)]
+                values[indices] = self._voltage_function_values(v, np.atleast_1d(indices))
         self.excitation_types = types
         self.excitation_values = values
         self.jac_buffer, self.pos_buffer = (None, None)
-        self._dev = None
+
+    def _element_centers_device(self):
+        """(N, 2) device tensor of the elements' collocation points (r, z) at
+        alpha = 0 and (N, 2) normals (tb_element_targets)."""
+        if self._centers is None:
+            torch = B._torch()
+            v = B.to_dev(self.vertices, torch.float64)
+            self._centers = B.dev_element_targets(v)
+        return self._centers
+
+    def _voltage_function_values(self, fun, indices):
+        """A VOLTAGE_FUN excitation at the centres of the given elements
+        (traceon/solver.py:57-61 calls it once per element).  The centres are
+        computed on the device, and the function is first called once on the
+        device tensors x = r, y = 0, z, so that a function written with
+        arithmetic and torch operations is evaluated on the GPU in one call;
+        then once on NumPy arrays; a function that accepts neither (Python
+        control flow on its arguments, math-module calls) is called per
+        element as in the reference.  Returns a float64 array."""
+        torch = B._torch()
+        tgt, _ = self._element_centers_device()
+        idx = torch.as_tensor(indices, dtype=torch.int64, device=tgt.device)
+        r, z = tgt[idx, 0], tgt[idx, 1]
+        n = len(indices)
+        for args in ((r, torch.zeros_like(r), z), None):
+            try:
+                if args is None:
+                    rn, zn = r.cpu().numpy(), z.cpu().numpy()
+                    out = fun(rn, np.zeros_like(rn), zn)
+                else:
+                    out = fun(*args)
+                if isinstance(out, torch.Tensor):
+                    out = out.to(torch.float64).cpu().numpy()
+                out = np.broadcast_to(np.asarray(out, dtype=np.float64), (n,)).copy()
+                if np.all(np.isfinite(out)):
+                    return out
+            except Exception:
+                pass
+        c = tgt[idx].cpu().numpy()
+        return np.array([fun(c[k, 0], 0.0, c[k, 1]) for k in range(n)], dtype=np.float64)
 
     # ---- device state
     def device(self):
@@ -76,23 +117,31 @@ class SolverRadial:
     def get_preexisting_field(self, point):
         return np.zeros(3)
 
+    def preexisting_field_device(self, centers):
+        """Pre-existing field (N, 3) at the collocation points (r, 0, z) given
+        as (N, 2) device tensor, or None when there is none."""
+        return None
+
+    def get_right_hand_side_device(self):
+        """traceon/solver.py:118-150 on the device: voltage rows take their
+        value, dielectric rows 0, magnetizable rows -factor(mu) H . n with the
+        pre-existing field H at each element's collocation point, all in one
+        launch (tb_rhs_radial_field).  Returns an (N,) device tensor."""
+        torch = B._torch()
+        v, t, val, _, _ = self.device()
+        N = len(self.vertices)
+        F = torch.empty(N, dtype=torch.float64, device=v.device)
+        if N == 0:
+            return F
+        tgt, nrm = self._element_centers_device()
+        field = self.preexisting_field_device(tgt) if (self.excitation_types == ET.MAGNETIZABLE).any() else None
+        B._call('tb_rhs_radial_field', t.data_ptr(), val.data_ptr(), nrm.data_ptr(), B._ptr(field), F.data_ptr(), N,
+                B._stream())
+        return F
+
     def get_right_hand_side(self):
         """traceon/solver.py:118-150"""
-        N = self.get_number_of_matrix_elements()
-        F = np.zeros(N)
-        normals = None
-        for i, (t, v) in enumerate(zip(self.excitation_types, self.excitation_values)):
-            if t in (ET.VOLTAGE_FIXED, ET.VOLTAGE_FUN, ET.MAGNETOSTATIC_POT):
-                F[i] = v
-            elif t == ET.DIELECTRIC:
-                F[i] = 0.0
-            elif t == ET.MAGNETIZABLE:
-                if normals is None:
-                    normals = self.get_normal_vectors()
-                center = self.get_center_of_element(i)
-                n = normals[i]
-                F[i] = -B.flux_density_to_charge_factor(v) * np.dot(self.get_preexisting_field(center),
-                                                                     [n[0], 0.0, n[1]])
+        F = self.get_right_hand_side_device().cpu().numpy()
         assert np.all(np.isfinite(F))
         return F
 
@@ -178,6 +227,17 @@ class MagnetostaticSolverRadial(SolverRadial):
 
     def get_preexisting_field(self, point):
         return self.preexisting_field.magnetostatic_field_at_point(point)
+
+    def preexisting_field_device(self, centers):
+        """The current rings' field at all collocation points in one launch
+        (tb_current_field_points)."""
+        if not len(self.current_point_charges):
+            return None
+        torch = B._torch()
+        pts = torch.zeros((centers.shape[0], 3), dtype=torch.float64, device=centers.device)
+        pts[:, 0] = centers[:, 0]
+        pts[:, 2] = centers[:, 1]
+        return B.dev_current_field_points(pts, self.current_point_charges.device_sources())
 
     def charges_to_field(self, charges):
         return FieldRadialBEM(magnetostatic_point_charges=charges,

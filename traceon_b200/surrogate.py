@@ -30,7 +30,8 @@ import numpy as np
 
 from . import backend as B
 
-IN, H, OUT = 16, 128, 16
+IN, H, OUT = 16, 128, 32
+MAX_SOURCES = OUT // 3  # electrodes + coils, 3 outputs each
 OFF = {}
 _o = 0
 for _name, _n in (('W1', H * IN), ('b1', H), ('W2', H * H), ('b2', H), ('W3', H * H), ('b3', H), ('W4', H * H),
@@ -60,8 +61,9 @@ class TbSurrogate(C.Structure):
     """tb_surrogate_t of include/traceon_b200.h"""
     _fields_ = [('weights_bf16', _vp), ('params_f32', _vp), ('r_max', C.c_double), ('z_c', C.c_double),
                 ('z_half', C.c_double), ('z_lo', C.c_double), ('z_hi', C.c_double), ('n_electrodes', C.c_int),
-                ('volts', C.c_double * 5), ('scale', C.c_float * 16), ('env_power', C.c_int), ('segments', _vp),
-                ('n_segments', C.c_int), ('fallback_dist', C.c_double), ('engine', C.c_int)]
+                ('n_coils', C.c_int), ('strengths', C.c_double * MAX_SOURCES), ('scale', C.c_float * OUT),
+                ('env_power', C.c_int), ('segments', _vp), ('n_segments', C.c_int), ('fallback_dist', C.c_double),
+                ('engine', C.c_int)]
 
 
 def _call(name, *args):
@@ -101,7 +103,7 @@ class MLP:
         return t[o:o + n]
 
     def forward(self, X, keep=False):
-        """X (M, 16) bf16 features -> (M, 16) fp32 outputs; with keep, also
+        """X (M, 16) bf16 features -> (M, 32) fp32 outputs; with keep, also
         the pre-activations Z_l (fp32) and activations Y_l (bf16)."""
         torch = B._torch()
         M = X.shape[0]
@@ -167,29 +169,40 @@ def features(points_t, r_max, z_c, z_half):
 
 
 class SurrogateModel:
-    """Network + normalisation of a surrogate for one lens geometry."""
+    """Network + normalisation of a surrogate for one lens geometry.  Its
+    field sources are n_electrodes electrodes (per unit voltage; outputs
+    (phi, E_r, E_z)) followed by n_coils current coils (per unit current;
+    outputs (magnetostatic potential, H_r, H_z))."""
 
-    def __init__(self, n_electrodes, r_max, z_lo, z_hi, scale, env_power=8, params=None, seed=0):
+    def __init__(self, n_electrodes, r_max, z_lo, z_hi, scale, env_power=8, params=None, seed=0, n_coils=0):
         self.n_el = int(n_electrodes)
+        self.n_coils = int(n_coils)
+        if not 1 <= self.n_el + self.n_coils <= MAX_SOURCES:
+            raise ValueError(f'1 to {MAX_SOURCES} field sources (electrodes + coils)')
         self.r_max, self.z_lo, self.z_hi = float(r_max), float(z_lo), float(z_hi)
         self.z_c, self.z_half = 0.5 * (z_lo + z_hi), 0.5 * (z_hi - z_lo)
         self.scale = np.asarray(scale, dtype=np.float32)
         self.env_power = int(env_power)
         self.mlp = MLP(seed=seed, params=params)
 
+    @property
+    def n_src(self):
+        return self.n_el + self.n_coils
+
     def n_out(self):
-        return 3 * self.n_el
+        return 3 * self.n_src
 
     def envelope(self, r):
-        """(M, n_out) envelope: rho^p for phi and E_z, rho^(p+1) for E_r."""
+        """(M, n_out) envelope: rho^p for the potential and the axial
+        component, rho^(p+1) for the radial component."""
         rho = np.asarray(r) / self.r_max
         e = rho ** self.env_power
-        cols = [e, e * rho, e] * self.n_el
+        cols = [e, e * rho, e] * self.n_src
         return np.stack(cols, axis=1)
 
     def state(self):
-        return {'params': self.mlp.p.cpu().numpy(), 'n_el': self.n_el, 'r_max': self.r_max, 'z_lo': self.z_lo,
-                'z_hi': self.z_hi, 'scale': self.scale, 'env_power': self.env_power}
+        return {'params': self.mlp.p.cpu().numpy(), 'n_el': self.n_el, 'n_coils': self.n_coils, 'r_max': self.r_max,
+                'z_lo': self.z_lo, 'z_hi': self.z_hi, 'scale': self.scale, 'env_power': self.env_power}
 
     def save(self, path):
         np.savez(path, **self.state())
@@ -198,27 +211,74 @@ class SurrogateModel:
     def load(path):
         d = np.load(path)
         return SurrogateModel(int(d['n_el']), float(d['r_max']), float(d['z_lo']), float(d['z_hi']), d['scale'],
-                              int(d['env_power']), params=d['params'])
+                              int(d['env_power']), params=d['params'], n_coils=int(d['n_coils']))
 
     def predict_residual(self, points):
-        """Per-electrode corrections (M, n_el, 3) = (phi, E_r, E_z) at 1 V."""
+        """Per-source corrections (M, n_src, 3) at unit strength: (phi, E_r,
+        E_z) of the electrodes, then (potential, H_r, H_z) of the coils."""
         torch = B._torch()
         pts = B.to_dev(np.asarray(points, dtype=np.float64).reshape(-1, 3), torch.float64)
         y = self.mlp.forward(features(pts, self.r_max, self.z_c, self.z_half)).cpu().numpy()[:, :self.n_out()]
         r = np.hypot(points[:, 0], points[:, 1])
-        return (y * self.scale[:self.n_out()] * self.envelope(r)).reshape(-1, self.n_el, 3)
+        return (y * self.scale[:self.n_out()] * self.envelope(r)).reshape(-1, self.n_src, 3)
 
 
 # ---------------------------------------------------------------- data
-def unit_fields(geo, solver_exc_factory=None):
-    """FieldRadialBEM of every electrode at 1 V, others at 0 V, from one
-    factorisation (the superposition solve of traceon/solver.py:364-400)."""
+def unit_fields(geo, electrodes=None):
+    """FieldRadialBEM of every electrode (default: all names of geo) at 1 V,
+    the others at 0 V, from one factorisation (the superposition solve of
+    traceon/solver.py:364-400)."""
     from .excitation import Excitation, Mesh
     from .solver import ElectrostaticSolverRadial
+    names = list(geo.names) if electrodes is None else list(electrodes)
     exc = Excitation(Mesh.from_geometry(geo))
-    exc.add_voltage(**{n: 1.0 for n in geo.names})
+    exc.add_voltage(**{n: 1.0 for n in names})
     solver = ElectrostaticSolverRadial(exc)
-    return solver.solve_matrix(geo.unit_rhs())
+    F = np.zeros((len(names), len(solver.vertices)))
+    for k, n in enumerate(names):
+        F[k, solver.names[n]] = 1.0
+    return solver.solve_matrix(F)
+
+
+def unit_coil_fields(geo, magnetizable, coils):
+    """FieldRadialBEM of every coil at 1 A-turn, the others off: the current
+    ring plus the magnetostatic charges it induces on the magnetizable
+    electrodes (`magnetizable`: {name: mu_r}), all right-hand sides solved
+    with one factorisation (MagnetostaticSolverRadial, solver.py:267-353).
+    coils: an object with coil_sources(currents) -> (current densities,
+    jac (N, 12), pos (N, 12, 3)) (geometry.CombinedLens)."""
+    from .excitation import Excitation, Mesh
+    from .field import EffectivePointCharges, FieldRadialBEM
+    from .solver import MagnetostaticSolverRadial
+    exc = Excitation(Mesh.from_geometry(geo))
+    exc.add_magnetizable(**magnetizable)
+    n = len(coils.coil_r)
+    rings = []
+    F = []
+    for c in range(n):
+        cur = np.zeros(n)
+        cur[c] = 1.0
+        I, jac, pos = coils.coil_sources(cur)
+        one = EffectivePointCharges(I[c:c + 1], jac[c:c + 1], pos[c:c + 1])
+        rings.append(one)
+        F.append(MagnetostaticSolverRadial(exc, current_point_charges=one).get_right_hand_side())
+    solver = MagnetostaticSolverRadial(exc)
+    X = solver.solve_charges_device(np.array(F)).cpu().numpy()
+    jac, pos = solver.jacobians_and_positions()
+    return [FieldRadialBEM(magnetostatic_point_charges=EffectivePointCharges(x, jac, pos), current_point_charges=r)
+            for x, r in zip(X, rings)]
+
+
+def _field_table(f, zt, dz):
+    """Axial coefficient table (nz-1, 9, 6) of a unit field: its electrostatic
+    charges, or for a coil its magnetostatic charges plus its current ring
+    (FieldRadialAxial's magnetostatic table, traceon/field.py:971-991)."""
+    if len(f.electrostatic_point_charges):
+        d = B.dev_axial_derivatives(zt, f.electrostatic_point_charges.device_sources())
+    else:
+        d = B.dev_axial_derivatives(zt, f.magnetostatic_point_charges.device_sources())
+        d = d + B.dev_axial_derivatives(zt, f.current_point_charges.device_sources(), current=True)
+    return B.dev_axial_coefficients(d, dz)
 
 
 def axial_tables(fields, z_lo, z_hi, nz):
@@ -226,11 +286,7 @@ def axial_tables(fields, z_lo, z_hi, nz):
     torch = B._torch()
     z = np.linspace(z_lo, z_hi, nz)
     zt = B.to_dev(z, torch.float64)
-    tabs = []
-    for f in fields:
-        d = B.dev_axial_derivatives(zt, f.electrostatic_point_charges.device_sources())
-        tabs.append(B.dev_axial_coefficients(d, z[1] - z[0]))
-    return z, zt, tabs
+    return z, zt, [_field_table(f, zt, z[1] - z[0]) for f in fields]
 
 
 def _segment_distance(points_rz, segs):
@@ -262,15 +318,21 @@ def sample_points(n, seed, r_min, r_max, z_lo, z_hi, segs, exclude):
 
 
 def residual_targets(points, fields, zt, tabs, chunk=1 << 20):
-    """(M, n_el, 3) BEM minus axial-series (phi, E_r, E_z) of each unit field
-    at points with y = 0 (so E_x = E_r)."""
+    """(M, n_src, 3) BEM minus axial series of each unit field at points with
+    y = 0 (so the x component is the radial one): (phi, E_r, E_z) of an
+    electrode; (magnetostatic potential of the induced charges, H_r, H_z) of
+    a coil, H being the induced charges' field plus the ring's own."""
     torch = B._torch()
     M = len(points)
     out = np.zeros((M, len(fields), 3))
     for s in range(0, M, chunk):
         pts = B.to_dev(points[s:s + chunk], torch.float64)
         for e, (f, c) in enumerate(zip(fields, tabs)):
-            pb, fb = B.dev_field_points(pts, f.electrostatic_point_charges.device_sources())
+            if len(f.electrostatic_point_charges):
+                pb, fb = B.dev_field_points(pts, f.electrostatic_point_charges.device_sources())
+            else:
+                pb, fb = B.dev_field_points(pts, f.magnetostatic_point_charges.device_sources())
+                fb = fb + B.dev_current_field_points(pts, f.current_point_charges.device_sources())
             pa, fa = B.dev_axial_field_points(pts, zt, c)
             out[s:s + chunk, e, 0] = (pb - pa).cpu().numpy()
             out[s:s + chunk, e, 1] = (fb[:, 0] - fa[:, 0]).cpu().numpy()
@@ -279,14 +341,21 @@ def residual_targets(points, fields, zt, tabs, chunk=1 << 20):
 
 
 class SurrogateTrainer:
-    """Builds the data set of a geometry and trains a SurrogateModel."""
+    """Builds the data set of a geometry and trains a SurrogateModel.  Field
+    sources: the electrodes `electrodes` (default: every name of geo) and,
+    when `coils` is given, its current coils magnetising the `magnetizable`
+    electrodes ({name: mu_r})."""
 
     def __init__(self, geo, r_min=0.1e-3, r_max=0.95e-3, z_lo=-11.5e-3, z_hi=11.5e-3, nz=2301, exclude=50e-6,
-                 env_power=8):
+                 env_power=8, electrodes=None, magnetizable=None, coils=None):
         self.geo = geo
         self.r_min, self.r_max, self.z_lo, self.z_hi = r_min, r_max, z_lo, z_hi
         self.exclude, self.env_power = exclude, env_power
-        self.fields = unit_fields(geo)
+        self.fields = unit_fields(geo, electrodes)
+        self.n_el = len(self.fields)
+        if coils is not None:
+            self.fields = self.fields + unit_coil_fields(geo, magnetizable or {}, coils)
+        self.n_coils = len(self.fields) - self.n_el
         self.z, self.zt, self.tabs = axial_tables(self.fields, z_lo, z_hi, nz)
 
     def dataset(self, n, seed=0):
@@ -298,14 +367,16 @@ class SurrogateTrainer:
               log_every=0):
         torch = B._torch()
         pts, R = self.dataset(n_samples, seed)
-        n_el = len(self.fields)
-        tmp = SurrogateModel(n_el, self.r_max, self.z_lo, self.z_hi, np.ones(OUT), self.env_power, seed=seed)
+        n_el = len(self.fields)  # field sources: electrodes and coils, 3 outputs each
+        tmp = SurrogateModel(self.n_el, self.r_max, self.z_lo, self.z_hi, np.ones(OUT), self.env_power, seed=seed,
+                             n_coils=self.n_coils)
         env = tmp.envelope(np.hypot(pts[:, 0], pts[:, 1]))
         Y = R / env
         scale = np.ones(OUT, dtype=np.float32)
         scale[:3 * n_el] = np.sqrt(np.mean(Y ** 2, axis=0)) + 1e-300
         T = (Y / scale[:3 * n_el]).astype(np.float32)
-        model = SurrogateModel(n_el, self.r_max, self.z_lo, self.z_hi, scale, self.env_power, seed=seed)
+        model = SurrogateModel(self.n_el, self.r_max, self.z_lo, self.z_hi, scale, self.env_power, seed=seed,
+                               n_coils=self.n_coils)
         n_hold = max(1, int(len(pts) * holdout))
         dev = B.device()
         pts_t = torch.as_tensor(pts, device=dev)
@@ -333,13 +404,17 @@ class SurrogateTrainer:
 
 
 class FieldSurrogate:
-    """A traceable surrogate field for given electrode voltages: the axial
-    series of sum_e V_e (unit table e) plus the network's correction, with the
-    exact BEM field of the same charges as fallback."""
+    """A traceable surrogate field for given source strengths: the axial
+    series of sum_s V_s (unit table s) plus the network's correction, with the
+    exact BEM field of the same charges as fallback.  `strengths` lists the
+    electrode voltages, then (for a model with coils) the coil currents in
+    A-turns; the magnetic part is the axial series of sum_c I_c (coil table c)
+    plus the coils' corrections, its fallback the induced magnetostatic
+    charges and the current rings."""
 
     ENGINES = {'tc': 0, 'warp': 1}
 
-    def __init__(self, model, fields, z, tabs, volts, segments, fallback_dist=50e-6, engine='tc'):
+    def __init__(self, model, fields, z, tabs, strengths, segments, fallback_dist=50e-6, engine='tc'):
         """engine: 'tc' evaluates the network with tcgen05 MMAs (groups of 128
         particles, accumulators in tensor memory); 'warp' with warp-level
         mma.sync (32 particles per warp)."""
@@ -348,19 +423,34 @@ class FieldSurrogate:
             raise ValueError(f'unknown engine {engine!r}; expected one of {sorted(self.ENGINES)}')
         self.engine = engine
         self.model = model
-        self.volts = np.asarray(volts, dtype=np.float64)
-        assert len(self.volts) == model.n_el
+        self.strengths = np.asarray(strengths, dtype=np.float64)
+        assert len(self.strengths) == model.n_src == len(fields) == len(tabs)
+        ne = model.n_el
+        self.volts, self.currents = self.strengths[:ne], self.strengths[ne:]
         self.z = z
         self.zt = B.to_dev(z, torch.float64)
-        self.table = sum(float(v) * t for v, t in zip(self.volts, tabs)).contiguous()
-        bem = fields[0] * float(self.volts[0])
-        for f, v in zip(fields[1:], self.volts[1:]):
+        self.table = sum(float(v) * t for v, t in zip(self.volts, tabs[:ne])).contiguous()
+        self.mag_table = sum(float(c) * t for c, t in zip(self.currents, tabs[ne:])).contiguous() \
+            if model.n_coils else None
+        bem = fields[0] * float(self.strengths[0])
+        for f, v in zip(fields[1:], self.strengths[1:]):
             bem = bem + f * float(v)
         self.bem = bem
         self.sources = bem.electrostatic_point_charges.device_sources()
+        self.mag_sources = bem.magnetostatic_point_charges.device_sources() if model.n_coils else None
+        self.cur_sources = bem.current_point_charges.device_sources() if model.n_coils else None
         self.segments = B.to_dev(np.asarray(segments, dtype=np.float64).reshape(-1, 4), torch.float64)
         self.fallback_dist = float(fallback_dist)
         self.field_bounds = None
+
+    def _tb_field(self):
+        def src(t):
+            return (t.data_ptr() if t is not None and t.numel() else None), (t.shape[1] if t is not None else 0)
+        e, ne = src(self.sources)
+        m, nm = src(self.mag_sources)
+        c, nc = src(self.cur_sources)
+        return B.TbField(e, ne, m, nm, c, nc, None, self.zt.data_ptr(), self.table.data_ptr(),
+                         B._ptr(self.mag_table), len(self.z))
 
     def _descriptor(self):
         m = self.model
@@ -369,8 +459,9 @@ class FieldSurrogate:
         s.params_f32 = m.mlp.p.data_ptr()
         s.r_max, s.z_c, s.z_half, s.z_lo, s.z_hi = m.r_max, m.z_c, m.z_half, m.z_lo, m.z_hi
         s.n_electrodes = m.n_el
-        for i, v in enumerate(self.volts):
-            s.volts[i] = float(v)
+        s.n_coils = m.n_coils
+        for i, v in enumerate(self.strengths):
+            s.strengths[i] = float(v)
         for i, v in enumerate(m.scale):
             s.scale[i] = float(v)
         s.env_power = m.env_power
@@ -378,9 +469,7 @@ class FieldSurrogate:
         s.n_segments = self.segments.shape[0]
         s.fallback_dist = self.fallback_dist
         s.engine = self.ENGINES[self.engine]
-        f = B.TbField(self.sources.data_ptr(), self.sources.shape[1], None, 0, None, 0, None, self.zt.data_ptr(),
-                      self.table.data_ptr(), None, len(self.z))
-        return f, s
+        return self._tb_field(), s
 
     def trace_device(self, start, qm, bounds, atol, plane_z=None, max_attempts=100_000, stream=None):
         torch = B._torch()
@@ -443,6 +532,39 @@ class FieldSurrogate:
         res._keep = (start, qm, work, self)
         return res
 
+    def trace_axial_device(self, start, qm, bounds, atol, plane_z=None, max_attempts=100_000, stream=None):
+        """The same particles through the axial series of this field's
+        coefficient tables alone (FieldRadialAxial's field, radial.c:347-384;
+        the tracer's k_trace_axial), without the network and without the BEM
+        fallback: the method the learned correction improves on.  Returns a
+        TraceResult of device tensors (counters (n, 2))."""
+        from .tracing import TraceResult
+        torch = B._torch()
+        n = start.shape[0]
+        dev = start.device
+        f = B.TbField(None, 0, None, 0, None, 0, None, self.zt.data_ptr(), self.table.data_ptr(),
+                      B._ptr(self.mag_table), len(self.z))
+        o = B.TbTraceOpts()
+        for i, v in enumerate(np.asarray(bounds, dtype=np.float64).reshape(-1)):
+            o.bounds[i] = float(v)
+        o.atol = float(atol)
+        o.plane_z = 0.0 if plane_z is None else float(plane_z)
+        o.record_plane = 0 if plane_z is None else 1
+        o.max_attempts = int(max_attempts)
+        o.max_rows = 0
+        o.team_warps = 0
+        status = torch.empty(n, dtype=torch.int32, device=dev)
+        final = torch.empty((n, 7), dtype=torch.float64, device=dev)
+        plane = torch.empty((n, 7), dtype=torch.float64, device=dev) if plane_z is not None else None
+        counters = torch.empty((n, 2), dtype=torch.int64, device=dev)
+        work = torch.empty(1, dtype=torch.int32, device=dev)
+        B._call('tb_trace_rk45', start.data_ptr(), None, qm.data_ptr(), n, C.byref(f), C.byref(o), None, None,
+                status.data_ptr(), final.data_ptr(), B._ptr(plane), counters.data_ptr(), work.data_ptr(),
+                B._stream() if stream is None else stream)
+        res = TraceResult(status, final, plane, counters)
+        res._keep = (start, qm, work, self)
+        return res
+
     def trace_endpoints(self, position, velocity, bounds, plane_z, mass=None, charge=None, atol=1e-8,
                         max_attempts=100_000):
         """Batched endpoint tracing with host arrays in and out (the public
@@ -465,19 +587,23 @@ class FieldSurrogate:
         """A TraceSession for repeated batches of n particles (see there)."""
         return TraceSession(self, n, bounds, plane_z, mass, charge, atol, max_attempts)
 
-    def kernel_field_at_points(self, points):
+    def kernel_field_at_points(self, points, magnetic=False):
         """Surrogate E at points (M, 3) as the tracer's kernel evaluates it
-        (electrode fallback included); returns (E, used_bem)."""
+        (electrode fallback included); returns (E, used_bem), or with
+        magnetic=True (E, H, used_bem)."""
         torch = B._torch()
         pts = B.to_dev(np.asarray(points, dtype=np.float64).reshape(-1, 3), torch.float64)
         M = pts.shape[0]
         out = torch.empty((M, 3), dtype=torch.float64, device=pts.device)
+        out_h = torch.empty((M, 3), dtype=torch.float64, device=pts.device) if magnetic else None
         ub = torch.empty(M, dtype=torch.int32, device=pts.device)
         f, s = self._descriptor()
-        r = _lib.tb_surrogate_field_points(pts.data_ptr(), M, C.byref(f), C.byref(s), out.data_ptr(), ub.data_ptr(),
-                                           B._stream())
+        r = _lib.tb_surrogate_field_points(pts.data_ptr(), M, C.byref(f), C.byref(s), out.data_ptr(),
+                                           B._ptr(out_h), ub.data_ptr(), B._stream())
         if r != B.TB_OK:
             raise B.BackendError(f'tb_surrogate_field_points failed with status {r}')
+        if magnetic:
+            return out.cpu().numpy(), out_h.cpu().numpy(), ub.cpu().numpy()
         return out.cpu().numpy(), ub.cpu().numpy()
 
     def field_at_points(self, points):
@@ -486,7 +612,7 @@ class FieldSurrogate:
         pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
         _, fa = B.dev_axial_field_points(B.to_dev(pts, torch.float64), self.zt, self.table)
         E = fa.cpu().numpy()
-        corr = self.model.predict_residual(pts)  # (M, n_el, 3)
+        corr = self.model.predict_residual(pts)[:, :self.model.n_el]  # (M, n_el, 3): the electrodes
         r = np.hypot(pts[:, 0], pts[:, 1])
         er = np.einsum('e,me->m', self.volts, corr[:, :, 1])
         ez = np.einsum('e,me->m', self.volts, corr[:, :, 2])
@@ -502,7 +628,8 @@ class FieldSurrogate:
 _tb_trace_surrogate_args = [_vp, _vp, _vp, _i64, C.POINTER(B.TbField), C.POINTER(TbSurrogate),
                             C.POINTER(B.TbTraceOpts), _vp, _vp, _vp, _vp, _vp, _vp]
 _lib.tb_trace_surrogate.argtypes = _tb_trace_surrogate_args
-_lib.tb_surrogate_field_points.argtypes = [_vp, _i64, C.POINTER(B.TbField), C.POINTER(TbSurrogate), _vp, _vp, _vp]
+_lib.tb_surrogate_field_points.argtypes = [_vp, _i64, C.POINTER(B.TbField), C.POINTER(TbSurrogate), _vp, _vp, _vp,
+                                           _vp]
 _lib.tb_surrogate_field_points.restype = C.c_int
 _lib.tb_trace_surrogate.restype = C.c_int
 
