@@ -3,28 +3,35 @@ the einzel-lens workload, learned surrogate vs plain BEM field.
 
 Workload: the three-tube einzel lens of 1,000 cubic line elements graded
 toward the tube edges (0 V / V_mid / 0 V, V_mid from the seed), solved once on
-the GPU (FP64 fill, singular self terms, FP64 LU).  A step traces a batch of
-electrons (default 262,144) at 1 keV +-5 %, angles +-20 mrad, start radius
-<= 0.2 mm at z = -9.5 mm, with adaptive RKF45 at atol = 1e-10 m until they
-leave the bounds (|x|,|y| <= 2 mm, |z| <= 10 mm), recording each electron's
-crossing of the exit plane z = +9.5 mm.  Synthetic inputs; no dataset.
+the GPU.  A step traces a batch of electrons (default 262,144) at 1 keV +-5 %,
+angles +-20 mrad, start radius up to the beam's r_max at z = -9.5 mm, with
+adaptive RKF45 at atol = 1e-10 m until they leave the bounds (|x|,|y| <= 2 mm,
+|z| <= 10 mm), recording each electron's crossing of the exit plane
+z = +9.5 mm.  Two beams: `wide` (r0 <= 0.6 mm, the headline: the axial series
+alone misses 1 nm there, the learned correction holds it) and `narrow`
+(r0 <= 0.2 mm, the plain-method workload's beam).  Synthetic inputs; no
+dataset.
 
-  --field surrogate (default): the surrogate field (axial series + BF16 MLP
-      correction trained on the GPU from BEM samples in the setup phase, BEM
-      fallback near electrodes); the plain BEM tracer is measured beside it
-      on a 16,384-electron slice of the same beam (`plain_bem`).
+On each beam three arms: the surrogate (axial series + BF16 MLP correction
+trained on the GPU from BEM samples in the setup phase, BEM fallback near
+electrodes), the axial series alone (the same table, no network), and the
+plain FP64 BEM tracer on a 16,384-electron slice.  Endpoint errors of the
+surrogate and of the axial series against the CPU oracle on a held-out
+sample of each beam (1 % of the headline beam), traced in spawned processes
+while the GPU works; CPU baselines: the reference C backend's plain-BEM
+tracer and its axial-series tracer on all host threads.
+
   --field bem: the plain FP64 BEM field only.
   --impl reference: the reference C backend's plain BEM tracer on host cores.
   --workload solve: only the precision workload's solve (the lens at
       --precision-n elements, 8 right-hand sides): GPU FP64 fill, FP64
       pivoted LU and the mixed tensor-core solve (also reported, as
       `precision_solve`, beside the tracer in the default run).
+  --workload combined: the combined electro-magnetostatic workload.
 
 `value` is whole-job electrons/s with the start states resident in HBM;
 `e2e` is the same through the public API with host arrays over a stream of
-batches (two in flight), host<->device copies inside the timed region.  Endpoints of a sample of electrons are
-checked every run against the full CPU oracle (oracle charges, FP64 BEM
-trace): `accuracy.endpoint_err_max_nm` must stay <= 1.
+batches (two in flight), host<->device copies inside the timed region.
 """
 from __future__ import annotations
 
@@ -47,14 +54,23 @@ SEED = 1
 ATOL = 1e-10
 METRIC = 'traced electrons/s at <=1 nm endpoint error, surrogate vs plain BEM field'
 
+# Start-radius range of the two beams (1 keV +-5 %, +-20 mrad, z0 = -9.5 mm).
+# narrow: the plain-method workload's r0 <= 0.2 mm, where the axial series
+# alone already traces within 1 nm.  wide: start radii out to where the axial
+# series alone misses 1 nm and the learned correction is what holds it.
+BEAMS = {'narrow': {'r_max': 0.2e-3}, 'wide': {'r_max': 0.6e-3}}
 
-def workload_config(electrons, field):
+
+def workload_config(electrons, field, beam):
     desc = {'surrogate': 'learned surrogate field (axial series + BF16 MLP correction, BEM fallback)',
             'bem': 'plain BEM field (FP64)'}[field]
+    r_mm = BEAMS[beam]['r_max'] * 1e3
     return {'workload': f'einzel lens, {N_ELEMENTS} cubic elements, {desc}, {electrons} electrons/step at '
-                        f'1 keV +-5%, +-20 mrad, r0<=0.2 mm, RKF45 atol=1e-10 m, exit plane z=+9.5 mm',
+                        f'1 keV +-5%, +-20 mrad, r0<={r_mm:g} mm ({beam} beam), RKF45 atol=1e-10 m, '
+                        f'exit plane z=+9.5 mm',
             'elements': N_ELEMENTS, 'electrons_per_step': electrons, 'atol_m': ATOL, 'seed': SEED,
-            'field': field, 'l2': 'L2 flushed (256 MiB write, inside the step time) before every timed step'}
+            'field': field, 'beam': beam, 'beam_r0_max_m': BEAMS[beam]['r_max'],
+            'l2': 'L2 flushed (256 MiB write, inside the step time) before every timed step'}
 
 
 def dist_info():
@@ -115,11 +131,13 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- workload
-def lens_inputs(electrons, seed=SEED):
+def lens_inputs(electrons, beam='wide', seed=SEED):
+    """The lens (1,000 elements), its voltages and `electrons` start states
+    of the named beam."""
     from traceon_b200 import geometry as G
     geo = G.einzel_lens(N_ELEMENTS)
     volts = G.einzel_lens_voltages(SEED)
-    p0, v0 = G.surrogate_beam(electrons, seed + 100)
+    p0, v0 = G.surrogate_beam(electrons, seed + 100, r_max=BEAMS[beam]['r_max'])
     return geo, volts, p0, v0
 
 
@@ -134,28 +152,68 @@ def oracle_charges(geo, volts, threads):
     return q, jac, pos
 
 
-def check_endpoints(plane_gpu, p0, v0, q, jac, pos, sample, threads):
-    """Max |(x, y)| difference (nm) at the exit plane between the GPU and the
-    CPU oracle (both cubic-Hermite crossings) on `sample` electrons."""
-    from oracle.oracle import Oracle, EM, hermite_plane_crossing
+# The CPU judge of endpoints: the oracle's FP64 BEM trace of each checked
+# electron and its cubic-Hermite crossing of the exit plane, in a pool of
+# spawned processes (no CUDA in them) that runs while the GPU work proceeds.
+_JUDGE = {}
+
+
+def _judge_init(q, jac, pos):
+    try:
+        os.nice(10)  # below the bench's own host thread
+    except OSError:
+        pass
+    from oracle.oracle import Oracle
+    _JUDGE.update(oracle=Oracle('port'), q=q, jac=jac, pos=pos)
+
+
+def _judge_one(state):
+    from oracle.oracle import EM, hermite_plane_crossing
     from traceon_b200 import geometry as G
-    from concurrent.futures import ThreadPoolExecutor
-    port = Oracle('port')
-
-    def one(i):
-        t, s = port.trace_bem(p0[i], v0[i], EM, q, jac, pos, G.LENS_BOUNDS, ATOL)
-        h = hermite_plane_crossing(t, s, G.LENS_EXIT_Z)
-        return np.max(np.abs(plane_gpu[i, 1:3] - h[:2]))
-
-    with ThreadPoolExecutor(threads) as ex:
-        errs = list(ex.map(one, sample))
-    return float(max(errs)) * 1e9, float(np.percentile(errs, 99)) * 1e9
+    t, s = _JUDGE['oracle'].trace_bem(state[:3], state[3:], EM, _JUDGE['q'], _JUDGE['jac'], _JUDGE['pos'],
+                                      G.LENS_BOUNDS, ATOL)
+    h = hermite_plane_crossing(t, s, G.LENS_EXIT_Z)
+    return (np.nan, np.nan) if h is None else (float(h[0]), float(h[1]))
 
 
-def cpu_reference_rate(geo, q, jac, pos, p0, v0, threads, seconds, kind='ref'):
+class OracleJudge:
+    """Exit-plane crossings of electrons traced by the CPU oracle, computed
+    asynchronously in `workers` spawned processes."""
+
+    def __init__(self, q, jac, pos, workers):
+        import multiprocessing as mp
+        self.workers = workers
+        self.pool = mp.get_context('spawn').Pool(workers, _judge_init, (q, jac, pos))
+        self.jobs = {}
+        self.t0 = time.perf_counter()
+
+    def submit(self, name, p0, v0):
+        states = [np.concatenate([a, b]) for a, b in zip(p0, v0)]
+        self.jobs[name] = self.pool.map_async(_judge_one, states, chunksize=4)
+
+    def result(self, name):
+        return np.array(self.jobs[name].get(), dtype=np.float64).reshape(-1, 2)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+        return time.perf_counter() - self.t0
+
+
+def endpoint_errors_nm(plane, ref_xy):
+    """Max and p99 over electrons of max(|dx|, |dy|) at the exit plane, nm;
+    electrons without a crossing on either side count as infinite."""
+    d = np.max(np.abs(plane[:, 1:3] - ref_xy), axis=1) * 1e9
+    d = np.where(np.isfinite(d), d, np.inf)
+    return {'max_nm': float(np.max(d)), 'p99_nm': float(np.percentile(d, 99)), 'n': int(len(d)),
+            'within_1nm': int(np.sum(d <= 1.0))}
+
+
+def cpu_reference_rate(q, jac, pos, p0, v0, threads, seconds, kind='ref', axial=None):
     """The reference's own CPU tracer (oracle/_ref: trace_particle with its
-    field_radial_traceable callback) on `threads` host threads for about
-    `seconds`; returns (electrons/s, electrons traced)."""
+    field_radial_traceable callback, or with field_radial_derivs_traceable
+    when `axial` = (z, coefficients) is given) on `threads` host threads for
+    about `seconds`; returns (electrons/s, electrons traced, kind)."""
     from oracle.oracle import Oracle, EM, available
     from traceon_b200 import geometry as G
     if kind == 'ref' and not available('ref'):
@@ -165,6 +223,7 @@ def cpu_reference_rate(geo, q, jac, pos, p0, v0, threads, seconds, kind='ref'):
     lock = threading.Lock()
     stop = time.perf_counter() + seconds
     counter = iter(range(len(p0)))
+    zero_mag = None if axial is None else np.zeros_like(axial[1])
 
     def worker():
         while time.perf_counter() < stop:
@@ -172,7 +231,10 @@ def cpu_reference_rate(geo, q, jac, pos, p0, v0, threads, seconds, kind='ref'):
                 i = next(counter, None)
             if i is None:
                 return
-            o.trace_bem(p0[i], v0[i], EM, q, jac, pos, G.LENS_BOUNDS, ATOL)
+            if axial is None:
+                o.trace_bem(p0[i], v0[i], EM, q, jac, pos, G.LENS_BOUNDS, ATOL)
+            else:
+                o.trace_axial(p0[i], v0[i], EM, axial[0], axial[1], zero_mag, G.LENS_BOUNDS, ATOL)
             with lock:
                 done.append(i)
 
@@ -184,6 +246,15 @@ def cpu_reference_rate(geo, q, jac, pos, p0, v0, threads, seconds, kind='ref'):
         t.join()
     el = time.perf_counter() - t0
     return len(done) / el, len(done), kind
+
+
+def reference_axial_table(q, jac, pos, z):
+    """The reference's FieldRadialAxial table of the oracle charges on the
+    grid z: its C axial-derivative sums (oracle/_ref) and its SciPy spline
+    coefficients (traceon/field.py:971-991)."""
+    from oracle.oracle import Oracle, available, axial_coefficients
+    o = Oracle('ref' if available('ref') else 'port')
+    return axial_coefficients(z, o.axial_derivatives_radial(z, q, jac, pos))
 
 
 def host_cores():
@@ -199,16 +270,16 @@ def run_reference(args):
     if rank != 0:
         return
     cores = host_cores()
-    geo, volts, p0, v0 = lens_inputs(4096)
+    geo, volts, p0, v0 = lens_inputs(4096, args.beam)
     q, jac, pos = oracle_charges(geo, volts, cores)
     for _ in range(args.warmup):
-        cpu_reference_rate(geo, q, jac, pos, p0, v0, cores, 2.0)
+        cpu_reference_rate(q, jac, pos, p0, v0, cores, 2.0)
     rates, n_total, t_total = [], 0, 0.0
     # each step a bounded sample: about two minutes of CPU work in total
     step_s = min(args.ref_seconds, max(2.0, 120.0 / max(args.steps, 1)))
     for s in range(args.steps):
         sl = slice((s * cores * 4) % len(p0), None)
-        r, n, kind = cpu_reference_rate(geo, q, jac, pos, p0[sl], v0[sl], cores, step_s)
+        r, n, kind = cpu_reference_rate(q, jac, pos, p0[sl], v0[sl], cores, step_s)
         rates.append(r)
         n_total += n
         t_total += n / r if r else 0
@@ -216,11 +287,11 @@ def run_reference(args):
     line = {'metric': METRIC, 'value': value, 'unit': 'electrons/s', 'n_gpus': ws, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': 1e3 * t_total / max(args.steps, 1), 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic', 'impl': 'reference',
-            'config': workload_config(args.electrons, args.field),
+            'config': workload_config(args.electrons, args.field, args.beam),
             'reference_field': 'plain BEM (the reference has no learned surrogate)',
             'cpu_baseline': {'value': value, 'unit': 'electrons/s', 'cores': cores,
                              'kind': 'reference' if kind == 'ref' else 'port',
-                             'sample': f'{n_total} electrons over {args.steps} steps of ~{step_s:.0f} s '
+                             'sample': f'{n_total} electrons of this beam over {args.steps} steps of ~{step_s:.0f} s '
                                        f'(reference C backend trace_particle + field_radial_traceable, '
                                        f'{cores} threads)'},
             'e2e': {'value': value, 'unit': 'electrons/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
@@ -228,13 +299,20 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- precision solve
-def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True):
+def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True, fp64_peak=None, check=4096):
     """The precision workload's charge solve: the three-electrode lens meshed
     to n cubic elements, nrhs right-hand sides with every electrode voltage
     ~U[-3, 3] kV.  GPU FP64 fill (+ singular self terms), then (a) the FP64
     LU with partial pivoting (numpy.linalg.solve's factorisation) and (b) the
     mixed solve (FP32 tensor-core LU of the equilibrated matrix, FP64
-    iterative refinement).  CUDA-event times; charges of (b) against (a)."""
+    iterative refinement).  CUDA-event times; charges of (b) against (a).
+    Then potential and field of the first right-hand side's charges at
+    `field_points` points, and the axial derivatives of the same charges on
+    2,000 z-points; FP64 rooflines of the fill, field and axial kernels
+    against `fp64_peak` (TFLOP/s) with the algorithmic flop counts of their
+    formulas.  `check` points of the field are re-evaluated by the CPU oracle
+    here (check = 0: the caller runs precision_field_check later on
+    out['_field_state'])."""
     import torch
     from traceon_b200 import backend as B
     from traceon_b200.geometry import einzel_lens
@@ -253,14 +331,18 @@ def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True):
     t = B.to_dev(np.ones(n, np.uint8), torch.uint8)
     val = B.to_dev(np.zeros(n), torch.float64)
     A = torch.empty((n, n), dtype=torch.float64, device='cuda')
+    jac, pos = B.dev_jacobian_buffer(v)
 
-    def fill():
-        jac, pos = B.dev_jacobian_buffer(v)
+    def fill_offdiag():
         B.dev_fill_matrix(A, v, t, val, jac, pos)
+
+    def self_terms():
         B.dev_self_integrals(v, t, val, A)
 
-    fill()  # warm-up
-    fill_ms, _ = timed(fill)
+    fill_offdiag()
+    self_terms()  # warm-up
+    fill_ms, _ = timed(fill_offdiag)
+    self_ms, _ = timed(self_terms)
     rng = np.random.default_rng(seed)
     F = torch.as_tensor(geo.voltages_to_values(rng.uniform(-3000, 3000, (nrhs, 3)).T).T.copy(), device='cuda')
 
@@ -282,29 +364,48 @@ def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True):
         lib_ms, _ = timed(lambda: torch.linalg.solve(A, F.T))
     else:  # profiling the mixed solve alone
         lu_ms, err = None, None
+    fill_ms_total = fill_ms + self_ms
     out = {'workload': f'einzel lens, {n} cubic elements, {nrhs} right-hand sides (electrode voltages U[-3,3] kV)',
-           'fill_fp64_ms': fill_ms, 'solve_fp64_lu_ms': lu_ms, 'solve_mixed_ms': mixed_ms,
+           'fill_fp64_ms': fill_ms_total, 'fill_offdiagonal_ms': fill_ms, 'self_integrals_ms': self_ms,
+           'solve_fp64_lu_ms': lu_ms, 'solve_mixed_ms': mixed_ms,
            'mixed_iterations': iters, 'mixed_last_correction': rel, 'charges_rel_err_vs_fp64': err,
            'solve_fp64_vendor_lu_ms': lib_ms,
            'speedup_vs_vendor_fp64_lu': lib_ms / mixed_ms if lib_ms else None,
            'speedup_solve': lu_ms / mixed_ms if lu_ms else None,
-           'speedup_fill_plus_solve': (fill_ms + lu_ms) / (fill_ms + mixed_ms) if lu_ms else None,
+           'speedup_fill_plus_solve': (fill_ms_total + lu_ms) / (fill_ms_total + mixed_ms) if lu_ms else None,
+           'fill_plus_mixed_solve_ms': fill_ms_total + mixed_ms,
+           'speedup_fill_plus_solve_vs_vendor': (fill_ms_total + lib_ms) / (fill_ms_total + mixed_ms)
+           if lib_ms else None,
            'lu_flop': 2.0 / 3.0 * n ** 3}
+    # fill roofline: N^2 entries x 16 ring potentials (the diagonal's Gauss
+    # terms are computed and overwritten, as in the reference)
+    pots = float(n) * n * 16
+    out['fill_roofline'] = fp64_roofline(pots, FLOP_RING_POT, fill_ms, fp64_peak, 'k_fill_matrix',
+                                         'ring-potential evaluations (+ 1 log, 1 rsqrt each)')
     del A
     torch.cuda.empty_cache()
     if field_points:
-        out.update(precision_fields(geo, Xm[0], field_points, seed))
+        out.update(precision_fields(geo, Xm[0], field_points, seed, fp64_peak))
+        if check:
+            out.update(precision_field_check(out.pop('_field_state'), check, host_cores()))
+    out.update(axial_roofline(geo, Xm[0], fp64_peak))
     return out
 
 
-def precision_fields(geo, charges_t, m, seed, check=64):
-    """Potential and field of the first right-hand side's charges at m points
-    (x = r ~ U[0, 0.9] mm, y = 0, z ~ U[-8, 8] mm), FP64 ring sums on the GPU;
-    `check` of them re-evaluated by the CPU oracle (its own element
-    quadrature and the same charges) as the check."""
+def fp64_roofline(units, flop_per_unit, ms, peak, kernel, unit_desc):
+    achieved = units * flop_per_unit / (ms * 1e-3) / 1e12
+    return {'bound': 'fp64', 'kernel': kernel, 'units': units, 'flop_per_unit': flop_per_unit,
+            'unit_desc': unit_desc, 'achieved': achieved, 'unit': 'TFLOP/s', 'peak': peak,
+            'frac': achieved / peak if peak else None,
+            'peak_source': 'FP64 FMA throughput measured in this run (tests/probe tb_probe_fp64_fma)'}
+
+
+def precision_fields(geo, charges_t, m, seed, fp64_peak=None):
+    """Potential and field of the charges at m points (x = r ~ U[0, 0.9] mm,
+    y = 0, z ~ U[-8, 8] mm), FP64 ring sums on the GPU; the inputs and
+    outputs are kept in '_field_state' for precision_field_check."""
     import torch
     from traceon_b200 import backend as B
-    from oracle.oracle import Oracle
     rng = np.random.default_rng(seed + 1)
     pts = np.zeros((m, 3))
     pts[:, 0] = rng.uniform(0.0, 0.9e-3, m)
@@ -321,18 +422,55 @@ def precision_fields(geo, charges_t, m, seed, check=64):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    sample = rng.choice(m, check, replace=False)
+    pairs = float(m) * src.shape[1]
+    return {'field_points': m, 'field_ms': ms, 'field_ring_pairs_per_s': pairs / (ms * 1e-3),
+            'field_roofline': fp64_roofline(pairs, FLOP_FIELD_PAIR_POT, ms, fp64_peak, 'k_field_points',
+                                            'ring-pair potential + field evaluations (+ 1 log, 1 rsqrt, '
+                                            '1 reciprocal each)'),
+            '_field_state': (geo.vertices, charges_t.cpu().numpy(), pts, pot.cpu().numpy(), fld.cpu().numpy(), seed)}
+
+
+def precision_field_check(state, check, threads):
+    """`check` of the field points re-evaluated by the CPU oracle (its own
+    element quadrature and the same charges) on `threads` host threads."""
+    from oracle.oracle import Oracle
+    vertices, q, pts, pot, fld, seed = state
+    rng = np.random.default_rng(seed + 2)
+    sample = rng.choice(len(pts), min(check, len(pts)), replace=False)
     port = Oracle('port')
-    q = charges_t.cpu().numpy()
-    jac_o, pos_o = port.fill_jacobian_buffer_radial(geo.vertices)
-    f_or = port.field_radial_many(pts[sample], q, jac_o, pos_o)
-    p_or = port.potential_radial_many(pts[sample], q, jac_o, pos_o)
-    f_gpu, p_gpu = fld.cpu().numpy()[sample], pot.cpu().numpy()[sample]
+    jac_o, pos_o = port.fill_jacobian_buffer_radial(vertices)
+    t0 = time.perf_counter()
+    f_or = port.field_radial_many(pts[sample], q, jac_o, pos_o, threads=threads)
+    p_or = port.potential_radial_many(pts[sample], q, jac_o, pos_o, threads=threads)
+    f_gpu, p_gpu = fld[sample], pot[sample]
+    # relative to the largest value of the sample (E_r vanishes on the axis)
     ferr = float(np.max(np.abs(f_gpu - f_or)) / np.max(np.abs(f_or)))
     perr = float(np.max(np.abs(p_gpu - p_or)) / np.max(np.abs(p_or)))
-    pairs = m * src.shape[1]
-    return {'field_points': m, 'field_ms': ms, 'field_ring_pairs_per_s': pairs / (ms * 1e-3),
-            'field_rel_err_vs_oracle': ferr, 'potential_rel_err_vs_oracle': perr, 'field_checked_points': check}
+    return {'field_rel_err_vs_oracle': ferr, 'potential_rel_err_vs_oracle': perr, 'field_checked_points': len(sample),
+            'field_check_s': time.perf_counter() - t0}
+
+
+def axial_roofline(geo, charges_t, fp64_peak, nz=2000):
+    """Axial derivatives (9 per z) of the charges on nz z-points over the
+    lens: nz x 16 N ring recurrences."""
+    import torch
+    from traceon_b200 import backend as B
+    v = B.to_dev(geo.vertices, torch.float64)
+    jac, pos = B.dev_jacobian_buffer(v)
+    src = B.dev_pack_sources(charges_t.contiguous(), jac, pos)
+    z = B.to_dev(np.linspace(-9.95e-3, 9.95e-3, nz), torch.float64)
+    B.dev_axial_derivatives(z, src)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    B.dev_axial_derivatives(z, src)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    units = float(nz) * src.shape[1]
+    return {'axial_ms': ms, 'axial_z_points': nz,
+            'axial_roofline': fp64_roofline(units, FLOP_AXIAL_RING, ms, fp64_peak, 'k_axial_derivs',
+                                            'ring recurrences of 9 axial derivatives (+ 1 sqrt, 2 divisions each)')}
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -377,7 +515,18 @@ def read_peaks():
         return {}
 
 
-MLP_FLOP_PER_EVAL = 2 * (16 * 128 + 3 * 128 * 128 + 128 * 16)  # dense BF16 flops of one network evaluation
+MLP_FLOP_PER_EVAL = 2 * (16 * 128 + 3 * 128 * 128 + 128 * 32)  # dense BF16 flops of one network evaluation
+# Algorithmic FP64 flops of one ring pair, counted on the formulas (FMA = 2;
+# the Cody polynomials of K and E: 4 polynomials of degree 7, 14 flops each;
+# the transcendental steps listed separately):
+#   field pair (E_r, E_z sums):           87 flops + 1 log + 1 rsqrt + 1 reciprocal
+#   potential + field pair:               90 flops + the same
+#   ring potential term of the fill:      46 flops + 1 log + 1 rsqrt
+#   axial derivative recurrence (9 terms): 54 flops + 1 sqrt + 2 divisions
+FLOP_FIELD_PAIR = 87
+FLOP_FIELD_PAIR_POT = 90
+FLOP_RING_POT = 46
+FLOP_AXIAL_RING = 54
 FALLBACK_BF16_TFLOPS = 1590.0  # dense bf16 burst of a cuBLAS GEMM on this pool's B200s, used without MEASURED_PEAKS.json
 
 
@@ -403,9 +552,37 @@ def time_steps(fn, steps, flush):
     return ms, results
 
 
+def timed_launches(fn, steps, flush):
+    """Device time (ms) of each of `steps` calls of fn, each after an L2
+    flush, with one untimed call first; returns (ms list, last result)."""
+    fn()
+    ms, res = time_steps(fn, steps, flush)
+    return ms, res[-1]
+
+
 def run_gpu(args):
     import torch
     ws, rank, local = dist_info()
+    cores = host_cores()
+    E = args.electrons
+    beam = args.beam
+    other = 'narrow' if beam == 'wide' else 'wide'
+    geo, volts, p0, v0 = lens_inputs(E, beam, SEED + rank)
+    _, _, p0o, v0o = lens_inputs(E, other, SEED + rank + 1000)
+    # ---- the CPU judge starts first and overlaps the GPU work (rank 0)
+    judge = None
+    n_check = min(args.check, E) if rank == 0 else 0
+    n_check_o = min(args.check_other, E) if rank == 0 else 0
+    t_or = time.perf_counter()
+    q_or = jac_or = pos_or = None
+    if n_check or n_check_o or (ws == 1 and args.cpu_seconds > 0):
+        q_or, jac_or, pos_or = oracle_charges(geo, volts, cores)
+    if n_check or n_check_o:
+        judge = OracleJudge(q_or, jac_or, pos_or, max(1, cores - 1))
+        judge.submit(beam, p0[:n_check], v0[:n_check])
+        judge.submit(other, p0o[:n_check_o], v0o[:n_check_o])
+    oracle_setup_s = time.perf_counter() - t_or
+
     torch.cuda.set_device(local)
     if ws > 1:
         import torch.distributed as dist
@@ -418,8 +595,6 @@ def run_gpu(args):
     from traceon_b200.tracing import Tracer
     from scipy.constants import e as qe, m_e
 
-    E = args.electrons
-    geo, volts, p0, v0 = lens_inputs(E, SEED + rank)
     # ---- setup (timed separately, not part of a step): GPU solve
     exc = Excitation(Mesh.from_geometry(geo))
     exc.add_voltage(**{n: float(v) for n, v in zip(geo.names, volts)})
@@ -427,7 +602,7 @@ def run_gpu(args):
     t0 = time.perf_counter()
     field = ElectrostaticSolverRadial(exc).solve_matrix()[0]
     torch.cuda.synchronize()
-    setup = {'solve_s': time.perf_counter() - t0}
+    setup = {'solve_s': time.perf_counter() - t0, 'oracle_charges_s': oracle_setup_s}
     bem_tracer = Tracer(field, G.LENS_BOUNDS)
     Nq = len(field.electrostatic_point_charges) * B.N_QUAD_2D
     sur = None
@@ -439,28 +614,34 @@ def run_gpu(args):
         torch.cuda.synchronize()
         setup['surrogate_train_s'] = time.perf_counter() - t0
         setup['surrogate_holdout_mse'] = info['holdout_mse']
-        setup['surrogate_train'] = f'{args.train_samples} BEM samples, {args.train_steps} Adam steps of 8192'
+        setup['surrogate_train'] = (f'{args.train_samples} BEM samples of the unit-voltage fields, '
+                                    f'{args.train_steps} Adam steps of 8192 (one network for every voltage setting '
+                                    f'of this lens)')
         sur = FieldSurrogate(model, trainer.fields, trainer.z, trainer.tabs, volts, geo.segments, engine=args.engine)
 
-    start = torch.as_tensor(np.concatenate([p0, v0], 1), device='cuda', dtype=torch.float64).contiguous()
+    def start_of(p, v):
+        return torch.as_tensor(np.concatenate([p, v], 1), device='cuda', dtype=torch.float64).contiguous()
+
+    start, start_o = start_of(p0, v0), start_of(p0o, v0o)
     qm = torch.full((E,), -qe / m_e, device='cuda', dtype=torch.float64)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device='cuda')
+    MAXA = 20000
 
-    def step_bem(st=start, q=qm):
+    def step_bem(st, q=qm):
         return bem_tracer.trace_device(st, q, atol=ATOL, plane_z=G.LENS_EXIT_Z, team_warps=args.team_warps,
-                                       max_attempts=20000)
+                                       max_attempts=MAXA)
 
     sess = None
     if sur is not None:
         # the public batched API: static buffers, the step captured as a CUDA graph
-        sess = sur.trace_session(E, G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=ATOL, max_attempts=20000)
+        sess = sur.trace_session(E, G.LENS_BOUNDS, G.LENS_EXIT_Z, atol=ATOL, max_attempts=MAXA)
         sess.start.copy_(start)  # start states resident in HBM for `value`
 
     def step_sur():
         sess.replay_device()
         return sess
 
-    step = step_sur if sur is not None else step_bem
+    step = step_sur if sur is not None else (lambda: step_bem(start))
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -478,8 +659,7 @@ def run_gpu(args):
     status = res.status.cpu().numpy()
     plane = res.plane.cpu().numpy()
     counters = res.counters.cpu().numpy()
-    attempts = [int(counters[:, 1].sum())] * args.steps if sess is not None else \
-        [int(r.counters[:, 1].sum().item()) for r in results]
+    attempts = float(counters[:, 1].sum())
     value = ws * E * args.steps / (total_ms * 1e-3)
 
     # ---- e2e through the public API with host arrays: every step copies the
@@ -509,29 +689,65 @@ def run_gpu(args):
             torch.cuda.synchronize()
             t1 = time.perf_counter()
             bem_tracer.trace_endpoints(p0, v0, G.LENS_EXIT_Z, atol=ATOL, team_warps=args.team_warps,
-                                       max_attempts=20000)
+                                       max_attempts=MAXA)
             torch.cuda.synchronize()
             e2e_ms.append((time.perf_counter() - t1) * 1e3)
         h2d, d2h = E * 6 * 8 + E * 8, E * (7 + 7) * 8 + E * 4 + E * 2 * 8
         e2e_api = 'Tracer.trace_endpoints(positions, velocities, ...)'
     e2e_value = ws * E / (np.median(e2e_ms) * 1e-3)
 
-
-    # ---- plain BEM tracer on a slice of the same beam (for the comparison)
-    plain = None
+    # ---- the arms on both beams: surrogate, axial series alone, plain BEM
+    # (a 16,384-electron slice); their exit-plane crossings for the errors
+    arms = {}
     if sur is not None:
         m = min(E, args.bem_electrons)
-        st_m, qm_m = start[:m].contiguous(), qm[:m].contiguous()
-        step_bem(st_m, qm_m)
-        ms_b, res_b = time_steps(lambda: step_bem(st_m, qm_m), 2, flush)
-        pairs = np.mean([int(r.counters[:, 1].sum().item()) for r in res_b]) * 6 * Nq
-        launch_s = np.mean(ms_b) * 1e-3
-        plain = {'value': ws * m / launch_s, 'unit': 'electrons/s', 'electrons': m,
-                 'ms_per_step': float(np.mean(ms_b)),
-                 'roofline': {'bound': 'fp64', 'achieved': pairs * args.flop_per_pair / launch_s / 1e12,
-                              'unit': 'TFLOP/s', 'kernel': 'k_trace_bem', 'flop_per_pair': args.flop_per_pair}}
+        for name, st, pl_sur in ((beam, start, plane), (other, start_o, None)):
+            row = {}
+            if pl_sur is None:
+                ms_s, r_s = timed_launches(
+                    lambda: sur.trace_device(st, qm, G.LENS_BOUNDS, ATOL, plane_z=G.LENS_EXIT_Z, max_attempts=MAXA),
+                    3, flush)
+                pl_sur = r_s.plane.cpu().numpy()
+                row['surrogate'] = {'value': E / (np.mean(ms_s) * 1e-3), 'ms_per_step': float(np.mean(ms_s)),
+                                    'attempts_mean': float(r_s.counters[:, 1].double().mean()),
+                                    'bem_fallback_evals': int(r_s.counters[:, 2].sum().item()),
+                                    'status_exited': int((r_s.status == 0).sum().item())}
+            else:
+                row['surrogate'] = {'value': value, 'ms_per_step': total_ms / args.steps,
+                                    'attempts_mean': attempts / E,
+                                    'bem_fallback_evals': int(counters[:, 2].sum()),
+                                    'status_exited': int((status == 0).sum())}
+            ms_a, r_a = timed_launches(
+                lambda: sur.trace_axial_device(st, qm, G.LENS_BOUNDS, ATOL, plane_z=G.LENS_EXIT_Z,
+                                               max_attempts=MAXA), 3, flush)
+            pl_ax = r_a.plane.cpu().numpy()
+            row['axial_only'] = {'value': E / (np.mean(ms_a) * 1e-3), 'ms_per_step': float(np.mean(ms_a)),
+                                 'attempts_mean': float(r_a.counters[:, 1].double().mean()),
+                                 'status_exited': int((r_a.status == 0).sum().item()),
+                                 'kernel': 'k_trace_axial'}
+            st_m, qm_m = st[:m].contiguous(), qm[:m].contiguous()
+            ms_b, r_b = timed_launches(lambda: step_bem(st_m, qm_m), 2, flush)
+            pl_bem = r_b.plane.cpu().numpy()
+            pairs = float(r_b.counters[:, 1].sum().item()) * 6 * Nq
+            launch_s = np.mean(ms_b) * 1e-3
+            row['plain_bem'] = {'value': ws * m / launch_s, 'electrons': m, 'ms_per_step': float(np.mean(ms_b)),
+                                'kernel': 'k_trace_bem',
+                                'roofline': {'bound': 'fp64', 'unit': 'TFLOP/s', 'flop_per_pair': FLOP_FIELD_PAIR,
+                                             'achieved': pairs * FLOP_FIELD_PAIR / launch_s / 1e12,
+                                             'unit_desc': 'ring-pair field evaluations, algorithmic FP64 flops '
+                                                          '(+ 1 log, 1 rsqrt, 1 reciprocal per pair)'}}
+            row['speedup_surrogate_vs_plain_bem'] = row['surrogate']['value'] / row['plain_bem']['value']
+            row['speedup_axial_only_vs_plain_bem'] = row['axial_only']['value'] / row['plain_bem']['value']
+            # errors against the GPU FP64 BEM trace of the slice (itself
+            # pinned to the CPU oracle by the parity tests)
+            row['err_vs_gpu_bem'] = {'surrogate': endpoint_errors_nm(pl_sur[:m], pl_bem[:, 1:3]),
+                                     'axial_only': endpoint_errors_nm(pl_ax[:m], pl_bem[:, 1:3])}
+            row['_planes'] = (pl_sur, pl_ax)
+            arms[name] = row
 
     if rank != 0:
+        if judge is not None:
+            judge.close()
         if ws > 1:
             import torch.distributed as dist
             dist.barrier()
@@ -543,7 +759,7 @@ def run_gpu(args):
     fp64_peak = measure_fp64_peak(B, torch)
     launch_s = total_ms / args.steps * 1e-3
     if sur is not None:
-        evals = np.mean(attempts) * 6
+        evals = attempts * 6
         achieved = evals * MLP_FLOP_PER_EVAL / launch_s / 1e12
         peak = peaks.get('bf16_tflops')
         peak_source = 'MEASURED_PEAKS.json bf16_tflops (burst)'
@@ -554,55 +770,94 @@ def run_gpu(args):
                 'traffic': args.traffic if args.engine == 'tc' else None, 'traffic_unit': 'bytes per launch (ncu)',
                 'kernel': 'k_trace_surrogate_tc' if args.engine == 'tc' else 'k_trace_surrogate',
                 'flop_per_unit': MLP_FLOP_PER_EVAL, 'units_per_launch': evals,
-                'unit_desc': 'network evaluations (dense BF16 flops of the 16-128x4-16 MLP)',
+                'unit_desc': 'network evaluations (dense BF16 flops of the 16-128x4-32 MLP)',
                 'peak_source': peak_source}
-        if plain is not None:
-            plain['roofline']['peak'] = fp64_peak
-            plain['roofline']['frac'] = plain['roofline']['achieved'] / fp64_peak
+        for row in arms.values():
+            rf = row['plain_bem']['roofline']
+            rf['peak'] = fp64_peak
+            rf['frac'] = rf['achieved'] / fp64_peak
+            rf['peak_source'] = 'FP64 FMA throughput measured in this run (tests/probe tb_probe_fp64_fma)'
     else:
-        pairs_per_launch = np.mean(attempts) * 6 * Nq
-        achieved = pairs_per_launch * args.flop_per_pair / launch_s / 1e12
+        pairs_per_launch = attempts * 6 * Nq
+        achieved = pairs_per_launch * FLOP_FIELD_PAIR / launch_s / 1e12
         roof = {'bound': 'fp64', 'achieved': achieved, 'peak': fp64_peak, 'unit': 'TFLOP/s',
                 'frac': achieved / fp64_peak if fp64_peak else None, 'traffic': None, 'kernel': 'k_trace_bem',
-                'flop_per_unit': args.flop_per_pair, 'units_per_launch': pairs_per_launch,
-                'unit_desc': 'ring-pair field evaluations (executed FP64 flops per pair, ncu)',
-                'peak_source': 'measured FP64 FMA probe (tb_probe_fp64_fma) in this run'}
+                'flop_per_unit': FLOP_FIELD_PAIR, 'units_per_launch': pairs_per_launch,
+                'unit_desc': 'ring-pair field evaluations, algorithmic FP64 flops (+ 1 log, 1 rsqrt, '
+                             '1 reciprocal per pair)',
+                'peak_source': 'FP64 FMA throughput measured in this run (tests/probe tb_probe_fp64_fma)'}
 
-    precision = precision_solve(args.precision_n) if args.precision_n > 0 else None
+    precision = precision_solve(args.precision_n, fp64_peak=fp64_peak, check=0) if args.precision_n > 0 else None
 
-    # ---- accuracy vs the CPU oracle and the CPU baseline (rank 0, N = 1)
-    cores = host_cores()
-    q_or, jac_or, pos_or = oracle_charges(geo, volts, cores)
-    q_gpu = field.electrostatic_point_charges.charges
-    charge_err = float(np.max(np.abs(q_gpu - q_or)) / np.abs(q_or).max())
-    rng = np.random.default_rng(7)
-    sample = rng.choice(E, min(args.check, E), replace=False)
-    err_max_nm = err_p99_nm = None
-    if len(sample):
-        err_max_nm, err_p99_nm = check_endpoints(plane, p0, v0, q_or, jac_or, pos_or, sample, cores)
-    cpu = None
-    if ws == 1 and args.cpu_seconds > 0:
-        rate, n, kind = cpu_reference_rate(geo, q_or, jac_or, pos_or, p0, v0, cores, args.cpu_seconds)
+    # ---- accuracy against the CPU oracle (the held-out sample of each beam)
+    accuracy = {'checked_against': 'CPU oracle: FP64 fill + QUADPACK diagonal + LAPACK solve on the host, FP64 BEM '
+                                   'RKF45 trace, cubic-Hermite crossing of the exit plane'}
+    if judge is not None:
+        for name, n_c in ((beam, n_check), (other, n_check_o)):
+            if not n_c:
+                continue
+            ref_xy = judge.result(name)
+            row = arms.get(name)
+            if row is not None:
+                pl_sur, pl_ax = row['_planes']
+                row['err_vs_oracle'] = {'surrogate': endpoint_errors_nm(pl_sur[:n_c], ref_xy),
+                                        'axial_only': endpoint_errors_nm(pl_ax[:n_c], ref_xy)}
+            elif name == beam:
+                accuracy[name] = endpoint_errors_nm(plane[:n_c], ref_xy)
+        accuracy['oracle_wall_s'] = judge.close()
+        accuracy['oracle_workers'] = judge.workers
+    if q_or is not None:
+        q_gpu = field.electrostatic_point_charges.charges
+        accuracy['charges_rel_err'] = float(np.max(np.abs(q_gpu - q_or)) / np.abs(q_or).max())
+    if beam in arms and 'err_vs_oracle' in arms[beam]:
+        eh = arms[beam]['err_vs_oracle']['surrogate']
+        accuracy.update({'endpoint_err_max_nm': eh['max_nm'], 'endpoint_err_p99_nm': eh['p99_nm'],
+                         'checked_electrons': eh['n'], 'checked_fraction': eh['n'] / E})
+    for row in arms.values():
+        row.pop('_planes', None)
+    if precision is not None and args.field_check > 0:
+        precision.update(precision_field_check(precision.pop('_field_state'), args.field_check, cores))
+    elif precision is not None:
+        precision.pop('_field_state', None)
+
+    # ---- CPU baselines (rank 0, N = 1): the reference's plain-BEM tracer and
+    # its axial-series tracer on this beam, all host threads, bounded samples
+    cpu = cpu_axial = None
+    if ws == 1 and args.cpu_seconds > 0 and q_or is not None:
+        rate, n, kind = cpu_reference_rate(q_or, jac_or, pos_or, p0, v0, cores, args.cpu_seconds)
         cpu = {'value': rate, 'unit': 'electrons/s', 'cores': cores, 'kind': 'reference' if kind == 'ref' else 'port',
                'sample': f'{n} electrons of this beam traced by the reference C backend (trace_particle + '
                          f'field_radial_traceable, plain BEM; the reference has no surrogate) on {cores} threads '
                          f'for ~{args.cpu_seconds:.0f} s'}
+        if sur is not None:
+            coeffs = reference_axial_table(q_or, jac_or, pos_or, sur.z)
+            rate, n, kind = cpu_reference_rate(q_or, jac_or, pos_or, p0, v0, cores, args.cpu_seconds / 2,
+                                               axial=(sur.z, coeffs))
+            cpu_axial = {'value': rate, 'unit': 'electrons/s', 'cores': cores,
+                         'kind': 'reference' if kind == 'ref' else 'port',
+                         'sample': f'{n} electrons of this beam traced by the reference C backend through its axial '
+                                   f'series (trace_particle + field_radial_derivs_traceable, FieldRadialAxial '
+                                   f'table of {len(sur.z)} z-points) on {cores} threads for '
+                                   f'~{args.cpu_seconds / 2:.0f} s'}
 
+    if sur is not None and beam in arms:
+        sp = arms[beam]['plain_bem']['value']
+        # electrons after which training + surrogate tracing beats the plain BEM tracer
+        setup['break_even_electrons'] = setup['surrogate_train_s'] / max(1.0 / sp - 1.0 / value, 1e-30)
     line = {'metric': METRIC, 'value': value, 'unit': 'electrons/s', 'n_gpus': ws, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
             'step_ms': {'min': float(np.min(ms_list)), 'median': float(np.median(ms_list)),
                         'max': float(np.max(ms_list))},
             'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'bf16+f64' if sur is not None else 'f64',
-            'data': 'synthetic', 'config': workload_config(E, args.field),
+            'data': 'synthetic', 'config': workload_config(E, args.field, beam),
             'e2e': {'value': e2e_value, 'unit': 'electrons/s', 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
                     'api': e2e_api},
-            'gpu_launches': args.steps, 'roofline': roof, 'plain_bem': plain,
-            'speedup_vs_plain_bem': (value / plain['value']) if plain else None,
-            'cpu_baseline': cpu, 'clocks': clk.summary(),
-            'accuracy': {'endpoint_err_max_nm': err_max_nm, 'endpoint_err_p99_nm': err_p99_nm,
-                         'checked_electrons': int(len(sample)), 'checked_against': 'CPU oracle FP64 BEM trace, Hermite crossing',
-                         'charges_rel_err': charge_err},
+            'gpu_launches': args.steps, 'roofline': roof,
+            'speedup_vs_plain_bem': arms[beam]['speedup_surrogate_vs_plain_bem'] if beam in arms else None,
+            'beams': arms or None,
+            'cpu_baseline': cpu, 'cpu_baseline_axial': cpu_axial, 'clocks': clk.summary(),
+            'accuracy': accuracy,
             'trace_stats': {'status_exited': int((status == 0).sum()),
                             'accepted_steps_mean': float(counters[:, 0].mean()),
                             'attempts_mean': float(counters[:, 1].mean()),
@@ -620,11 +875,150 @@ def run_solve(args):
     JSON line; used for the solver's profiles)."""
     import torch
     torch.cuda.set_device(dist_info()[2])
-    p = precision_solve(args.precision_n, fp64_lu=not args.skip_fp64_lu)
+    from traceon_b200 import backend as B
+    p = precision_solve(args.precision_n, fp64_lu=not args.skip_fp64_lu, fp64_peak=measure_fp64_peak(B, torch),
+                        check=args.field_check)
     line = {'metric': 'mixed-precision charge solve time (precision workload)', 'value': p['solve_mixed_ms'],
             'unit': 'ms', 'higher_is_better': False, 'n_gpus': 1, 'dtype': 'f32 tensor-core LU + f64 refinement',
             'data': 'synthetic', 'config': {'workload': p['workload'], 'elements': args.precision_n},
             'precision_solve': p}
+    print(json.dumps(line), flush=True)
+
+
+COMBINED_VOLTS = (0.0, 3000.0, 0.0)
+
+
+def run_combined(args):
+    """--workload combined: the combined electro-magnetostatic workload.  The
+    einzel lens meshed to 16,384 elements inside an iron pole piece
+    (mu_r = 1000) of 16,384 magnetizable elements magnetised by 4 coils (r ~
+    U[3, 6] mm, U[0.5, 5] kA-turns): both systems filled on the GPU and solved
+    by the mixed solve (beside the vendor FP64 LU), the surrogate trained on
+    (phi, E, H) of the 3 electrodes and 4 coils at unit strength, then
+    1,048,576 electrons at 5 keV (lognormal 2 %) traced through E + B by the
+    tensor-core surrogate tracer; the plain BEM tracer on a slice for the
+    comparison and as the judge of the slice's endpoints; a sample re-traced
+    by the CPU oracle."""
+    import torch
+    ws, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    from traceon_b200 import backend as B
+    from traceon_b200 import geometry as G
+    from traceon_b200.excitation import Excitation, Mesh
+    from traceon_b200.field import EffectivePointCharges
+    from traceon_b200.solver import ElectrostaticSolverRadial, MagnetostaticSolverRadial
+    from traceon_b200.surrogate import SurrogateTrainer, FieldSurrogate
+    from traceon_b200.tracing import Tracer
+    from scipy.constants import e as qe, m_e
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    cl = G.combined_lens(SEED, n_elec=args.combined_n, n_mag=args.combined_n)
+    geo = cl.geometry
+    exc = Excitation(Mesh.from_geometry(geo))
+    exc.add_voltage(**{n: v for n, v in zip(geo.names[:3], COMBINED_VOLTS)})
+    exc.add_magnetizable(pole=1000.0)
+    coils = EffectivePointCharges(*cl.coil_sources())
+    se = ElectrostaticSolverRadial(exc)
+    sm = MagnetostaticSolverRadial(exc, current_point_charges=coils)
+    solve = {}
+    fields = []
+    for name, sv in (('electrostatic', se), ('magnetostatic', sm)):
+        A = sv.get_matrix_device()
+        F = sv.get_right_hand_side_device()[None].contiguous()
+        B.dev_solve_mixed(A, F)
+        fill_ms, _ = timed(sv.get_matrix_device)
+        rhs_ms, _ = timed(sv.get_right_hand_side_device)
+        mixed_ms, (X, iters, rel) = timed(lambda: B.dev_solve_mixed(A, F))
+        torch.linalg.solve(A, F.T)
+        vendor_ms, X64 = timed(lambda: torch.linalg.solve(A, F.T))
+        err = float(((X[0] - X64[:, 0]).abs().max() / X64.abs().max()).item())
+        solve[name] = {'elements': len(sv.vertices), 'fill_fp64_ms': fill_ms, 'rhs_ms': rhs_ms,
+                       'solve_mixed_ms': mixed_ms, 'mixed_iterations': iters,
+                       'solve_fp64_vendor_lu_ms': vendor_ms, 'speedup_vs_vendor_fp64_lu': vendor_ms / mixed_ms,
+                       'charges_rel_err_vs_fp64': err}
+        jac, pos = sv.jacobians_and_positions()
+        fields.append(sv.charges_to_field(EffectivePointCharges(X[0].cpu().numpy(), jac, pos)))
+        del A
+        torch.cuda.empty_cache()
+    field = fields[0] + fields[1]
+    t0 = time.perf_counter()
+    tr = SurrogateTrainer(geo, electrodes=geo.names[:3], magnetizable={'pole': 1000.0}, coils=cl)
+    model, info = tr.train(n_samples=args.train_samples, steps=args.train_steps, batch=8192, seed=0)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    strengths = np.concatenate([COMBINED_VOLTS, cl.coil_current])
+    fs = FieldSurrogate(model, tr.fields, tr.z, tr.tabs, strengths, geo.segments, engine=args.engine)
+    E = args.combined_electrons
+    p0, v0 = G.combined_beam(E, SEED + 200)
+    start = torch.as_tensor(np.concatenate([p0, v0], 1), device='cuda')
+    qm = torch.full((E,), -qe / m_e, device='cuda', dtype=torch.float64)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device='cuda')
+
+    def run():
+        return fs.trace_device(start, qm, G.LENS_BOUNDS, ATOL, plane_z=G.LENS_EXIT_Z, max_attempts=50000)
+
+    run()
+    with Clocks(local) as clk:
+        ms, res = time_steps(run, args.steps, flush)
+    res = res[-1]
+    plane = res.plane.cpu().numpy()
+    status = res.status.cpu().numpy()
+    counters = res.counters.cpu().numpy()
+    value = E / (np.mean(ms) * 1e-3)
+    m = min(E, args.combined_bem_electrons)
+    bem = Tracer(field, G.LENS_BOUNDS)
+    st_m, qm_m = start[:m].contiguous(), qm[:m].contiguous()
+    ms_b, r_b = timed_launches(lambda: bem.trace_device(st_m, qm_m, atol=ATOL, plane_z=G.LENS_EXIT_Z,
+                                                        max_attempts=50000), 1, flush)
+    pl_b = r_b.plane.cpu().numpy()
+    plain = {'value': m / (np.mean(ms_b) * 1e-3), 'electrons': m, 'ms_per_step': float(np.mean(ms_b))}
+    acc = {'vs_gpu_bem': endpoint_errors_nm(plane[:m], pl_b[:, 1:3])}
+    evals = float(counters[:, 1].sum()) * 6
+    peak = read_peaks().get('bf16_tflops') or FALLBACK_BF16_TFLOPS
+    achieved = evals * MLP_FLOP_PER_EVAL / (np.mean(ms) * 1e-3) / 1e12
+    if args.check > 0:
+        from oracle.oracle import Oracle, EM, hermite_plane_crossing
+        from concurrent.futures import ThreadPoolExecutor
+        port = Oracle('port')
+        qe_, qm_ = fields[0].electrostatic_point_charges, fields[1].magnetostatic_point_charges
+        cur = cl.coil_sources()
+        n_c = min(args.check, m)
+
+        def one(i):
+            t, s_ = port.trace_bem(p0[i], v0[i], EM, qe_.charges, qe_.jacobians, qe_.positions, G.LENS_BOUNDS, ATOL,
+                                   mag=(qm_.charges, qm_.jacobians, qm_.positions), current=cur)
+            h = hermite_plane_crossing(t, s_, G.LENS_EXIT_Z)
+            return (np.nan, np.nan) if h is None else (h[0], h[1])
+
+        with ThreadPoolExecutor(host_cores()) as ex:
+            ref = np.array(list(ex.map(one, range(n_c))))
+        acc['vs_cpu_oracle'] = endpoint_errors_nm(plane[:n_c], ref)
+        acc['vs_cpu_oracle_note'] = 'the GPU solve\'s charges traced by the oracle (FP64 BEM, E + B)'
+    line = {'metric': 'traced electrons/s at <=1 nm endpoint error, combined electro-magnetostatic lens, '
+                      'surrogate (phi, E, B) vs plain BEM field', 'value': value, 'unit': 'electrons/s',
+            'n_gpus': 1, 'steps': args.steps, 'ms_per_step': float(np.mean(ms)), 'higher_is_better': True,
+            'dtype': 'bf16+f64', 'data': 'synthetic',
+            'config': {'workload': f'combined electro-magnetostatic lens: einzel lens of {args.combined_n} elements '
+                                   f'(0 / 3 kV / 0) in an iron pole piece (mu_r 1000) of {args.combined_n} elements, '
+                                   f'4 coils {np.round(cl.coil_current).tolist()} A-turns; {E} electrons at 5 keV '
+                                   f'(lognormal 2 %), r0 <= 0.2 mm, +-10 mrad, RKF45 atol 1e-10 m',
+                       'electrons_per_step': E},
+            'solve': solve, 'surrogate_train_s': train_s, 'surrogate_holdout_mse': info['holdout_mse'],
+            'plain_bem': plain, 'speedup_vs_plain_bem': value / plain['value'],
+            'roofline': {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                         'frac': achieved / peak, 'kernel': 'k_trace_surrogate_tc<MAG>',
+                         'flop_per_unit': MLP_FLOP_PER_EVAL, 'units_per_launch': evals},
+            'trace_stats': {'status_exited': int((status == 0).sum()), 'attempts_mean': float(counters[:, 1].mean()),
+                            'bem_fallback_evals': int(counters[:, 2].sum())},
+            'accuracy': acc, 'clocks': clk.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -634,8 +1028,12 @@ def main():
     ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='tracer', choices=['tracer', 'solve'],
-                    help='tracer: the headline metric (default); solve: only the precision-workload solve')
+    ap.add_argument('--workload', default='tracer', choices=['tracer', 'solve', 'combined'],
+                    help='tracer: the headline metric (default); solve: only the precision-workload solve; '
+                         'combined: the combined electro-magnetostatic workload')
+    ap.add_argument('--combined-n', type=int, default=16384, help='elements of each part of the combined lens')
+    ap.add_argument('--combined-electrons', type=int, default=1 << 20)
+    ap.add_argument('--combined-bem-electrons', type=int, default=2048)
     ap.add_argument('--electrons', type=int, default=262144)
     ap.add_argument('--field', default='surrogate', choices=['surrogate', 'bem'])
     ap.add_argument('--bem-electrons', type=int, default=16384, help='slice traced with the plain BEM field')
@@ -644,16 +1042,20 @@ def main():
     ap.add_argument('--team-warps', type=int, default=0)
     ap.add_argument('--engine', default='tc', choices=['tc', 'warp'],
                     help='surrogate network engine: tcgen05 (tc) or warp-level mma.sync (warp)')
-    ap.add_argument('--check', type=int, default=16, help='electrons checked against the CPU oracle')
+    ap.add_argument('--beam', default='wide', choices=sorted(BEAMS),
+                    help='beam of the headline number (the other beam is measured beside it)')
+    ap.add_argument('--check', type=int, default=2621,
+                    help='electrons of the headline beam judged by the CPU oracle (default: 1 %% of 262,144)')
+    ap.add_argument('--check-other', type=int, default=256,
+                    help='electrons of the other beam judged by the CPU oracle')
+    ap.add_argument('--field-check', type=int, default=4096,
+                    help='points of the precision workload field judged by the CPU oracle')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
     ap.add_argument('--skip-fp64-lu', action='store_true',
                     help='--workload solve: time only the mixed solve (for profiles)')
     ap.add_argument('--precision-n', type=int, default=16384,
                     help='elements of the precision-workload solve measured beside the tracer (0: skip)')
     ap.add_argument('--ref-seconds', type=float, default=20.0)
-    # executed FP64 flops per ring-pair evaluation of the tracer's field sum
-    # (dadd + dmul + 2 dfma per pair, from the ncu instruction counts)
-    ap.add_argument('--flop-per-pair', type=float, default=162.0)
     # DRAM bytes (read + write) of one full-size launch of the dominant kernel
     # from an ncu capture of this workload (k_trace_surrogate_tc: 18.67 MB read
     # + 4.96 MB written; see the profile summary of that kernel)
@@ -663,6 +1065,8 @@ def main():
         run_reference(args)
     elif args.workload == 'solve':
         run_solve(args)
+    elif args.workload == 'combined':
+        run_combined(args)
     else:
         run_gpu(args)
 
