@@ -787,7 +787,8 @@ def run_gpu(args):
                              '1 reciprocal per pair)',
                 'peak_source': 'FP64 FMA throughput measured in this run (tests/probe tb_probe_fp64_fma)'}
 
-    precision = precision_solve(args.precision_n, fp64_peak=fp64_peak, check=0) if args.precision_n > 0 else None
+    precision = precision_solve(args.precision_n, fp64_peak=fp64_peak, check=0, field_points=args.field_points) \
+        if args.precision_n > 0 else None
 
     # ---- accuracy against the CPU oracle (the held-out sample of each beam)
     accuracy = {'checked_against': 'CPU oracle: FP64 fill + QUADPACK diagonal + LAPACK solve on the host, FP64 BEM '
@@ -877,7 +878,7 @@ def run_solve(args):
     torch.cuda.set_device(dist_info()[2])
     from traceon_b200 import backend as B
     p = precision_solve(args.precision_n, fp64_lu=not args.skip_fp64_lu, fp64_peak=measure_fp64_peak(B, torch),
-                        check=args.field_check)
+                        check=args.field_check, field_points=args.field_points)
     line = {'metric': 'mixed-precision charge solve time (precision workload)', 'value': p['solve_mixed_ms'],
             'unit': 'ms', 'higher_is_better': False, 'n_gpus': 1, 'dtype': 'f32 tensor-core LU + f64 refinement',
             'data': 'synthetic', 'config': {'workload': p['workload'], 'elements': args.precision_n},
@@ -1048,6 +1049,8 @@ def main():
                     help='electrons of the headline beam judged by the CPU oracle (default: 1 %% of 262,144)')
     ap.add_argument('--check-other', type=int, default=256,
                     help='electrons of the other beam judged by the CPU oracle')
+    ap.add_argument('--field-points', type=int, default=1 << 20,
+                    help='points of the precision workload field evaluation')
     ap.add_argument('--field-check', type=int, default=4096,
                     help='points of the precision workload field judged by the CPU oracle')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)

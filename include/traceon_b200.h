@@ -318,8 +318,11 @@ int tb_gemm_sub_tf32x3(float *C, int64_t ldc, const float *A, int64_t lda, const
 /* Mixed-precision solve of A x = f for the nrhs (<= 16) rows of F (nrhs, N)
  * into X (nrhs, N): FP32 LU without pivoting of A diag(c), c_j = 1 / max_i
  * |A_ij|, then FP64 iterative refinement with the FP64 matrix until, for
- * every right-hand side, max |correction| / max |x| <= tol (at most max_iter
- * rounds; corrections that stall within 100 tol count as converged).  `work`
+ * every right-hand side, max |correction| / max |x| <= tol, or the error
+ * left after the last correction, extrapolated from the contraction of the
+ * last two, is (at most max_iter rounds; corrections that stall within 100
+ * tol count as converged); *last_rel_out gets the last correction's size or
+ * that extrapolated error.  `work`
  * is device scratch of tb_solve_mixed_workspace(N, nrhs) bytes.  Returns
  * TB_SINGULAR when refinement does not converge (the caller then solves with
  * tb_lu_factor_perm / tb_lu_solve_perm).  Replaces numpy.linalg.solve

@@ -235,7 +235,10 @@ def test_dielectric_rows_at_scale(cuda, port):
     """Flux (dielectric) rows at N = 4,002 (the middle electrode a
     dielectric of permittivity 4): the GPU fill of the flux rows against the
     oracle's fill of the same matrix (row sample, 1e-12 of the largest
-    entry), and the charges against LAPACK on the oracle's matrix (1e-10)."""
+    entry); the GPU solve against LAPACK on the GPU-filled matrix (1e-10);
+    and the charges against LAPACK on the oracle's matrix within what the
+    matrix agreement allows for this system's condition number (flux rows
+    make it far less well conditioned than voltage rows alone)."""
     from traceon_b200 import geometry as G
     from traceon_b200.excitation import Excitation, Mesh
     from traceon_b200.solver import ElectrostaticSolverRadial
@@ -252,5 +255,8 @@ def test_dielectric_rows_at_scale(cuda, port):
     assert np.max(np.abs(A_gpu[rows] - A[rows])) <= 1e-12 * np.max(np.abs(A))
     F = s.get_right_hand_side()
     X = s.solve_charges_device(np.array([F])).cpu().numpy()[0]
+    q_same = np.linalg.solve(A_gpu, F)
+    assert np.max(np.abs(X - q_same)) / np.max(np.abs(q_same)) < 1e-10
     q = np.linalg.solve(A, F)
-    assert np.max(np.abs(X - q)) / np.max(np.abs(q)) < 1e-10
+    bound = np.linalg.cond(A) * 1e-12
+    assert np.max(np.abs(X - q)) / np.max(np.abs(q)) < 10 * bound

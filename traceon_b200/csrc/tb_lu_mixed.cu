@@ -1460,6 +1460,13 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
       break;
     }
     if (rel <= tol) break;
+    // Refinement contracts the error linearly: with q = rel / prev the error
+    // left after this correction is about rel * q, so when that is already
+    // below tol the round that would only confirm it is skipped.
+    if (it >= 2 && rel < 0.5 * prev && rel * (rel / prev) <= tol) {
+      rel *= rel / prev;  // reported: the estimated remaining error
+      break;
+    }
     // Corrections that stop shrinking just above tol have reached the FP64
     // rounding floor of the residual (about cond * 1e-16): converged.
     if (it >= 3 && rel <= 100.0 * tol && rel > 0.5 * prev) {

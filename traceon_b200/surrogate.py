@@ -126,16 +126,17 @@ class MLP:
                 _call('tb_mlp_bias_out', Cm.data_ptr(), self._w(self.p, b).data_ptr(), out.data_ptr(), M, fout, _s())
         return (out, pre, acts) if keep else out
 
-    def loss_and_grad(self, X, T, n_out):
-        """MSE over the first n_out outputs; fills self.g, returns the loss (device scalar)."""
+    def loss_and_grad(self, X, T, n_out, w=None):
+        """MSE over the first n_out outputs (rows weighted by w (M) if given);
+        fills self.g, returns the loss (device scalar)."""
         torch = B._torch()
         M = X.shape[0]
         out, pre, acts = self.forward(X, keep=True)
         dY = torch.empty((M, OUT), dtype=torch.bfloat16, device=X.device)
         nblk = (M * OUT + 255) // 256
         part = torch.empty(nblk, dtype=torch.float32, device=X.device)
-        _call('tb_mlp_mse_grad', out.data_ptr(), T.data_ptr(), None, dY.data_ptr(), part.data_ptr(), M, OUT, n_out,
-              _s())
+        _call('tb_mlp_mse_grad', out.data_ptr(), T.data_ptr(), B._ptr(w), dY.data_ptr(), part.data_ptr(), M, OUT,
+              n_out, _s())
         g = dY
         for li in range(len(LAYERS) - 1, -1, -1):
             W, b, fin, fout = LAYERS[li]
@@ -364,7 +365,13 @@ class SurrogateTrainer:
         return pts, R
 
     def train(self, n_samples=1 << 22, steps=20000, batch=8192, lr=2e-3, lr_end=2e-5, seed=0, holdout=0.01,
-              log_every=0):
+              log_every=0, weighting='radial', bins=16):
+        """Adam on the MSE of the normalised residuals.  weighting 'radial'
+        weights every sample by the inverse mean square of the targets in
+        its band of rho (`bins` bands), so that the network is fitted to the
+        same relative accuracy at every radius instead of being dominated by
+        the largest residuals near the electrodes; 'uniform' weights all
+        samples alike."""
         torch = B._torch()
         pts, R = self.dataset(n_samples, seed)
         n_el = len(self.fields)  # field sources: electrodes and coils, 3 outputs each
@@ -382,7 +389,19 @@ class SurrogateTrainer:
         pts_t = torch.as_tensor(pts, device=dev)
         X = features(pts_t, model.r_max, model.z_c, model.z_half)
         Tt = torch.as_tensor(T, device=dev)
+        if weighting == 'radial':
+            rho = np.hypot(pts[:, 0], pts[:, 1]) / model.r_max
+            band = np.minimum((rho * bins).astype(int), bins - 1)
+            ms = np.array([np.mean(T[band == b] ** 2) if np.any(band == b) else 1.0 for b in range(bins)])
+            wts = 1.0 / np.maximum(ms[band], 1e-30)
+            wts = (wts / wts.mean()).astype(np.float32)
+        elif weighting == 'uniform':
+            wts = None
+        else:
+            raise ValueError(f'unknown weighting {weighting!r}')
+        Wt = None if wts is None else torch.as_tensor(wts, device=dev)
         Xtr, Ttr = X[n_hold:], Tt[n_hold:]
+        Wtr = None if Wt is None else Wt[n_hold:]
         Xho, Tho = X[:n_hold], Tt[:n_hold]
         ntr = Xtr.shape[0]
         gen = torch.Generator(device=dev)
@@ -390,7 +409,8 @@ class SurrogateTrainer:
         hist = []
         for step in range(steps):
             idx = torch.randint(0, ntr, (batch,), device=dev, generator=gen)
-            loss = model.mlp.loss_and_grad(Xtr[idx].contiguous(), Ttr[idx].contiguous(), 3 * n_el)
+            loss = model.mlp.loss_and_grad(Xtr[idx].contiguous(), Ttr[idx].contiguous(), 3 * n_el,
+                                           None if Wtr is None else Wtr[idx].contiguous())
             frac = step / max(1, steps - 1)
             cur = lr_end + 0.5 * (lr - lr_end) * (1 + math.cos(math.pi * frac))
             model.mlp.adam(cur)
