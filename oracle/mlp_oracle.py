@@ -37,16 +37,6 @@ def silu(z):
     return z / (1 + np.exp(-z))
 
 
-def silu_bf16(z):
-    """The activation as the GPU evaluates it in packed BF16 arithmetic:
-    h = bf16(z / 2), t = bf16(tanh(h)), silu = bf16(h + h t) (one rounding
-    of the fused multiply-add).  Exact tanh here; the GPU's tanh.approx
-    differs from it by at most a BF16 rounding step."""
-    h = bf16(0.5 * np.asarray(z, dtype=np.float64))
-    t = bf16(np.tanh(h))
-    return bf16(h + h * t)
-
-
 def silu_grad(z):
     s = 1 / (1 + np.exp(-z))
     return s * (1 + z * (1 - s))
@@ -73,7 +63,7 @@ def forward(params, X):
         z = a @ bf16(P[W]).T + P[b]
         if W != 'W5':
             pre.append(z)
-            a = silu_bf16(z)
+            a = bf16(silu(z))
             acts.append(a)
         else:
             out = z

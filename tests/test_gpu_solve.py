@@ -255,8 +255,10 @@ def test_dielectric_rows_at_scale(cuda, port):
     assert np.max(np.abs(A_gpu[rows] - A[rows])) <= 1e-12 * np.max(np.abs(A))
     F = s.get_right_hand_side()
     X = s.solve_charges_device(np.array([F])).cpu().numpy()[0]
+    # FP64 solves of this system agree only to about cond(A) x 1e-16 (far
+    # looser than the charge tolerance of the voltage-row systems)
+    cond = np.linalg.cond(A_gpu)
     q_same = np.linalg.solve(A_gpu, F)
-    assert np.max(np.abs(X - q_same)) / np.max(np.abs(q_same)) < 1e-10
+    assert np.max(np.abs(X - q_same)) / np.max(np.abs(q_same)) < max(1e-10, 10 * cond * 1e-16)
     q = np.linalg.solve(A, F)
-    bound = np.linalg.cond(A) * 1e-12
-    assert np.max(np.abs(X - q)) / np.max(np.abs(q)) < 10 * bound
+    assert np.max(np.abs(X - q)) / np.max(np.abs(q)) < 10 * cond * 1e-12
