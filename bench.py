@@ -58,7 +58,7 @@ METRIC = 'traced electrons/s at <=1 nm endpoint error, surrogate vs plain BEM fi
 # narrow: the plain-method workload's r0 <= 0.2 mm, where the axial series
 # alone already traces within 1 nm.  wide: start radii out to where the axial
 # series alone misses 1 nm and the learned correction is what holds it.
-BEAMS = {'narrow': {'r_max': 0.2e-3}, 'wide': {'r_max': 0.6e-3}}
+BEAMS = {'narrow': {'r_max': 0.2e-3}, 'wide': {'r_max': 0.35e-3}}
 
 
 def workload_config(electrons, field, beam):
@@ -985,13 +985,13 @@ def run_combined(args):
     evals = float(counters[:, 1].sum()) * 6
     peak = read_peaks().get('bf16_tflops') or FALLBACK_BF16_TFLOPS
     achieved = evals * MLP_FLOP_PER_EVAL / (np.mean(ms) * 1e-3) / 1e12
-    if args.check > 0:
+    if args.combined_check > 0:
         from oracle.oracle import Oracle, EM, hermite_plane_crossing
         from concurrent.futures import ThreadPoolExecutor
         port = Oracle('port')
         qe_, qm_ = fields[0].electrostatic_point_charges, fields[1].magnetostatic_point_charges
         cur = cl.coil_sources()
-        n_c = min(args.check, m)
+        n_c = min(args.combined_check, m)
 
         def one(i):
             t, s_ = port.trace_bem(p0[i], v0[i], EM, qe_.charges, qe_.jacobians, qe_.positions, G.LENS_BOUNDS, ATOL,
@@ -1035,11 +1035,13 @@ def main():
     ap.add_argument('--combined-n', type=int, default=16384, help='elements of each part of the combined lens')
     ap.add_argument('--combined-electrons', type=int, default=1 << 20)
     ap.add_argument('--combined-bem-electrons', type=int, default=2048)
+    ap.add_argument('--combined-check', type=int, default=16,
+                    help='electrons of the combined workload re-traced by the CPU oracle (~1.5 min each per core)')
     ap.add_argument('--electrons', type=int, default=262144)
     ap.add_argument('--field', default='surrogate', choices=['surrogate', 'bem'])
     ap.add_argument('--bem-electrons', type=int, default=16384, help='slice traced with the plain BEM field')
     ap.add_argument('--train-samples', type=int, default=1 << 22)
-    ap.add_argument('--train-steps', type=int, default=40000)
+    ap.add_argument('--train-steps', type=int, default=80000)
     ap.add_argument('--team-warps', type=int, default=0)
     ap.add_argument('--engine', default='tc', choices=['tc', 'warp'],
                     help='surrogate network engine: tcgen05 (tc) or warp-level mma.sync (warp)')

@@ -347,7 +347,7 @@ class SurrogateTrainer:
     when `coils` is given, its current coils magnetising the `magnetizable`
     electrodes ({name: mu_r})."""
 
-    def __init__(self, geo, r_min=0.1e-3, r_max=0.95e-3, z_lo=-11.5e-3, z_hi=11.5e-3, nz=2301, exclude=50e-6,
+    def __init__(self, geo, r_min=0.1e-3, r_max=0.75e-3, z_lo=-11.5e-3, z_hi=11.5e-3, nz=4601, exclude=50e-6,
                  env_power=8, electrodes=None, magnetizable=None, coils=None):
         self.geo = geo
         self.r_min, self.r_max, self.z_lo, self.z_hi = r_min, r_max, z_lo, z_hi
@@ -364,7 +364,7 @@ class SurrogateTrainer:
         R = residual_targets(pts, self.fields, self.zt, self.tabs).reshape(len(pts), -1)
         return pts, R
 
-    def train(self, n_samples=1 << 22, steps=20000, batch=8192, lr=2e-3, lr_end=2e-5, seed=0, holdout=0.01,
+    def train(self, n_samples=1 << 22, steps=80000, batch=8192, lr=2e-3, lr_end=2e-5, seed=0, holdout=0.01,
               log_every=0, weighting='radial', bins=16):
         """Adam on the MSE of the normalised residuals.  weighting 'radial'
         weights every sample by the inverse mean square of the targets in
