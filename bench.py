@@ -7,8 +7,8 @@ the GPU.  A step traces a batch of electrons (default 262,144) at 1 keV +-5 %,
 angles +-20 mrad, start radius up to the beam's r_max at z = -9.5 mm, with
 adaptive RKF45 at atol = 1e-10 m until they leave the bounds (|x|,|y| <= 2 mm,
 |z| <= 10 mm), recording each electron's crossing of the exit plane
-z = +9.5 mm.  Two beams: `wide` (r0 <= 0.6 mm, the headline: the axial series
-alone misses 1 nm there, the learned correction holds it) and `narrow`
+z = +9.5 mm.  Two beams: `wide` (r0 <= 0.35 mm, the headline: the axial
+series alone misses 1 nm there, the learned correction holds it) and `narrow`
 (r0 <= 0.2 mm, the plain-method workload's beam).  Synthetic inputs; no
 dataset.
 
