@@ -245,6 +245,49 @@ int tb_fill_matrix_radial_batched(const tb_geometry_t *geoms, int n_geoms, int64
  * stored on each geometry's matrix diagonal; one launch. */
 int tb_self_integrals_batched(const tb_geometry_t *geoms, int n_geoms, int64_t total_elements, tb_stream_t stream);
 
+/* ---- Batched solve: many geometries of uneven N filled, factored and
+ * solved in ONE persistent launch.  No counterpart in the reference, which
+ * fills (solver.py:204-232) and solves (solver.py:160-180, LAPACK dgesv) one
+ * geometry at a time.  Each matrix is padded to T x T tiles of 64 x 64 and
+ * factored without pivoting (left-looking, tile tasks in dependency order,
+ * FP64); a zero or non-finite pivot or charge marks the geometry
+ * TB_SINGULAR for the caller to solve with the pivoted LU. */
+typedef struct {
+  const double *vertices;   /* (N, 4, 3) cubic line elements (device) */
+  const uint8_t *types;     /* (N) excitation types */
+  const double *values;     /* (N) excitation values */
+  const double *rhs;        /* (N) right-hand side */
+  double *charges;          /* (N) solution (out) */
+  int64_t N;
+  /* set by tb_batch_solve_plan: */
+  int64_t T;                /* tiles per side, ceil(N / 64) */
+  int64_t a_off;            /* workspace offset (doubles) of the padded (64 T)^2 matrix */
+  int64_t inv_off;          /* workspace offset of the T inverse tiles (64 x 64) */
+  int64_t v_off;            /* workspace offset of the 64 T sweep vector */
+  int64_t flag_off;         /* flag offset (int32 words) of T^2 + 2 T + 1 words */
+  int64_t ring_off;         /* the geometry's first ring in the packed sources (16 N rings) */
+} tb_batch_item_t;
+
+/* Host helper: sets T and the offsets of n_items items (host array), writes
+ * the task list (4 int32 per task) when tasks is not NULL and returns the
+ * number of tasks (-1 on bad sizes).  sizes[0] = workspace doubles,
+ * sizes[1] = flag words, sizes[2] = source rings (16 x sum N).  Copy items
+ * and tasks to device memory for tb_batch_solve. */
+int64_t tb_batch_solve_plan(tb_batch_item_t *items, int n_items, int32_t *tasks, int64_t *sizes);
+
+/* Fills, factors and solves every item in one persistent launch (items,
+ * tasks, work (16-byte aligned), flags, sources, status: device memory).
+ * flags (n_flags = sizes[1] words) and status are reset by this call with
+ * two memsets on the stream, so a CUDA graph captured around it replays
+ * cleanly.  sources: NULL, or (3, total_rings) receiving the charges packed
+ * as tb_pack_sources does (r | z | charge x jacobian), geometry g from ring
+ * ring_off -- the layout tb_trace_rk45_geometries reads.  status[g]: TB_OK,
+ * TB_SINGULAR, or -1 if the launch gave up on a bounded wait (every wait is
+ * bounded by tb_set_wait_limit).  blocks_per_sm: 0 = as many as fit. */
+int tb_batch_solve(const tb_batch_item_t *items, int n_items, const int32_t *tasks, int64_t n_tasks, double *work,
+                   int32_t *flags, int64_t n_flags, double *sources, int64_t total_rings, int32_t *status,
+                   int blocks_per_sm, tb_stream_t stream);
+
 /* Singular self terms: diag[i] = integral over alpha in [-1, 1] of the
  * self integrand of element i (self_potential_radial, radial.c:182-196, for
  * voltage rows; self_field_dot_normal_radial - 1, radial.c:203-222 and
@@ -434,11 +477,13 @@ int tb_trace_rk45(const double *start, const double *t0, const double *qm, int64
  * src_offsets[geom[i] + 1] - 1 of field->elec_sources (n_elec = total).
  *   geom (n) int32 device, ids in [0, n_geoms) (an id outside sums no rings)
  *   src_offsets (n_geoms + 1) int64 device, non-decreasing, last <= n_elec
+ *   geom_bounds NULL (opts->bounds for every particle) or (n_geoms, 6)
+ *   device: each geometry's own bounding box, as opts->bounds
  * Electrostatic sources only (n_mag = n_cur = 0, no axial table); TB_BAD_ARG
  * otherwise. */
 int tb_trace_rk45_geometries(const double *start, const double *t0, const double *qm, const int32_t *geom,
                              int64_t n, const tb_field_t *field, const int64_t *src_offsets, int64_t n_geoms,
-                             const tb_trace_opts_t *opts, double *rows, int64_t *nrows, int32_t *status,
+                             const double *geom_bounds, const tb_trace_opts_t *opts, double *rows, int64_t *nrows, int32_t *status,
                              double *final_state, double *plane, int64_t *counters, int32_t *work,
                              tb_stream_t stream);
 

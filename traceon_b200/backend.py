@@ -145,6 +145,12 @@ class TbGeometry(C.Structure):
                 ("lda", i64), ("N", i64), ("tile0", i64), ("elem0", i64)]
 
 
+class TbBatchItem(C.Structure):
+    """tb_batch_item_t of include/traceon_b200.h"""
+    _fields_ = [("vertices", vp), ("types", vp), ("values", vp), ("rhs", vp), ("charges", vp), ("N", i64),
+                ("T", i64), ("a_off", i64), ("inv_off", i64), ("v_off", i64), ("flag_off", i64), ("ring_off", i64)]
+
+
 class TbTraceOpts(C.Structure):
     """tb_trace_opts_t of include/traceon_b200.h"""
     _fields_ = [("bounds", dbl * 6), ("atol", dbl), ("plane_z", dbl), ("record_plane", C.c_int),
@@ -217,8 +223,9 @@ _DEV = {
     'tb_axial_coefficients': (vp, i64, dbl, vp, vp),
     'tb_axial_field_points': (vp, i64, vp, i64, vp, vp, vp, vp),
     'tb_trace_rk45': (vp, vp, vp, i64, C.POINTER(TbField), C.POINTER(TbTraceOpts), vp, vp, vp, vp, vp, vp, vp, vp),
-    'tb_trace_rk45_geometries': (vp, vp, vp, vp, i64, C.POINTER(TbField), vp, i64, C.POINTER(TbTraceOpts), vp, vp, vp,
-                                 vp, vp, vp, vp, vp),
+    'tb_trace_rk45_geometries': (vp, vp, vp, vp, i64, C.POINTER(TbField), vp, i64, vp, C.POINTER(TbTraceOpts), vp, vp,
+                                 vp, vp, vp, vp, vp, vp),
+    'tb_batch_solve': (vp, C.c_int, vp, i64, vp, vp, i64, vp, i64, vp, C.c_int, vp),
     'tb_num_sms': (),
     'tb_lu_nopiv_f64': (vp, i64, i64, vp),
     'tb_lu_nopiv_f32': (vp, i64, i64, vp),
@@ -234,6 +241,8 @@ for _name, _args in _DEV.items():
     _f = getattr(backend_lib, _name)
     _f.restype = C.c_int
     _f.argtypes = list(_args)
+backend_lib.tb_batch_solve_plan.restype = i64
+backend_lib.tb_batch_solve_plan.argtypes = [vp, C.c_int, vp, C.POINTER(i64)]
 backend_lib.tb_set_wait_limit.restype = i64
 backend_lib.tb_set_wait_limit.argtypes = [i64]
 

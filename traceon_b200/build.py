@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libtraceon_b200.so')
 INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
 
-SOURCES = ['tb_bem.cu', 'tb_lu.cu', 'tb_trace.cu', 'tb_compat.cu', 'tb_mlp.cu', 'tb_lu_mixed.cu', 'tb_post.cu']
+SOURCES = ['tb_bem.cu', 'tb_lu.cu', 'tb_trace.cu', 'tb_compat.cu', 'tb_mlp.cu', 'tb_lu_mixed.cu', 'tb_post.cu', 'tb_batch.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '-shared', '--expt-relaxed-constexpr',
          '-Xptxas', '-v']

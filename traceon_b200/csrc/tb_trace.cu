@@ -60,6 +60,7 @@ struct TraceParams {
   const int32_t* geom = nullptr;
   const int64_t* eoff = nullptr;
   int64_t ngeom = 0;
+  const double* gbounds = nullptr;  // (ngeom, 6) per-geometry bounds, or null: bounds
   long long wait_cycles = DEFAULT_WAIT_CYCLES;  // bound of the engine's progress waits
 };
 
@@ -258,6 +259,7 @@ struct BemTeamField {
   int team, lt;
   double (*red)[6];  // [TW][6] per team
   int64_t e0 = 0, e1 = 0;  // GEOM: the electrostatic rings of the current particle's geometry
+  const double* bnd = nullptr;  // GEOM: its bounding box (null: P.bounds)
 
   __device__ void operator()(const double* p, double* E, double* H) {
     constexpr int T = 32 * TW;
@@ -365,11 +367,12 @@ __device__ void rk45_team(const TraceParams& P, int64_t idx, BemTeamField<TW, GE
     for (int c = 0; c < 7; c++) P.plane[idx * 7 + c] = __longlong_as_double(0x7ff8000000000000LL);
   const double atol = P.atol;
 
+  const double* bounds = GEOM && field.bnd ? field.bnd : P.bounds;
   for (;;) {
     {
       double y[6];
       for (int c = 0; c < 6; c++) y[c] = S->y[c];
-      if (!in_bounds(P.bounds, y)) break;
+      if (!in_bounds(bounds, y)) break;
     }
     if (S->attempts >= P.max_attempts) {
       S->status = TRACE_MAX_ATTEMPTS;
@@ -506,6 +509,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, 2) k_trace_bem(TraceParams P) {
       const bool ok = g >= 0 && g < P.ngeom;
       field.e0 = ok ? P.eoff[g] : 0;
       field.e1 = ok ? P.eoff[g + 1] : 0;
+      field.bnd = ok && P.gbounds ? P.gbounds + 6 * g : nullptr;
     }
     rk45_team(P, idx, field, &s_state[team][lt / 32], lt == 0);
     __syncwarp();
@@ -1420,7 +1424,8 @@ extern "C" int tb_trace_surrogate(const double* start, const double* t0, const d
 }
 
 static int trace_rk45(const double* start, const double* t0, const double* qm, const int32_t* geom, int64_t n,
-                      const tb_field_t* field, const int64_t* src_offsets, int64_t n_geoms, const tb_trace_opts_t* opts,
+                      const tb_field_t* field, const int64_t* src_offsets, int64_t n_geoms,
+                      const double* geom_bounds, const tb_trace_opts_t* opts,
                       double* rows, int64_t* nrows, int32_t* status, double* final_state, double* plane,
                       int64_t* counters, int32_t* work, tb_stream_t stream) {
   if (!field || !opts || n < 0 || !work) return BAD_ARG;
@@ -1468,6 +1473,7 @@ static int trace_rk45(const double* start, const double* t0, const double* qm, c
     P.geom = geom;
     P.eoff = src_offsets;
     P.ngeom = n_geoms;
+    P.gbounds = geom_bounds;
   }
   cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemsetAsync(work, 0, sizeof(int32_t), s) != cudaSuccess) return CUDA_ERR;
@@ -1501,18 +1507,20 @@ extern "C" int tb_trace_rk45(const double* start, const double* t0, const double
                              const tb_field_t* field, const tb_trace_opts_t* opts, double* rows, int64_t* nrows,
                              int32_t* status, double* final_state, double* plane, int64_t* counters, int32_t* work,
                              tb_stream_t stream) {
-  return trace_rk45(start, t0, qm, nullptr, n, field, nullptr, 0, opts, rows, nrows, status, final_state, plane,
+  return trace_rk45(start, t0, qm, nullptr, n, field, nullptr, 0, nullptr, opts, rows, nrows, status, final_state, plane,
                     counters, work, stream);
 }
 
 extern "C" int tb_trace_rk45_geometries(const double* start, const double* t0, const double* qm, const int32_t* geom,
                                         int64_t n, const tb_field_t* field, const int64_t* src_offsets,
-                                        int64_t n_geoms, const tb_trace_opts_t* opts, double* rows, int64_t* nrows,
+                                        int64_t n_geoms, const double* geom_bounds, const tb_trace_opts_t* opts,
+                                        double* rows, int64_t* nrows,
                                         int32_t* status, double* final_state, double* plane, int64_t* counters,
                                         int32_t* work, tb_stream_t stream) {
   if (n > 0 && !geom) return BAD_ARG;
   if (n == 0) return OK;
-  return trace_rk45(start, t0, qm, geom, n, field, src_offsets, n_geoms, opts, rows, nrows, status, final_state,
+  return trace_rk45(start, t0, qm, geom, n, field, src_offsets, n_geoms, geom_bounds, opts, rows, nrows, status,
+                    final_state,
                     plane, counters, work, stream);
 }
 

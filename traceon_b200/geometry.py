@@ -218,6 +218,64 @@ def random_lens(seed: int, n_range=(500, 6000), tubes_range=(2, 5), r_range=(0.5
     return geo, rng.uniform(*volt_range, k)
 
 
+class MirrorLens:
+    """A lens of the batching workload: a random_lens stack followed by an
+    electrostatic mirror (an aperture plate) at -1.1 x the beam voltage.
+    geometry: LensGeometry whose last electrode is 'mirror'; voltages: one per
+    electrode; z_start: where the beam starts (0.5 mm before the first tube);
+    bounds: (3, 2) box the particles are traced in (a square inside the
+    narrowest bore in x and y, from 0.5 mm behind the start to 1 mm past the
+    mirror in z)."""
+
+    def __init__(self, geometry, voltages, z_start, bounds):
+        self.geometry, self.voltages, self.z_start, self.bounds = geometry, voltages, z_start, bounds
+
+
+def mirror_lens(seed: int, n_range=(500, 6000), beam_voltage: float = 1000.0, mirror_gap=1.0 * MM,
+                plate=0.2 * MM) -> MirrorLens:
+    """random_lens(seed) with N ~ U[n_range] elements in all, the last ~10 %
+    (at least 24) on a mirror plate: bore radius half the narrowest tube's, the
+    same 0.5 mm cap, `plate` thick, `mirror_gap` after the last tube, at
+    -1.1 x beam_voltage."""
+    rng = np.random.default_rng(seed + 7919)
+    n = int(rng.integers(n_range[0], n_range[1] + 1))
+    n_mirror = max(24, n // 10)
+    geo, volts = random_lens(seed, n_range=(n - n_mirror, n - n_mirror))
+    segs = list(geo.segments)
+    r_min = min(s[2] for s in segs[1::3])  # the tube segments' radius
+    z_lo = min(min(s[1], s[3]) for s in segs)
+    z_hi = max(max(s[1], s[3]) for s in segs)
+    bore, cap = 0.5 * r_min, 0.5 * MM
+    z0 = z_hi + mirror_gap
+    v = aperture_tube(bore, bore + cap, z0, z0 + plate, n_mirror)
+    corners = [(bore + cap, z0), (bore, z0), (bore, z0 + plate), (bore + cap, z0 + plate)]
+    segs += [(a[0], a[1], b[0], b[1]) for a, b in zip(corners[:-1], corners[1:])]
+    counts = list(geo.segment_counts) + tube_counts(bore, bore + cap, z0, z0 + plate, n_mirror)
+    k = len(geo.names)
+    lens = LensGeometry(np.concatenate([geo.vertices, v]), np.concatenate([geo.electrode_index, np.full(len(v), k)]),
+                        list(geo.names) + ['mirror'], segs, counts)
+    z_start = z_lo - 0.5 * MM
+    h = 0.7 * bore
+    bounds = np.array([[-h, h], [-h, h], [z_start - 0.5 * MM, z0 + plate + 1.0 * MM]])
+    return MirrorLens(lens, np.concatenate([volts, [-1.1 * beam_voltage]]), z_start, bounds)
+
+
+def mirror_beam(n: int, seed: int, z0: float, r_max: float = 0.05 * MM, angle_max: float = 50e-3,
+                median_ev: float = 1000.0, sigma: float = 1.0, clip=(100.0, 10000.0)):
+    """The batching workload's beam: electrons at energies lognormal (median
+    1 keV, sigma 1, clipped to [100 eV, 10 keV]) from x = r ~ U[0, r_max],
+    y = 0, z = z0, heading +z at angles ~ U[-50, 50] mrad in the xz-plane."""
+    from scipy.constants import e, m_e
+    rng = np.random.default_rng(seed)
+    energy = np.clip(median_ev * np.exp(sigma * rng.standard_normal(n)), *clip)
+    r = rng.uniform(0.0, r_max, n)
+    ang = rng.uniform(-angle_max, angle_max, n)
+    speed = np.sqrt(2 * energy * e / m_e)[:, None]
+    pos = np.stack([r, np.zeros(n), np.full(n, z0)], axis=1)
+    vel = speed * np.stack([np.sin(ang), np.zeros(n), np.cos(ang)], axis=1)
+    return pos, vel
+
+
 # ---------------------------------------------------------------- combined lens
 # Outline of the iron pole piece of the combined workload's magnetic lens, in
 # (r, z) mm: a closed C-shaped yoke whose bore (r = 2.5 mm) is open over

@@ -260,7 +260,7 @@ def trace_geometries(fields, bounds, positions, velocities, plane_z, mass=m_e, c
     counters = torch.empty((n, 2), dtype=torch.int64, device=dev)
     work = torch.empty(1, dtype=torch.int32, device=dev)
     B._call('tb_trace_rk45_geometries', start.data_ptr(), None, qm.data_ptr(), geom_t.data_ptr(), n, C.byref(f),
-            off_t.data_ptr(), len(fields), C.byref(o), None, None, status.data_ptr(), final.data_ptr(),
+            off_t.data_ptr(), len(fields), None, C.byref(o), None, None, status.data_ptr(), final.data_ptr(),
             plane.data_ptr(), counters.data_ptr(), work.data_ptr(), B._stream())
     out = [a.cpu().numpy() for a in (plane, final, status, counters)]
     cuts = np.cumsum(counts)[:-1]
