@@ -28,6 +28,8 @@ tracer and its axial-series tracer on all host threads.
       pivoted LU and the mixed tensor-core solve (also reported, as
       `precision_solve`, beside the tracer in the default run).
   --workload combined: the combined electro-magnetostatic workload.
+  --workload batch: the batching workload (64 mirror lenses filled, solved
+      and traced with the direct BEM field, one CUDA graph per step).
 
 `value` is whole-job electrons/s with the start states resident in HBM;
 `e2e` is the same through the public API with host arrays over a stream of
@@ -1023,13 +1025,170 @@ def run_combined(args):
     print(json.dumps(line), flush=True)
 
 
+def _batch_judge_init(items):
+    try:
+        os.nice(10)
+    except OSError:
+        pass
+    from oracle.oracle import Oracle
+    _JUDGE.update(oracle=Oracle('port'), items=items)
+
+
+def _batch_judge_one(job):
+    """The oracle's FP64 BEM trace of one particle of geometry g (the GPU
+    solve's charges), returned as its final state (t, x, y, z)."""
+    g, state, atol = job
+    from oracle.oracle import EM
+    q, jac, pos, bounds = _JUDGE['items'][g]
+    t, s = _JUDGE['oracle'].trace_bem(state[:3], state[3:], EM, q, jac, pos, bounds, atol, max_attempts=20000)
+    return (float(t[-1]), float(s[-1, 0]), float(s[-1, 1]), float(s[-1, 2]))
+
+
+def run_batch(args):
+    """--workload batch: the batching workload.  64 mirror lenses (a
+    random_lens stack of 2-5 tubes, radii U[0.5, 3] mm, gaps U[0.2, 1] mm,
+    electrodes U[-5, 5] kV, followed by an aperture-plate mirror at -1.1 kV;
+    N ~ U[500, 6000] elements each) filled, factored and solved in one
+    persistent launch, then 65,536 electrons per lens (lognormal energies,
+    median 1 keV, sigma 1, clipped to [100 eV, 10 keV]; angles U[-50, 50]
+    mrad) traced through the direct BEM field in one more; the two captured as
+    one CUDA graph with launch shapes picked by the autotuner.  A step is one
+    replay of the graph.  Oracle checks: the charges of the smallest lenses
+    against its own fill and LAPACK solve, and a seeded subsample of every
+    lens's electrons traced by the oracle through the GPU charges."""
+    import torch
+    torch.cuda.set_device(dist_info()[2])
+    from traceon_b200 import backend as B
+    from traceon_b200 import geometry as G
+    from traceon_b200 import autotune
+    from traceon_b200.batch import BatchPipeline
+    from traceon_b200.excitation import Excitation, Mesh
+    cores = host_cores()
+    ng, ne = args.batch_geometries, args.batch_electrons
+    lenses = [G.mirror_lens(SEED * 1000 + g) for g in range(ng)]
+    excs, starts = [], []
+    for g, m in enumerate(lenses):
+        exc = Excitation(Mesh.from_geometry(m.geometry))
+        exc.add_voltage(**{n: float(v) for n, v in zip(m.geometry.names, m.voltages)})
+        excs.append(exc)
+        starts.append(G.mirror_beam(ne, SEED * 1000 + 500 + g, m.z_start))
+    Ns = np.array([len(m.geometry) for m in lenses])
+    t0 = time.perf_counter()
+    pipe = BatchPipeline(excs, [s_[0] for s_ in starts], [s_[1] for s_ in starts], [m.bounds for m in lenses],
+                         atol=args.batch_atol, max_attempts=20000)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    tuned = autotune.tune_batch_pipeline(pipe)
+    pipe.batch.launch()
+    pipe.batch.check()  # every lens solved without falling back
+    status_solve = pipe.batch.status.cpu().numpy()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    solve_ms = [timed(pipe.batch.launch) for _ in range(2)]
+    pipe.capture()
+    for _ in range(args.warmup):
+        pipe.replay()
+    torch.cuda.synchronize()
+    with Clocks(0) as clk:
+        ms_list = [timed(pipe.replay) for _ in range(args.steps)]
+    final = pipe.final.cpu().numpy()
+    status = pipe.status.cpu().numpy()
+    counters = pipe.counters.cpu().numpy()
+    value = pipe.n / (np.mean(ms_list) * 1e-3)
+    # how the electrons ended: back out of the entrance (reflected), through
+    # the mirror bore, or out of the side of the box
+    gid = np.repeat(np.arange(ng), pipe.counts)
+    zlo = np.array([m.bounds[2, 0] for m in lenses])[gid]
+    zhi = np.array([m.bounds[2, 1] for m in lenses])[gid]
+    reflected = float(np.mean(final[:, 3] < zlo))
+    through = float(np.mean(final[:, 3] > zhi))
+    # the FP64 rooflines: ring-pair evaluations of the trace, ring potentials of the fill
+    rings = 16 * Ns[gid]
+    pairs = float(np.sum(counters[:, 1] * 6.0 * rings))
+    fp64_peak = measure_fp64_peak(B, torch)
+    trace_ms = float(np.mean(ms_list)) - float(np.mean(solve_ms))
+    acc = {}
+    # charges of the smallest lenses against the oracle's own fill + LAPACK
+    from oracle.oracle import Oracle
+    port = Oracle('port')
+    err = []
+    for g in np.argsort(Ns)[:args.batch_charge_check]:
+        geo = lenses[g].geometry
+        vals = geo.voltages_to_values(lenses[g].voltages)
+        A = port.matrix(geo.vertices, np.ones(len(geo), np.uint8), vals, threads=cores)
+        x = np.linalg.solve(A, vals)
+        got = pipe.batch.charges[g].cpu().numpy()
+        err.append(float(np.max(np.abs(got - x)) / np.max(np.abs(x))))
+    acc['charges_rel_err_vs_oracle'] = {'max': max(err) if err else None, 'lenses': len(err),
+                                        'elements': [int(Ns[g]) for g in np.argsort(Ns)[:args.batch_charge_check]]}
+    if args.batch_check > 0:
+        import multiprocessing as mp
+        items = []
+        for g, s_ in enumerate(pipe.batch.solvers):
+            jac, pos = port.fill_jacobian_buffer_radial(s_.vertices)
+            items.append((pipe.batch.charges[g].cpu().numpy(), jac, pos, lenses[g].bounds))
+        rng = np.random.default_rng(SEED + 77)
+        jobs, where = [], []
+        offs = np.concatenate([[0], np.cumsum(pipe.counts)])
+        start_h = pipe.start.cpu().numpy()
+        for g in range(ng):
+            pick = np.sort(rng.choice(pipe.counts[g], min(args.batch_check, pipe.counts[g]), replace=False))
+            for i in pick:
+                jobs.append((g, start_h[offs[g] + i], args.batch_atol))
+                where.append(offs[g] + i)
+        t1 = time.perf_counter()
+        with mp.get_context('spawn').Pool(max(1, cores), _batch_judge_init, (items,)) as pool:
+            ref = np.array(pool.map(_batch_judge_one, jobs, chunksize=4))
+        got = final[where][:, :4]
+        d_pos = np.max(np.abs(got[:, 1:] - ref[:, 1:]), axis=1) * 1e9
+        d_t = np.abs(got[:, 0] - ref[:, 0]) / np.abs(ref[:, 0])
+        acc['endpoints_vs_oracle'] = {'particles': len(jobs), 'per_lens': args.batch_check,
+                                      'max_nm': float(d_pos.max()), 'p99_nm': float(np.percentile(d_pos, 99)),
+                                      'within_1nm': int(np.sum(d_pos <= 1.0)), 'time_rel_max': float(d_t.max()),
+                                      'oracle_s': time.perf_counter() - t1, 'oracle_workers': max(1, cores),
+                                      'note': 'final state (first point outside the lens box) of the oracle\'s '
+                                              'FP64 RKF45 through the GPU solve\'s charges'}
+    line = {'metric': 'traced electrons/s, batching workload (fill + solve + trace of 64 lenses, one CUDA graph)',
+            'value': value, 'unit': 'electrons/s', 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': float(np.mean(ms_list)), 'higher_is_better': True, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': f'{ng} mirror lenses, N ~ U[500, 6000] (sum {int(Ns.sum())}), {ne} electrons '
+                                   f'each (lognormal energies median 1 keV, sigma 1, clipped 100 eV-10 keV; '
+                                   f'+-50 mrad), direct BEM field, RKF45 atol {args.batch_atol:g} m',
+                       'geometries': ng, 'electrons_per_geometry': ne, 'elements_total': int(Ns.sum()),
+                       'elements_min_max': [int(Ns.min()), int(Ns.max())]},
+            'graph': {'launches_per_replay': 2, 'kernels': ['k_batch_solve', 'k_trace_bem'],
+                      'memset_nodes_per_replay': 3},
+            'solve_ms': float(np.mean(solve_ms)), 'trace_ms': trace_ms,
+            'solve_status': {'ok': int(np.sum(status_solve == 0)), 'fallback_lu': int(np.sum(status_solve == 5))},
+            'autotune': tuned,
+            'trace_stats': {'status_exited': int(np.sum(status == 0)), 'max_attempts': int(np.sum(status == 1)),
+                            'reflected_fraction': reflected, 'through_mirror_fraction': through,
+                            'side_exit_fraction': 1.0 - reflected - through,
+                            'attempts_mean': float(counters[:, 1].mean()),
+                            'attempts_p50_p99_max': [float(np.percentile(counters[:, 1], 50)),
+                                                     float(np.percentile(counters[:, 1], 99)),
+                                                     int(counters[:, 1].max())]},
+            'trace_roofline': fp64_roofline(pairs, FLOP_FIELD_PAIR, trace_ms, fp64_peak, 'k_trace_bem',
+                                            'ring-pair field evaluations (+ 1 log, 1 rsqrt, 1 reciprocal each)'),
+            'setup_s': setup_s, 'accuracy': acc, 'clocks': clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='tracer', choices=['tracer', 'solve', 'combined'],
+    ap.add_argument('--workload', default='tracer', choices=['tracer', 'solve', 'combined', 'batch'],
                     help='tracer: the headline metric (default); solve: only the precision-workload solve; '
                          'combined: the combined electro-magnetostatic workload')
     ap.add_argument('--combined-n', type=int, default=16384, help='elements of each part of the combined lens')
@@ -1037,6 +1196,11 @@ def main():
     ap.add_argument('--combined-bem-electrons', type=int, default=2048)
     ap.add_argument('--combined-check', type=int, default=16,
                     help='electrons of the combined workload re-traced by the CPU oracle (~1.5 min each per core)')
+    ap.add_argument('--batch-geometries', type=int, default=64)
+    ap.add_argument('--batch-electrons', type=int, default=65536, help='electrons per lens of the batching workload')
+    ap.add_argument('--batch-atol', type=float, default=1e-8)
+    ap.add_argument('--batch-check', type=int, default=32, help='electrons per lens re-traced by the CPU oracle')
+    ap.add_argument('--batch-charge-check', type=int, default=4, help='smallest lenses solved by the CPU oracle')
     ap.add_argument('--electrons', type=int, default=262144)
     ap.add_argument('--field', default='surrogate', choices=['surrogate', 'bem'])
     ap.add_argument('--bem-electrons', type=int, default=16384, help='slice traced with the plain BEM field')
@@ -1072,6 +1236,8 @@ def main():
         run_solve(args)
     elif args.workload == 'combined':
         run_combined(args)
+    elif args.workload == 'batch':
+        run_batch(args)
     else:
         run_gpu(args)
 

@@ -9,6 +9,11 @@ the launching stream) and keeps the fastest in a process-wide table keyed by
 device and problem size, guarded by a lock (entry points may be called from
 several host threads).
 
+`tune_batch_pipeline` does the same for the batching workload's pipeline:
+the CTAs per SM of the persistent tile-task solve (1 or 2; each CTA holds
+two 64 x 64 FP64 tiles of shared memory) and the BEM team size of the
+multi-geometry trace (on a sample of the batch's particles).
+
 The table is the library's only mutable global state; `clear()` empties it.
 """
 from __future__ import annotations
@@ -79,3 +84,44 @@ def best_team_warps(tracer, start, qm, atol: float, max_attempts: int, rings: in
         _table[key] = best
         _table[key + ('times_ms',)] = times
     return best
+
+
+BATCH_BLOCK_CANDIDATES = (1, 2)
+
+
+def tune_batch_pipeline(pipe, sample: int = 8192) -> dict:
+    """Measured launch shape of a traceon_b200.batch.BatchPipeline: the
+    solve launch timed with every CTAs-per-SM candidate, the trace timed with
+    every team size on `sample` of its particles spread over the batch; the
+    fastest of each is set on `pipe` (before its graph is captured) and kept
+    per device and size bucket (total tiles, rings, particles).  Returns
+    {'blocks_per_sm': b, 'team_warps': tw, 'times_ms': {...}}."""
+    torch = B._torch()
+    bs = pipe.batch
+    tiles = int(sum(p[0] * p[0] for p in bs.plan))
+    key = ('batch_pipeline', torch.cuda.get_device_name(bs.work.device), _bucket(tiles), _bucket(bs.rings),
+           _bucket(pipe.n))
+    with _lock:
+        hit = _table.get(key)
+    if hit is None:
+        t_solve = {}
+        for b in BATCH_BLOCK_CANDIDATES:
+            bs.blocks_per_sm = b
+            t_solve[b] = _time_ms(bs.launch, reps=1)
+        best_b = min(t_solve, key=t_solve.get)
+        bs.blocks_per_sm = best_b
+        bs.launch()  # the sources the trace samples read
+        m = min(sample, pipe.n)
+        idx = torch.linspace(0, pipe.n - 1, m, device=bs.work.device).long()
+        t_trace = {}
+        for tw in TEAM_CANDIDATES:
+            t_trace[tw] = _time_ms(lambda tw=tw: pipe.trace_subset(idx, tw), reps=1)
+        best_tw = min(t_trace, key=t_trace.get)
+        hit = {'blocks_per_sm': best_b, 'team_warps': best_tw,
+               'times_ms': {'solve_by_blocks_per_sm': t_solve, 'trace_sample_by_team_warps': t_trace,
+                            'trace_sample_particles': m}}
+        with _lock:
+            _table[key] = hit
+    bs.blocks_per_sm = hit['blocks_per_sm']
+    pipe.opts.team_warps = hit['team_warps']
+    return hit

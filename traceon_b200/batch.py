@@ -163,6 +163,25 @@ class BatchPipeline:
                 self.gbounds.data_ptr(), C.byref(self.opts), None, None, self.status.data_ptr(),
                 self.final.data_ptr(), None, self.counters.data_ptr(), self.work.data_ptr(), B._stream())
 
+    def trace_subset(self, idx, team_warps: int):
+        """The trace launch on the particles idx (a device index tensor) with
+        the given team size, into scratch outputs: the autotuner's sample."""
+        torch = B._torch()
+        idx = idx.to(self.start.device)
+        st, qm, geom = self.start[idx].contiguous(), self.qm[idx].contiguous(), self.geom[idx].contiguous()
+        m = st.shape[0]
+        status = torch.empty(m, dtype=torch.int32, device=st.device)
+        final = torch.empty((m, 7), dtype=torch.float64, device=st.device)
+        counters = torch.empty((m, 2), dtype=torch.int64, device=st.device)
+        work = torch.empty(1, dtype=torch.int32, device=st.device)
+        o = B.TbTraceOpts.from_buffer_copy(self.opts)
+        o.team_warps = int(team_warps)
+        B._call('tb_trace_rk45_geometries', st.data_ptr(), None, qm.data_ptr(), geom.data_ptr(), m,
+                C.byref(self.field), self.batch.ring_offsets.data_ptr(), len(self.batch), self.gbounds.data_ptr(),
+                C.byref(o), None, None, status.data_ptr(), final.data_ptr(), None, counters.data_ptr(),
+                work.data_ptr(), B._stream())
+        return final
+
     def capture(self):
         """Records enqueue() as a CUDA graph (after one eager run on the
         capture stream, which sets the kernels' attributes)."""
