@@ -301,7 +301,8 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- precision solve
-def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True, fp64_peak=None, check=4096):
+def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True, fp64_peak=None, check=4096,
+                    keep_state=False):
     """The precision workload's charge solve: the three-electrode lens meshed
     to n cubic elements, nrhs right-hand sides with every electrode voltage
     ~U[-3, 3] kV.  GPU FP64 fill (+ singular self terms), then (a) the FP64
@@ -313,8 +314,8 @@ def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True, fp64_
     2,000 z-points; FP64 rooflines of the fill, field and axial kernels
     against `fp64_peak` (TFLOP/s) with the algorithmic flop counts of their
     formulas.  `check` points of the field are re-evaluated by the CPU oracle
-    here (check = 0: the caller runs precision_field_check later on
-    out['_field_state'])."""
+    here; with keep_state the inputs and outputs stay in out['_field_state']
+    for the caller's own precision_field_check instead."""
     import torch
     from traceon_b200 import backend as B
     from traceon_b200.geometry import einzel_lens
@@ -388,8 +389,10 @@ def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True, fp64_
     torch.cuda.empty_cache()
     if field_points:
         out.update(precision_fields(geo, Xm[0], field_points, seed, fp64_peak))
-        if check:
-            out.update(precision_field_check(out.pop('_field_state'), check, host_cores()))
+        if not keep_state:
+            state = out.pop('_field_state')
+            if check:
+                out.update(precision_field_check(state, check, host_cores()))
     out.update(axial_roofline(geo, Xm[0], fp64_peak))
     return out
 
@@ -555,11 +558,19 @@ def time_steps(fn, steps, flush):
 
 
 def timed_launches(fn, steps, flush):
-    """Device time (ms) of each of `steps` calls of fn, each after an L2
-    flush, with one untimed call first; returns (ms list, last result)."""
+    """Device time (ms) of `steps` launches of fn, each after an L2 flush:
+    one eager call, then fn captured as a CUDA graph whose replays are timed
+    (so the host's launch overhead stays out of the short launches); returns
+    (ms list, the captured call's result, refreshed by every replay)."""
+    import torch
     fn()
-    ms, res = time_steps(fn, steps, flush)
-    return ms, res[-1]
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, capture_error_mode='thread_local'):
+        res = fn()
+    ms, _ = time_steps(g.replay, steps, flush)
+    res._graph = g  # the outputs live in the graph's memory pool
+    return ms, res
 
 
 def run_gpu(args):
@@ -789,8 +800,8 @@ def run_gpu(args):
                              '1 reciprocal per pair)',
                 'peak_source': 'FP64 FMA throughput measured in this run (tests/probe tb_probe_fp64_fma)'}
 
-    precision = precision_solve(args.precision_n, fp64_peak=fp64_peak, check=0, field_points=args.field_points) \
-        if args.precision_n > 0 else None
+    precision = precision_solve(args.precision_n, fp64_peak=fp64_peak, field_points=args.field_points,
+                                keep_state=True) if args.precision_n > 0 else None
 
     # ---- accuracy against the CPU oracle (the held-out sample of each beam)
     accuracy = {'checked_against': 'CPU oracle: FP64 fill + QUADPACK diagonal + LAPACK solve on the host, FP64 BEM '
@@ -891,6 +902,12 @@ def run_solve(args):
 COMBINED_VOLTS = (0.0, 3000.0, 0.0)
 
 
+def _log(t0, msg):
+    """A progress line on stderr (seconds since t0), for the long workloads."""
+    sys.stderr.write(f'[{time.perf_counter() - t0:8.1f} s] {msg}\n')
+    sys.stderr.flush()
+
+
 def run_combined(args):
     """--workload combined: the combined electro-magnetostatic workload.  The
     einzel lens meshed to 16,384 elements inside an iron pole piece
@@ -923,8 +940,10 @@ def run_combined(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), r
 
+    T0 = time.perf_counter()
     cl = G.combined_lens(SEED, n_elec=args.combined_n, n_mag=args.combined_n)
     geo = cl.geometry
+    _log(T0, f'combined lens: {len(geo)} elements')
     exc = Excitation(Mesh.from_geometry(geo))
     exc.add_voltage(**{n: v for n, v in zip(geo.names[:3], COMBINED_VOLTS)})
     exc.add_magnetizable(pole=1000.0)
@@ -951,10 +970,13 @@ def run_combined(args):
         fields.append(sv.charges_to_field(EffectivePointCharges(X[0].cpu().numpy(), jac, pos)))
         del A
         torch.cuda.empty_cache()
+        _log(T0, f'{name} system filled and solved: {solve[name]}')
     field = fields[0] + fields[1]
     t0 = time.perf_counter()
     tr = SurrogateTrainer(geo, electrodes=geo.names[:3], magnetizable={'pole': 1000.0}, coils=cl)
+    _log(T0, 'unit fields and axial tables of the 7 sources')
     model, info = tr.train(n_samples=args.train_samples, steps=args.train_steps, batch=8192, seed=0)
+    _log(T0, f'surrogate trained: holdout mse {info["holdout_mse"]:.3g}')
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     strengths = np.concatenate([COMBINED_VOLTS, cl.coil_current])
@@ -969,8 +991,11 @@ def run_combined(args):
         return fs.trace_device(start, qm, G.LENS_BOUNDS, ATOL, plane_z=G.LENS_EXIT_Z, max_attempts=50000)
 
     run()
+    torch.cuda.synchronize()
+    _log(T0, 'first surrogate trace done')
     with Clocks(local) as clk:
         ms, res = time_steps(run, args.steps, flush)
+    _log(T0, f'timed surrogate traces: {np.mean(ms):.1f} ms per step')
     res = res[-1]
     plane = res.plane.cpu().numpy()
     status = res.status.cpu().numpy()
@@ -983,6 +1008,7 @@ def run_combined(args):
                                                         max_attempts=50000), 1, flush)
     pl_b = r_b.plane.cpu().numpy()
     plain = {'value': m / (np.mean(ms_b) * 1e-3), 'electrons': m, 'ms_per_step': float(np.mean(ms_b))}
+    _log(T0, f'plain BEM slice: {plain}')
     acc = {'vs_gpu_bem': endpoint_errors_nm(plane[:m], pl_b[:, 1:3])}
     evals = float(counters[:, 1].sum()) * 6
     peak = read_peaks().get('bf16_tflops') or FALLBACK_BF16_TFLOPS
@@ -1004,6 +1030,7 @@ def run_combined(args):
         with ThreadPoolExecutor(host_cores()) as ex:
             ref = np.array(list(ex.map(one, range(n_c))))
         acc['vs_cpu_oracle'] = endpoint_errors_nm(plane[:n_c], ref)
+        _log(T0, f'oracle traces: {acc["vs_cpu_oracle"]}')
         acc['vs_cpu_oracle_note'] = 'the GPU solve\'s charges traced by the oracle (FP64 BEM, E + B)'
     line = {'metric': 'traced electrons/s at <=1 nm endpoint error, combined electro-magnetostatic lens, '
                       'surrogate (phi, E, B) vs plain BEM field', 'value': value, 'unit': 'electrons/s',

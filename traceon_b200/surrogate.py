@@ -522,38 +522,6 @@ class FieldSurrogate:
 
     def trace_axial_device(self, start, qm, bounds, atol, plane_z=None, max_attempts=100_000, stream=None):
         """The same particles through the axial series of this field's
-        coefficient table alone (FieldRadialAxial's field, radial.c:347-384;
-        the tracer's k_trace_axial), without the network and without the BEM
-        fallback: the method the learned correction improves on.  Returns a
-        TraceResult of device tensors (counters (n, 2))."""
-        from .tracing import TraceResult
-        torch = B._torch()
-        n = start.shape[0]
-        dev = start.device
-        f = B.TbField(None, 0, None, 0, None, 0, None, self.zt.data_ptr(), self.table.data_ptr(), None, len(self.z))
-        o = B.TbTraceOpts()
-        for i, v in enumerate(np.asarray(bounds, dtype=np.float64).reshape(-1)):
-            o.bounds[i] = float(v)
-        o.atol = float(atol)
-        o.plane_z = 0.0 if plane_z is None else float(plane_z)
-        o.record_plane = 0 if plane_z is None else 1
-        o.max_attempts = int(max_attempts)
-        o.max_rows = 0
-        o.team_warps = 0
-        status = torch.empty(n, dtype=torch.int32, device=dev)
-        final = torch.empty((n, 7), dtype=torch.float64, device=dev)
-        plane = torch.empty((n, 7), dtype=torch.float64, device=dev) if plane_z is not None else None
-        counters = torch.empty((n, 2), dtype=torch.int64, device=dev)
-        work = torch.empty(1, dtype=torch.int32, device=dev)
-        B._call('tb_trace_rk45', start.data_ptr(), None, qm.data_ptr(), n, C.byref(f), C.byref(o), None, None,
-                status.data_ptr(), final.data_ptr(), B._ptr(plane), counters.data_ptr(), work.data_ptr(),
-                B._stream() if stream is None else stream)
-        res = TraceResult(status, final, plane, counters)
-        res._keep = (start, qm, work, self)
-        return res
-
-    def trace_axial_device(self, start, qm, bounds, atol, plane_z=None, max_attempts=100_000, stream=None):
-        """The same particles through the axial series of this field's
         coefficient tables alone (FieldRadialAxial's field, radial.c:347-384;
         the tracer's k_trace_axial), without the network and without the BEM
         fallback: the method the learned correction improves on.  Returns a
