@@ -23,7 +23,7 @@ def _excitation(m):
 @pytest.fixture(scope='module')
 def lenses():
     from traceon_b200 import geometry as G
-    return [G.mirror_lens(s, n_range=(40, 900)) for s in range(6)]
+    return [G.mirror_lens(0, n_range=(40, 40))] + [G.mirror_lens(s, n_range=(65, 900)) for s in range(1, 6)]
 
 
 def test_batch_solve_vs_oracle(cuda, port, lenses):
