@@ -633,45 +633,77 @@ __device__ __forceinline__ bool near_segments(const Seg* seg, int nseg, double r
   return nearby;
 }
 
-// Exact BEM field of the electrostatic rings at one point, by one lane, and
-// with MAG the magnetic field H of the magnetostatic charges and current
-// rings (field_radial_traceable, tracing.c:141-163).  Out of line: it is the
-// rare path of the surrogate tracer, and inlined its ring kernels' registers
-// would count against the whole tracer.
+// Raw ring sums of the exact BEM field at (r0, z) over the rings first,
+// first + stride, ...: s[0], s[1] the electrostatic (S_r, S_z) and, with MAG,
+// s[2], s[3] the magnetostatic charges' and s[4], s[5] the current rings'
+// (H_r, H_z) (field_radial_traceable, tracing.c:141-163).  Out of line: it
+// is the rare path of the surrogate tracer, and inlined its ring kernels'
+// registers would count against the whole tracer.
+struct BemSums {
+  double s[6];
+};
+
 template <bool MAG>
-__device__ __noinline__ void bem_point_field(const TraceParams& P, const double* p, double* E, double* H) {
-  double r0 = sqrt(p[0] * p[0] + p[1] * p[1]);
+__device__ __noinline__ BemSums bem_sums(const TraceParams& P, double r0, double z, int first, int stride) {
+  BemSums out;
+  double* s = out.s;
   double Sr = 0, Sz = 0, dummy = 0;
   const double* er = P.esrc;
-  for (int64_t j = 0; j < P.ne; j++) ring_field_acc<false>(r0, p[2], er[j], er[P.ne + j], er[2 * P.ne + j], Sr, Sz, dummy);
+  for (int64_t j = first; j < P.ne; j += stride)
+    ring_field_acc<false>(r0, z, er[j], er[P.ne + j], er[2 * P.ne + j], Sr, Sz, dummy);
+  s[0] = Sr;
+  s[1] = Sz;
+  if (MAG) {
+    double Mr = 0, Mz = 0, Cr = 0, Cz = 0;
+    const double* mr = P.msrc;
+    for (int64_t j = first; j < P.nm; j += stride)
+      ring_field_acc<false>(r0, z, mr[j], mr[P.nm + j], mr[2 * P.nm + j], Mr, Mz, dummy);
+    const double* cr = P.csrc;
+    for (int64_t j = first; j < P.nc; j += stride) {
+      double hr, hz;
+      current_field_ring(r0, z, cr[j], cr[P.nc + j], hr, hz);
+      Cr = fma(cr[2 * P.nc + j], hr, Cr);
+      Cz = fma(cr[2 * P.nc + j], hz, Cz);
+    }
+    s[2] = Mr;
+    s[3] = Mz;
+    s[4] = Cr;
+    s[5] = Cz;
+  } else {
+    s[2] = s[3] = s[4] = s[5] = 0.0;
+  }
+  return out;
+}
+
+// E (and with MAG H) at p from the raw sums of bem_sums.
+template <bool MAG>
+__device__ __forceinline__ void bem_finish(const double* p, double r0, const double* s, double* E, double* H) {
   if (r0 >= MIN_AXIS) {
-    double e = Sr / (2 * PI * r0);
+    double e = s[0] / (2 * PI * r0);
     E[0] = p[0] / r0 * e;
     E[1] = p[1] / r0 * e;
   } else {
     E[0] = E[1] = 0.0;
   }
-  E[2] = -Sz * INV_PI;
+  E[2] = -s[1] * INV_PI;
   if (MAG) {
-    double Mr = 0, Mz = 0, Cr = 0, Cz = 0;
-    const double* mr = P.msrc;
-    for (int64_t j = 0; j < P.nm; j++) ring_field_acc<false>(r0, p[2], mr[j], mr[P.nm + j], mr[2 * P.nm + j], Mr, Mz, dummy);
-    const double* cr = P.csrc;
-    for (int64_t j = 0; j < P.nc; j++) {
-      double hr, hz;
-      current_field_ring(r0, p[2], cr[j], cr[P.nc + j], hr, hz);
-      Cr = fma(cr[2 * P.nc + j], hr, Cr);
-      Cz = fma(cr[2 * P.nc + j], hz, Cz);
-    }
     if (r0 >= MIN_AXIS) {
-      const double h = Mr / (2 * PI * r0) + Cr;
+      const double h = s[2] / (2 * PI * r0) + s[4];
       H[0] = p[0] / r0 * h;
       H[1] = p[1] / r0 * h;
     } else {
       H[0] = H[1] = 0.0;
     }
-    H[2] = -Mz * INV_PI + Cz;
+    H[2] = -s[3] * INV_PI + s[5];
   }
+}
+
+// Exact BEM field at one point, by one lane.
+template <bool MAG>
+__device__ __forceinline__ void bem_point_field(const TraceParams& P, const double* p, double* E, double* H) {
+  const double r0 = sqrt(p[0] * p[0] + p[1] * p[1]);
+  const BemSums s = bem_sums<MAG>(P, r0, p[2], 0, 1);
+  bem_finish<MAG>(p, r0, s.s, E, H);
 }
 
 // Axial series of one coefficient table plus the learned correction
@@ -695,24 +727,46 @@ __device__ __forceinline__ void axial_plus_correction(const TraceParams& P, cons
 // E_r, E_z and, with MAG, H_r, H_z corrections before the envelope): zero
 // outside the field bounds, exact BEM near electrodes and outside the
 // network's domain, else axial series + learned correction.
+constexpr int FIELD_ZERO = 0, FIELD_BEM = 1, FIELD_SURROGATE = 2;
+
+// Which field applies at p: none (not live, or outside the field bounds),
+// the exact BEM sums (near an electrode or outside the network's domain), or
+// the surrogate.
+__device__ __forceinline__ int surrogate_kind(const TraceParams& P, const SurrogateParams& S, const Seg* segs,
+                                              const double* p, double r, bool live) {
+  const double* fb = P.fb;
+  if (!live ||
+      (fb && !(fb[0] < p[0] && p[0] < fb[1] && fb[2] < p[1] && p[1] < fb[3] && fb[4] < p[2] && p[2] < fb[5])))
+    return FIELD_ZERO;
+  const bool out_of_domain = r > S.dom.r_max || p[2] < S.z_lo || p[2] > S.z_hi;
+  if (out_of_domain || near_segments(segs, S.nseg, r, p[2], float(S.fb_dist2))) return FIELD_BEM;
+  return FIELD_SURROGATE;
+}
+
+template <bool MAG>
+__device__ __forceinline__ void surrogate_apply(const TraceParams& P, const SurrogateParams& S, const double* p,
+                                                double r2, double r, const float* c, double* E, double* H);
+
 template <bool MAG>
 __device__ __forceinline__ void surrogate_combine(const TraceParams& P, const SurrogateParams& S,
                                                  const Seg* segs, const double* p, double r2, double r,
                                                  bool live, const float* c, double* E, double* H, bool& used_bem) {
-  used_bem = false;
-  const double* fb = P.fb;
-  if (!live ||
-      (fb && !(fb[0] < p[0] && p[0] < fb[1] && fb[2] < p[1] && p[1] < fb[3] && fb[4] < p[2] && p[2] < fb[5]))) {
+  const int kind = surrogate_kind(P, S, segs, p, r, live);
+  used_bem = kind == FIELD_BEM;
+  if (kind == FIELD_SURROGATE) {
+    surrogate_apply<MAG>(P, S, p, r2, r, c, E, H);
+  } else if (kind == FIELD_BEM) {
+    bem_point_field<MAG>(P, p, E, H);
+  } else {
     E[0] = E[1] = E[2] = 0.0;
     if (MAG) H[0] = H[1] = H[2] = 0.0;
-    return;
   }
-  const bool out_of_domain = r > S.dom.r_max || p[2] < S.z_lo || p[2] > S.z_hi;
-  if (out_of_domain || near_segments(segs, S.nseg, r, p[2], float(S.fb_dist2))) {
-    used_bem = true;
-    bem_point_field<MAG>(P, p, E, H);
-    return;
-  }
+}
+
+// Axial series + learned correction at p, inside the network's domain.
+template <bool MAG>
+__device__ __forceinline__ void surrogate_apply(const TraceParams& P, const SurrogateParams& S, const double* p,
+                                                double r2, double r, const float* c, double* E, double* H) {
   const double rho = r / S.dom.r_max;
   double env = 1.0;
   for (int i = 0; i < S.env_p; i++) env *= rho;
@@ -1180,8 +1234,58 @@ struct TcEngine {
       used_bem = false;
       return false;
     }
-    surrogate_combine<MAG>(P, S, s.segs, p, r2, r, live, c, E, H, used_bem);
+    const int kind = surrogate_kind(P, S, s.segs, p, r, live);
+    used_bem = kind == FIELD_BEM;
+    if (kind == FIELD_SURROGATE) {
+      surrogate_apply<MAG>(P, S, p, r2, r, c, E, H);
+    } else {
+      E[0] = E[1] = E[2] = 0.0;
+      if (MAG) H[0] = H[1] = H[2] = 0.0;
+    }
+    if (any(used_bem)) group_bem(p, used_bem, E, H);
     return true;
+  }
+
+  // The exact field at the points of the group's threads that need it,
+  // summed by all 128 threads together, one point at a time (the rings
+  // strided over the group, warp sums, then the four warps' partials in a
+  // fixed order).  Scratch: the group's activation tile, free between
+  // network evaluations (the last MMA that read it has completed).
+  __device__ __forceinline__ void group_bem(const double* p, bool need, double* E, double* H) {
+    double* sc = reinterpret_cast<double*>(&s.act[g][0][0]);  // [0..2] point, [4..27] partials
+    int* owner = reinterpret_cast<int*>(sc + 3);
+    double* part = sc + 4;
+    const int w = row >> 5, lane = row & 31;
+    bool pending = need;
+    while (any(pending)) {
+      if (row == 0) *owner = 128;
+      asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
+      if (pending) atomicMin(owner, row);
+      asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
+      const int o = *owner;
+      if (row == o) {
+        sc[0] = p[0];
+        sc[1] = p[1];
+        sc[2] = p[2];
+      }
+      asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
+      const double q[3] = {sc[0], sc[1], sc[2]};
+      const double r0 = sqrt(q[0] * q[0] + q[1] * q[1]);
+      const BemSums sums = bem_sums<MAG>(P, r0, q[2], row, 128);
+#pragma unroll
+      for (int k = 0; k < (MAG ? 6 : 2); k++) {
+        const double v = warp_sum(sums.s[k]);
+        if (lane == 0) part[w * 6 + k] = v;
+      }
+      asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
+      if (row == o) {
+        double tot[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) tot[k] = ((part[k] + part[6 + k]) + part[12 + k]) + part[18 + k];
+        bem_finish<MAG>(q, r0, tot, E, H);
+        pending = false;
+      }
+    }
   }
 };
 
