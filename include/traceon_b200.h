@@ -588,6 +588,15 @@ int tb_surrogate_field_points(const double *points, int64_t M, const tb_field_t 
 /* Number of SMs of the current device (grid sizing helper). */
 int tb_num_sms(void);
 
+/* Lookahead of the mixed solve's factorisation (tb_solve_mixed,
+ * tb_lu_nopiv_f32_tc): the trailing update of each 256-column panel is split
+ * into the next panel's columns (on every SM) and the remaining columns, which
+ * run on a second stream on all but reserve_sms SMs while the next panel is
+ * factored on the caller's stream.  0 (the default) turns it off.  One value
+ * per process; returns the previous one.  The factors are the same either
+ * way, bit for bit. */
+int tb_set_solve_lookahead(int reserve_sms);
+
 /* Bound, in SM clock cycles, of the progress waits inside this library's
  * kernels: the tensor-core engines' waits for their MMA chains and copy
  * stages, and the triangular sweeps' waits for blocks other CTAs publish.

@@ -54,6 +54,23 @@ def test_solvers_agree_with_lapack(cuda, n):
     assert _close(X.cpu().numpy(), X_ref) < 1e-10
 
 
+@pytest.mark.parametrize('reserve', [8, 40])
+def test_mixed_solve_lookahead_same_factors(cuda, reserve):
+    """With lookahead (the remaining columns of each trailing update on a
+    second stream beside the next panel's factorisation) the mixed solve
+    returns the same charges, bit for bit, on 3,000 elements (12 panels)."""
+    import torch
+    A, F = _matrix(cuda, 3000)
+    Ft = torch.as_tensor(F, device='cuda')
+    X0, it0, _ = cuda.dev_solve_mixed(A, Ft)
+    old = cuda.set_solve_lookahead(reserve)
+    try:
+        X1, it1, _ = cuda.dev_solve_mixed(A, Ft)
+    finally:
+        cuda.set_solve_lookahead(old)
+    assert it1 == it0 and torch.equal(X0, X1)
+
+
 @pytest.mark.parametrize('nrhs', [1, 9, 16])
 def test_mixed_solve_right_hand_side_counts(cuda, nrhs):
     """1, 9 and 16 (the maximum) right-hand sides against LAPACK on a

@@ -243,8 +243,17 @@ for _name, _args in _DEV.items():
     _f.argtypes = list(_args)
 backend_lib.tb_batch_solve_plan.restype = i64
 backend_lib.tb_batch_solve_plan.argtypes = [vp, C.c_int, vp, C.POINTER(i64)]
+backend_lib.tb_set_solve_lookahead.restype = C.c_int
+backend_lib.tb_set_solve_lookahead.argtypes = [C.c_int]
 backend_lib.tb_set_wait_limit.restype = i64
 backend_lib.tb_set_wait_limit.argtypes = [i64]
+
+
+def set_solve_lookahead(reserve_sms):
+    """SMs the mixed solve leaves to the next panel's factorisation while a
+    second stream runs the rest of each trailing update (0: no lookahead);
+    returns the previous value (tb_set_solve_lookahead)."""
+    return int(backend_lib.tb_set_solve_lookahead(int(reserve_sms)))
 
 
 def set_wait_limit(cycles):

@@ -21,6 +21,8 @@
 #include <cstdint>
 #include <cstring>
 
+#include <atomic>
+#include <mutex>
 #include "tb_common.cuh"
 #include "tb_internal.cuh"
 #include "tb_tc.cuh"
@@ -816,9 +818,7 @@ static int64_t gemm_pre_bytes(int64_t M, int64_t N, int64_t K) {
 
 static bool g_attr_gemm_pre[64];
 
-static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, const float* B, int64_t ldb, int64_t M,
-                        int64_t Nc, int K, uint8_t* work, int* err, cudaStream_t s) {
-  if (M <= 0 || Nc <= 0 || K <= 0) return OK;
+static int gemm_pre_attr() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return CUDA_ERR;
   if (dev >= 0 && dev < 64 && !g_attr_gemm_pre[dev]) {
@@ -827,17 +827,74 @@ static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, cons
       return CUDA_ERR;
     g_attr_gemm_pre[dev] = true;
   }
+  return OK;
+}
+
+// Operands of C (M x Nc) -= A (M x K) B (K x Nc) split into TF32 head / tail
+// blocks in `work` (A blocks first, then B blocks).
+static void gemm_split(const float* A, int64_t lda, const float* B, int64_t ldb, int64_t M, int64_t Nc, int K,
+                       uint8_t* work, cudaStream_t s) {
   const int nk = (K + GT_K - 1) / GT_K;
   const int64_t mbk = (M + GT_M - 1) / GT_M, nbk = (Nc + GT_N - 1) / GT_N;
-  uint8_t* pa = work;
-  uint8_t* pb = work + mbk * nk * (int64_t)PA_BLOCK;
-  k_split_a<<<dim3(unsigned(nk), unsigned(mbk)), 256, 0, s>>>(A, lda, M, K, pa);
-  k_split_b<<<dim3(unsigned(nk), unsigned(nbk)), 256, 0, s>>>(B, ldb, K, Nc, pb);
-  const int64_t ntiles = mbk * nbk;
-  const int64_t grid = ntiles < num_sms() ? ntiles : num_sms();
-  k_gemm_sub_persist<<<unsigned(grid), GQ_THREADS, GQ_SMEM_BYTES, s>>>(C, ldc, pa, pb, M, Nc, nk, nbk, ntiles, err,
-                                                                       wait_limit());
+  k_split_a<<<dim3(unsigned(nk), unsigned(mbk)), 256, 0, s>>>(A, lda, M, K, work);
+  k_split_b<<<dim3(unsigned(nk), unsigned(nbk)), 256, 0, s>>>(B, ldb, K, Nc, work + mbk * nk * (int64_t)PA_BLOCK);
+}
+
+// The update from split operands, restricted to the column blocks
+// [nb0, nb1) of 256 columns, on at most max_ctas CTAs (0: one per SM).
+static int gemm_persist_cols(float* C, int64_t ldc, const uint8_t* work, int64_t M, int64_t Nc, int K, int64_t nb0,
+                             int64_t nb1, int max_ctas, int* err, cudaStream_t s) {
+  const int nk = (K + GT_K - 1) / GT_K;
+  const int64_t mbk = (M + GT_M - 1) / GT_M;
+  const int64_t nbk = (Nc + GT_N - 1) / GT_N;
+  if (nb1 > nbk) nb1 = nbk;
+  if (nb0 >= nb1) return OK;
+  const uint8_t* pa = work;
+  const uint8_t* pb = work + mbk * nk * (int64_t)PA_BLOCK + nb0 * nk * (int64_t)PB_BLOCK;
+  const int64_t ncols = (nb1 == nbk ? Nc : nb1 * GT_N) - nb0 * GT_N;
+  const int64_t nbn = nb1 - nb0, ntiles = mbk * nbn;
+  int64_t grid = max_ctas > 0 && max_ctas < num_sms() ? max_ctas : num_sms();
+  if (grid > ntiles) grid = ntiles;
+  k_gemm_sub_persist<<<unsigned(grid), GQ_THREADS, GQ_SMEM_BYTES, s>>>(C + nb0 * GT_N, ldc, pa, pb, M, ncols, nk, nbn,
+                                                                       ntiles, err, wait_limit());
   return launch_status();
+}
+
+static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, const float* B, int64_t ldb, int64_t M,
+                        int64_t Nc, int K, uint8_t* work, int* err, cudaStream_t s) {
+  if (M <= 0 || Nc <= 0 || K <= 0) return OK;
+  if (gemm_pre_attr() != OK) return CUDA_ERR;
+  gemm_split(A, lda, B, ldb, M, Nc, K, work, s);
+  return gemm_persist_cols(C, ldc, work, M, Nc, K, 0, (Nc + GT_N - 1) / GT_N, 0, err, s);
+}
+
+// Lookahead of the panel factorisation: SMs left free of the trailing update
+// (0: no lookahead).  With lookahead the trailing update of a panel is split:
+// the next panel's 256 columns first, on every SM, then the remaining columns
+// on a second stream with all but this many SMs, while the next panel is
+// factored on the first stream.  Set by tb_set_solve_lookahead.
+static std::atomic<int> g_lookahead{0};
+
+struct SideStream {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+static std::mutex g_side_mutex;
+static SideStream g_side[64];
+
+static int side_stream(SideStream*& out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CUDA_ERR;
+  std::lock_guard<std::mutex> lock(g_side_mutex);
+  SideStream& ss = g_side[dev];
+  if (!ss.side) {
+    if (cudaStreamCreateWithFlags(&ss.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming) != cudaSuccess)
+      return CUDA_ERR;
+  }
+  out = &ss;
+  return OK;
 }
 
 // FP32 LU without pivoting, two-level blocked: panels of 256 columns are
@@ -848,6 +905,11 @@ static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, cons
 // receives 1 if a tensor-core wait ran out.
 constexpr int TC_PANEL = 256;
 static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* work, cudaStream_t s) {
+  const int reserve = g_lookahead.load(std::memory_order_relaxed);
+  SideStream* ss = nullptr;
+  if (reserve > 0 && side_stream(ss) != OK) return CUDA_ERR;
+  if (gemm_pre_attr() != OK) return CUDA_ERR;
+  bool pending = false;  // a remaining-columns update is running on the side stream
   for (int64_t p0 = 0; p0 < N; p0 += TC_PANEL) {
     const int64_t pe = p0 + TC_PANEL < N ? p0 + TC_PANEL : N;
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
@@ -867,6 +929,10 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
     }
     const int64_t rest = N - pe;
     if (rest <= 0) break;
+    if (pending) {  // the row block reads columns the side stream is updating
+      if (cudaStreamWaitEvent(s, ss->join, 0) != cudaSuccess) return CUDA_ERR;
+      pending = false;
+    }
     // row block right of the panel: U12 = L11^-1 A12, 64 rows at a time
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
       const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
@@ -878,10 +944,26 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
         if (st != OK) return st;
       }
     }
-    const int st = gemm_sub_pre(A + pe * lda + pe, lda, A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest,
-                                int(pe - p0), work, err, s);
-    if (st != OK) return st;
+    const int K = int(pe - p0);
+    float* C = A + pe * lda + pe;
+    gemm_split(A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest, K, work, s);
+    const int64_t nbk = (rest + GT_N - 1) / GT_N;
+    if (ss && nbk > 1) {
+      // the next panel's columns on every SM, then the rest beside the next panel's factorisation
+      int st = gemm_persist_cols(C, lda, work, rest, rest, K, 0, 1, 0, err, s);
+      if (st != OK) return st;
+      if (cudaEventRecord(ss->fork, s) != cudaSuccess || cudaStreamWaitEvent(ss->side, ss->fork, 0) != cudaSuccess)
+        return CUDA_ERR;
+      st = gemm_persist_cols(C, lda, work, rest, rest, K, 1, nbk, num_sms() - reserve, err, ss->side);
+      if (st != OK) return st;
+      if (cudaEventRecord(ss->join, ss->side) != cudaSuccess) return CUDA_ERR;
+      pending = true;
+    } else {
+      const int st = gemm_persist_cols(C, lda, work, rest, rest, K, 0, nbk, 0, err, s);
+      if (st != OK) return st;
+    }
   }
+  if (pending && cudaStreamWaitEvent(s, ss->join, 0) != cudaSuccess) return CUDA_ERR;
   return launch_status();
 }
 
@@ -1317,6 +1399,12 @@ extern "C" int tb_lu_nopiv_f32(float* A, int64_t lda, int64_t N, tb_stream_t str
 }
 
 static int64_t round256(int64_t b) { return (b + 255) / 256 * 256; }
+
+extern "C" int tb_set_solve_lookahead(int reserve_sms) {
+  const int prev = g_lookahead.load();
+  g_lookahead.store(reserve_sms > 0 && reserve_sms < num_sms() ? reserve_sms : 0);
+  return prev;
+}
 
 extern "C" int64_t tb_gemm_tf32x3_workspace(int64_t M, int64_t N, int64_t K) {
   if (M <= 0 || N <= 0 || K <= 0) return 0;
