@@ -172,8 +172,10 @@ def test_tc_engine_matches_warp_engine(cuda, trained):
     memory) evaluates the same network as the warp-level mma.sync engine:
     the same fallback decisions, and fields that differ only by FP32
     accumulation order (which can flip BF16 roundings of hidden activations),
-    far below the learned correction itself.  1,000 points: not a multiple of
-    the 128-row tile."""
+    far below the learned correction itself.  At the fallback points the
+    exact BEM sums agree to rounding: the tcgen05 engine sums each such point
+    with its whole 128-thread group, the warp engine with one thread.  1,000
+    points: not a multiple of the 128-row tile."""
     volts = np.array([0.0, 1500.0, 0.0])
     fs_w, axial_only = _fields(trained, volts, 'warp')
     fs_t, _ = _fields(trained, volts, 'tc')
@@ -190,7 +192,7 @@ def test_tc_engine_matches_warp_engine(cuda, trained):
     corr = np.abs(E_w - E_ax)[ok].max()
     assert corr > 0
     assert np.abs(E_t - E_w)[ok].max() < 0.02 * corr
-    assert np.array_equal(E_t[~ok], E_w[~ok])
+    assert np.abs(E_t[~ok] - E_w[~ok]).max() <= 1e-12 * np.abs(E_w[~ok]).max()
 
 
 def test_tc_engine_traces_vs_bem_oracle(cuda, port, trained):
