@@ -810,6 +810,8 @@ __global__ void __launch_bounds__(GQ_THREADS, 1)
   }
 }
 
+static int64_t round256(int64_t b) { return (b + 255) / 256 * 256; }
+
 // Workspace of the pre-split GEMM for an M x N x K update.
 static int64_t gemm_pre_bytes(int64_t M, int64_t N, int64_t K) {
   const int64_t nk = (K + GT_K - 1) / GT_K;
@@ -840,23 +842,27 @@ static void gemm_split(const float* A, int64_t lda, const float* B, int64_t ldb,
   k_split_b<<<dim3(unsigned(nk), unsigned(nbk)), 256, 0, s>>>(B, ldb, K, Nc, work + mbk * nk * (int64_t)PA_BLOCK);
 }
 
-// The update from split operands, restricted to the column blocks
-// [nb0, nb1) of 256 columns, on at most max_ctas CTAs (0: one per SM).
-static int gemm_persist_cols(float* C, int64_t ldc, const uint8_t* work, int64_t M, int64_t Nc, int K, int64_t nb0,
-                             int64_t nb1, int max_ctas, int* err, cudaStream_t s) {
+// The update from split operands, restricted to the row blocks [mb0, mb1)
+// of 128 rows and the column blocks [nb0, nb1) of 256 columns, on at most
+// max_ctas CTAs (0: one per SM).
+static int gemm_persist_part(float* C, int64_t ldc, const uint8_t* work, int64_t M, int64_t Nc, int K, int64_t mb0,
+                             int64_t mb1, int64_t nb0, int64_t nb1, int max_ctas, int* err, cudaStream_t s) {
   const int nk = (K + GT_K - 1) / GT_K;
   const int64_t mbk = (M + GT_M - 1) / GT_M;
   const int64_t nbk = (Nc + GT_N - 1) / GT_N;
+  if (mb1 > mbk) mb1 = mbk;
   if (nb1 > nbk) nb1 = nbk;
-  if (nb0 >= nb1) return OK;
-  const uint8_t* pa = work;
+  if (mb0 >= mb1 || nb0 >= nb1) return OK;
+  const uint8_t* pa = work + mb0 * nk * (int64_t)PA_BLOCK;
   const uint8_t* pb = work + mbk * nk * (int64_t)PA_BLOCK + nb0 * nk * (int64_t)PB_BLOCK;
+  const int64_t nrows = (mb1 == mbk ? M : mb1 * GT_M) - mb0 * GT_M;
   const int64_t ncols = (nb1 == nbk ? Nc : nb1 * GT_N) - nb0 * GT_N;
-  const int64_t nbn = nb1 - nb0, ntiles = mbk * nbn;
+  const int64_t nbn = nb1 - nb0, ntiles = (mb1 - mb0) * nbn;
   int64_t grid = max_ctas > 0 && max_ctas < num_sms() ? max_ctas : num_sms();
   if (grid > ntiles) grid = ntiles;
-  k_gemm_sub_persist<<<unsigned(grid), GQ_THREADS, GQ_SMEM_BYTES, s>>>(C + nb0 * GT_N, ldc, pa, pb, M, ncols, nk, nbn,
-                                                                       ntiles, err, wait_limit());
+  k_gemm_sub_persist<<<unsigned(grid), GQ_THREADS, GQ_SMEM_BYTES, s>>>(C + mb0 * GT_M * ldc + nb0 * GT_N, ldc, pa, pb,
+                                                                       nrows, ncols, nk, nbn, ntiles, err,
+                                                                       wait_limit());
   return launch_status();
 }
 
@@ -865,7 +871,7 @@ static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, cons
   if (M <= 0 || Nc <= 0 || K <= 0) return OK;
   if (gemm_pre_attr() != OK) return CUDA_ERR;
   gemm_split(A, lda, B, ldb, M, Nc, K, work, s);
-  return gemm_persist_cols(C, ldc, work, M, Nc, K, 0, (Nc + GT_N - 1) / GT_N, 0, err, s);
+  return gemm_persist_part(C, ldc, work, M, Nc, K, 0, (M + GT_M - 1) / GT_M, 0, (Nc + GT_N - 1) / GT_N, 0, err, s);
 }
 
 // Lookahead of the panel factorisation: SMs left free of the trailing update
@@ -873,11 +879,16 @@ static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, cons
 // the next panel's 256 columns first, on every SM, then the remaining columns
 // on a second stream with all but this many SMs, while the next panel is
 // factored on the first stream.  Set by tb_set_solve_lookahead.
-static std::atomic<int> g_lookahead{0};
+static std::atomic<int> g_lookahead{-1};  // -1: one SM in six
+
+static int lookahead_reserve() {
+  const int v = g_lookahead.load(std::memory_order_relaxed);
+  return v < 0 ? num_sms() / 6 : v;
+}
 
 struct SideStream {
   cudaStream_t side = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaEvent_t fork = nullptr, top = nullptr, bottom = nullptr;
 };
 static std::mutex g_side_mutex;
 static SideStream g_side[64];
@@ -890,7 +901,8 @@ static int side_stream(SideStream*& out) {
   if (!ss.side) {
     if (cudaStreamCreateWithFlags(&ss.side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&ss.top, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ss.bottom, cudaEventDisableTiming) != cudaSuccess)
       return CUDA_ERR;
   }
   out = &ss;
@@ -905,11 +917,21 @@ static int side_stream(SideStream*& out) {
 // receives 1 if a tensor-core wait ran out.
 constexpr int TC_PANEL = 256;
 static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* work, cudaStream_t s) {
-  const int reserve = g_lookahead.load(std::memory_order_relaxed);
+  const int reserve = lookahead_reserve();
   SideStream* ss = nullptr;
   if (reserve > 0 && side_stream(ss) != OK) return CUDA_ERR;
   if (gemm_pre_attr() != OK) return CUDA_ERR;
-  bool pending = false;  // a remaining-columns update is running on the side stream
+  // With lookahead the trailing update of panel p runs in three parts: the
+  // next panel's 256 columns first, on every SM, on the caller's stream;
+  // then, on the side stream with all but `reserve` SMs, the remaining
+  // columns of the next panel's 256 rows (the row block it factors next,
+  // event `top`) and of all rows below (event `bottom`).  The next panel's
+  // column factorisation runs beside `top`, its row block beside `bottom`.
+  // The split operands alternate between two buffers, so a panel's split
+  // never overwrites the operands of an update still running.
+  const int64_t buf_bytes = round256(gemm_pre_bytes(N, N, TC_PANEL));
+  bool top_pending = false, bottom_pending = false;
+  int buf = 0;
   for (int64_t p0 = 0; p0 < N; p0 += TC_PANEL) {
     const int64_t pe = p0 + TC_PANEL < N ? p0 + TC_PANEL : N;
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
@@ -929,9 +951,9 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
     }
     const int64_t rest = N - pe;
     if (rest <= 0) break;
-    if (pending) {  // the row block reads columns the side stream is updating
-      if (cudaStreamWaitEvent(s, ss->join, 0) != cudaSuccess) return CUDA_ERR;
-      pending = false;
+    if (top_pending) {  // the row block reads the columns `top` updates
+      if (cudaStreamWaitEvent(s, ss->top, 0) != cudaSuccess) return CUDA_ERR;
+      top_pending = false;
     }
     // row block right of the panel: U12 = L11^-1 A12, 64 rows at a time
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
@@ -946,24 +968,35 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
     }
     const int K = int(pe - p0);
     float* C = A + pe * lda + pe;
-    gemm_split(A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest, K, work, s);
-    const int64_t nbk = (rest + GT_N - 1) / GT_N;
+    uint8_t* w = work + (ss ? buf * buf_bytes : 0);
+    gemm_split(A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest, K, w, s);
+    if (bottom_pending) {  // the update below reads rows `bottom` updates
+      if (cudaStreamWaitEvent(s, ss->bottom, 0) != cudaSuccess) return CUDA_ERR;
+      bottom_pending = false;
+    }
+    const int64_t mbk = (rest + GT_M - 1) / GT_M, nbk = (rest + GT_N - 1) / GT_N;
     if (ss && nbk > 1) {
-      // the next panel's columns on every SM, then the rest beside the next panel's factorisation
-      int st = gemm_persist_cols(C, lda, work, rest, rest, K, 0, 1, 0, err, s);
+      constexpr int64_t TOP = TC_PANEL / GT_M;  // row blocks of the next panel
+      int st = gemm_persist_part(C, lda, w, rest, rest, K, 0, mbk, 0, 1, 0, err, s);
       if (st != OK) return st;
       if (cudaEventRecord(ss->fork, s) != cudaSuccess || cudaStreamWaitEvent(ss->side, ss->fork, 0) != cudaSuccess)
         return CUDA_ERR;
-      st = gemm_persist_cols(C, lda, work, rest, rest, K, 1, nbk, num_sms() - reserve, err, ss->side);
+      const int ctas = num_sms() - reserve;
+      st = gemm_persist_part(C, lda, w, rest, rest, K, 0, TOP, 1, nbk, ctas, err, ss->side);
       if (st != OK) return st;
-      if (cudaEventRecord(ss->join, ss->side) != cudaSuccess) return CUDA_ERR;
-      pending = true;
+      if (cudaEventRecord(ss->top, ss->side) != cudaSuccess) return CUDA_ERR;
+      st = gemm_persist_part(C, lda, w, rest, rest, K, TOP, mbk, 1, nbk, ctas, err, ss->side);
+      if (st != OK) return st;
+      if (cudaEventRecord(ss->bottom, ss->side) != cudaSuccess) return CUDA_ERR;
+      top_pending = bottom_pending = true;
+      buf ^= 1;
     } else {
-      const int st = gemm_persist_cols(C, lda, work, rest, rest, K, 0, nbk, 0, err, s);
+      const int st = gemm_persist_part(C, lda, w, rest, rest, K, 0, mbk, 0, nbk, 0, err, s);
       if (st != OK) return st;
     }
   }
-  if (pending && cudaStreamWaitEvent(s, ss->join, 0) != cudaSuccess) return CUDA_ERR;
+  if (top_pending && cudaStreamWaitEvent(s, ss->top, 0) != cudaSuccess) return CUDA_ERR;
+  if (bottom_pending && cudaStreamWaitEvent(s, ss->bottom, 0) != cudaSuccess) return CUDA_ERR;
   return launch_status();
 }
 
@@ -1004,7 +1037,7 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
                                                  double* __restrict__ R, int64_t N, int nrhs) {
   constexpr int NR = RPW == 4 ? 8 : 16;
   constexpr int RES_COLS = RPW == 4 ? 512 : 256;  // 32 KB of X per chunk
-  __shared__ double xs[NR][RES_COLS];
+  __shared__ __align__(16) double xs[NR][RES_COLS];
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int64_t row0 = ((int64_t)blockIdx.x * 8 + warp) * RPW;
   double acc[RPW][NR];
@@ -1012,6 +1045,7 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
   for (int q = 0; q < RPW; q++)
 #pragma unroll
     for (int r = 0; r < NR; r++) acc[q][r] = 0.0;
+  const bool vec = (lda % 2) == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0 && row0 + RPW <= N;
   for (int64_t c0 = 0; c0 < N; c0 += RES_COLS) {
     __syncthreads();
     for (int e = threadIdx.x; e < NR * RES_COLS; e += blockDim.x) {
@@ -1019,6 +1053,24 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
       xs[r][c] = (r < nrhs && c0 + c < N) ? X[(int64_t)r * N + c0 + c] : 0.0;
     }
     __syncthreads();
+    if (vec && c0 + RES_COLS <= N) {
+      // a whole chunk of the warp's rows: two columns per lane and 16-byte
+      // loads, every load of the chunk independent of the others (enough
+      // bytes in flight to keep HBM busy)
+#pragma unroll
+      for (int c = 2 * lane; c < RES_COLS; c += 64) {
+        double2 a[RPW];
+#pragma unroll
+        for (int q = 0; q < RPW; q++) a[q] = *reinterpret_cast<const double2*>(A + (row0 + q) * lda + c0 + c);
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+          const double2 x = *reinterpret_cast<const double2*>(&xs[r][c]);
+#pragma unroll
+          for (int q = 0; q < RPW; q++) acc[q][r] = fma(a[q].y, x.y, fma(a[q].x, x.x, acc[q][r]));
+        }
+      }
+      continue;
+    }
     // the warp's rows interleaved: RPW independent loads per column, and each
     // staged x value read once for all of them
 #pragma unroll 4
@@ -1398,11 +1450,10 @@ extern "C" int tb_lu_nopiv_f32(float* A, int64_t lda, int64_t N, tb_stream_t str
   return lu_nopiv<float>(A, lda, N, (cudaStream_t)stream);
 }
 
-static int64_t round256(int64_t b) { return (b + 255) / 256 * 256; }
 
 extern "C" int tb_set_solve_lookahead(int reserve_sms) {
-  const int prev = g_lookahead.load();
-  g_lookahead.store(reserve_sms > 0 && reserve_sms < num_sms() ? reserve_sms : 0);
+  const int prev = lookahead_reserve();
+  g_lookahead.store(reserve_sms < 0 ? -1 : (reserve_sms < num_sms() ? reserve_sms : 0));
   return prev;
 }
 
@@ -1413,7 +1464,7 @@ extern "C" int64_t tb_gemm_tf32x3_workspace(int64_t M, int64_t N, int64_t K) {
 
 extern "C" int64_t tb_lu_nopiv_f32_tc_workspace(int64_t N) {
   if (N <= 0) return 0;
-  return gemm_pre_bytes(N, N, TC_PANEL);
+  return 2 * round256(gemm_pre_bytes(N, N, TC_PANEL));  // two alternating split-operand buffers
 }
 
 extern "C" int tb_lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, void* work, int64_t work_bytes, int* err,
