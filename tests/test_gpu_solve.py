@@ -54,10 +54,10 @@ def test_solvers_agree_with_lapack(cuda, n):
     assert _close(X.cpu().numpy(), X_ref) < 1e-10
 
 
-@pytest.mark.parametrize('reserve', [8, 40])
+@pytest.mark.parametrize('reserve', [0, 8, 40])
 def test_mixed_solve_lookahead_same_factors(cuda, reserve):
-    """With lookahead (the remaining columns of each trailing update on a
-    second stream beside the next panel's factorisation) the mixed solve
+    """Lookahead (the rest of each trailing update on a second stream beside
+    the next panel's factorisation; on by default) or none: the mixed solve
     returns the same charges, bit for bit, on 3,000 elements (12 panels)."""
     import torch
     A, F = _matrix(cuda, 3000)
