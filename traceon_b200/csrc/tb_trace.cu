@@ -1114,10 +1114,8 @@ __device__ void tc_load_network(TcSmem& s, const __nv_bfloat16* __restrict__ wb,
 __device__ __forceinline__ void tc_issue_layer(const TcSmem& s, uint32_t act, uint32_t dtm, int layer) {
   constexpr uint32_t ID128 = tc::idesc_bf16_f32(128, 128);
   constexpr uint32_t IDOUT = tc::idesc_bf16_f32(128, MLP_OUT);
-  // every layer accumulates onto its bias, stored in the accumulator columns
-  // beforehand (tc_store_bias)
   if (layer == 0) {
-    tc::mma_bf16(dtm, tc::desc_sw128(act), tc::desc_sw128(tc::smem_u32(s.w1)), ID128, 1u);
+    tc::mma_bf16(dtm, tc::desc_sw128(act), tc::desc_sw128(tc::smem_u32(s.w1)), ID128, 0u);
     return;
   }
   const uint32_t wbase = layer < 4 ? tc::smem_u32(s.wh[layer - 1][0]) : tc::smem_u32(s.w5[0]);
@@ -1127,24 +1125,8 @@ __device__ __forceinline__ void tc_issue_layer(const TcSmem& s, uint32_t act, ui
   for (int kk = 0; kk < 8; kk++) {
     const uint32_t ka = (kk >> 2) * TC_ATOM + (kk & 3) * 32;
     const uint32_t kb = (kk >> 2) * watom + (kk & 3) * 32;
-    tc::mma_bf16(dtm, tc::desc_sw128(act + ka), tc::desc_sw128(wbase + kb), id, 1u);
+    tc::mma_bf16(dtm, tc::desc_sw128(act + ka), tc::desc_sw128(wbase + kb), id, kk > 0 ? 1u : 0u);
   }
-}
-
-// Columns 16 c .. 16 c + 15 of this warp's lanes of the accumulator set to
-// the bias values b[16 c ..] (the same in every lane), so that the layer's
-// MMA chain accumulates onto them.
-__device__ __forceinline__ void tc_store_bias(uint32_t tld, const float* b, int c) {
-  uint32_t v[16];
-#pragma unroll
-  for (int j = 0; j < 16; j += 4) {
-    const float4 f = *reinterpret_cast<const float4*>(b + 16 * c + j);
-    v[j] = __float_as_uint(f.x);
-    v[j + 1] = __float_as_uint(f.y);
-    v[j + 2] = __float_as_uint(f.z);
-    v[j + 3] = __float_as_uint(f.w);
-  }
-  tc::tmem_st16(tld + 16 * c, v);
 }
 
 // One group's view of the engine.
@@ -1166,9 +1148,6 @@ struct TcEngine {
   // strengths into c (contract_outputs); all 128 threads of the group call
   // it together.  False (group-uniform) if an MMA wait ran out.
   __device__ __forceinline__ bool forward(const float* feat, float* c) {
-#pragma unroll
-    for (int ch = 0; ch < 8; ch++) tc_store_bias(tld, s.b1, ch);
-    tc::tmem_wait_st();
     tc::st_shared_v4(act + tc::sw128(row, 0), pack_bf16(feat[0], feat[1]), pack_bf16(feat[2], feat[3]),
                      pack_bf16(feat[4], feat[5]), pack_bf16(feat[6], feat[7]));
     tc::st_shared_v4(act + tc::sw128(row, 1), pack_bf16(feat[8], feat[9]), pack_bf16(feat[10], feat[11]),
@@ -1195,12 +1174,10 @@ struct TcEngine {
       phase ^= 1u;
       tc::fence_after_sync();
       if (layer < 4) {
-        // the next layer's bias, stored into each chunk's columns once read
-        const float* next_bias = layer < 3 ? s.bh[layer] : s.b5;
-        const int next_chunks = layer < 3 ? 8 : MLP_OUT / 16;
+        const float* bias = layer == 0 ? s.b1 : s.bh[layer - 1];
         // 16 columns at a time, the TMEM load of the next chunk in flight
         // while this one is processed.  The staged weights and biases of
-        // these layers are pre-scaled by 1/2 (exact), so the accumulator is
+        // these layers are pre-scaled by 1/2 (exact), so acc + bias is
         // h = z / 2 and silu(z) = h + h tanh(h).
         uint32_t va[16], vb[16];
         tc::tmem_ld16(tld, va);
@@ -1213,15 +1190,14 @@ struct TcEngine {
           uint32_t q[8];
 #pragma unroll
           for (int j = 0; j < 8; j++)
-            q[j] = silu2_bf16_half(__uint_as_float(cur[2 * j]), __uint_as_float(cur[2 * j + 1]));
-          if (c < next_chunks) tc_store_bias(tld, next_bias, c);
+            q[j] = silu2_bf16_half(__uint_as_float(cur[2 * j]) + bias[16 * c + 2 * j],
+                                   __uint_as_float(cur[2 * j + 1]) + bias[16 * c + 2 * j + 1]);
           // next layer's K = 16c .. 16c + 15: atom c / 4, chunks 2 (c % 4), 2 (c % 4) + 1
           const uint32_t base = act + (c >> 2) * TC_ATOM;
           tc::st_shared_v4(base + tc::sw128(row, 2 * (c & 3)), q[0], q[1], q[2], q[3]);
           tc::st_shared_v4(base + tc::sw128(row, 2 * (c & 3) + 1), q[4], q[5], q[6], q[7]);
           if (c < 7) tc::tmem_wait_ld16(nxt);
         }
-        tc::tmem_wait_st();
       } else {
         // the MLP_OUT outputs 16 columns at a time, contracted as they come
         c[0] = c[1] = 0.f;
@@ -1234,7 +1210,7 @@ struct TcEngine {
 #pragma unroll
           for (int j = 0; j < 16; j++) {
             const int o = 16 * hc + j;
-            const float y = __uint_as_float(v[j]);
+            const float y = __uint_as_float(v[j]) + s.b5[o];
             c[0] = fmaf(S.wr[o], y, c[0]);
             c[1] = fmaf(S.wz[o], y, c[1]);
             if (MAG) {
