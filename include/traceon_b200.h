@@ -592,9 +592,10 @@ int tb_num_sms(void);
  * tb_lu_nopiv_f32_tc): the trailing update of each 256-column panel is split
  * into the next panel's columns (on every SM) and the remaining columns, which
  * run on a second stream on all but reserve_sms SMs while the next panel is
- * factored on the caller's stream.  0 (the default) turns it off.  One value
- * per process; returns the previous one.  The factors are the same either
- * way, bit for bit. */
+ * factored on the caller's stream.  Default: one SM in five; 0 turns it
+ * off, a negative value restores the default.  One value per process;
+ * returns the previous one.  The factors are the same either way, bit for
+ * bit. */
 int tb_set_solve_lookahead(int reserve_sms);
 
 /* Bound, in SM clock cycles, of the progress waits inside this library's

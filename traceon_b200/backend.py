@@ -251,8 +251,9 @@ backend_lib.tb_set_wait_limit.argtypes = [i64]
 
 def set_solve_lookahead(reserve_sms):
     """SMs the mixed solve leaves to the next panel's factorisation while a
-    second stream runs the rest of each trailing update (0: no lookahead);
-    returns the previous value (tb_set_solve_lookahead)."""
+    second stream runs the rest of each trailing update (0: no lookahead, a
+    negative value: the default, one SM in five); returns the previous value
+    (tb_set_solve_lookahead)."""
     return int(backend_lib.tb_set_solve_lookahead(int(reserve_sms)))
 
 

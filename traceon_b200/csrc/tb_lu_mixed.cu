@@ -879,11 +879,11 @@ static int gemm_sub_pre(float* C, int64_t ldc, const float* A, int64_t lda, cons
 // the next panel's 256 columns first, on every SM, then the remaining columns
 // on a second stream with all but this many SMs, while the next panel is
 // factored on the first stream.  Set by tb_set_solve_lookahead.
-static std::atomic<int> g_lookahead{-1};  // -1: one SM in six
+static std::atomic<int> g_lookahead{-1};  // -1: one SM in five
 
 static int lookahead_reserve() {
   const int v = g_lookahead.load(std::memory_order_relaxed);
-  return v < 0 ? num_sms() / 6 : v;
+  return v < 0 ? num_sms() / 5 : v;
 }
 
 struct SideStream {
@@ -1375,11 +1375,10 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
     const int r = RPT * grp + u;
     if (r < nrhs && row < N) X[(int64_t)r * N + row] = s_fail ? nan : y[u];
   }
+  // the barrier orders every thread's stores before thread 0's release
+  // (st.release is a release pattern at GPU scope: fence.acq_rel + store)
   __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    st_release(flags + b, epoch);
-  }
+  if (threadIdx.x == 0) st_release(flags + b, epoch);
 }
 
 // X[r, j] += c[j] D[r, j]; also, per right-hand side r, the largest
