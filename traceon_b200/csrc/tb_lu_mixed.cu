@@ -1111,8 +1111,12 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
 // waits; the step that gates the next block is one 64 x 64 FP64
 // matrix-vector product with the freshly published x_g.  D_b and M_b are
 // computed once per factorisation (k_diag_inverse) in FP64 from the FP32
-// factor values.  Published blocks: solution to X, then flags[b] = epoch
-// (release / acquire).  A CTA's place in the chain is the ticket it draws
+// factor values.  Published blocks: the sweep writes its solution into an
+// output vector that was filled with a sentinel bit pattern (all bytes 0xFF,
+// a NaN no arithmetic produces) before the launch; a consumer polls the
+// values of the block it needs until none is the sentinel (relaxed GPU-scope
+// stores and loads, each value single-copy atomic), so no flag, fence or
+// second read of the data sits on the chain.  A CTA's place in the chain is the ticket it draws
 // from a counter when it starts (not its block index), so it only ever
 // waits on CTAs that are already running, whatever order the hardware
 // starts them in.  Waits are bounded (the library's wait limit): when one
@@ -1127,6 +1131,17 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 }
 __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Sweep outputs: relaxed GPU-scope 8-byte accesses (single-copy atomic, and
+// never served from a stale L1 line).
+constexpr long long SWEEP_SENTINEL = -1LL;  // all bytes 0xFF
+__device__ __forceinline__ double ld_relaxed_f64(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_f64(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
 }
 
 // Bounded wait of one thread for flags[j] == epoch; false (and err set) when
@@ -1220,9 +1235,10 @@ __global__ void __launch_bounds__(TS_B) k_diag_inverse(const float* __restrict__
 // order), and owns right-hand sides NR/4 grp .. NR/4 grp + NR/4 - 1 of row i
 // in the two matrix-vector products.  Dynamic shared memory: D_b, M_b
 // (64 KB) and the column groups' partial sums (NR * 2 KB).
-// flags[blk] == epoch marks a published block; flags[nblk] is the ticket
-// counter (every launch of a solve draws nblk tickets, so the launch of
-// epoch e draws (e - 1) nblk .. e nblk - 1).
+// In holds the right-hand sides, Out (sentinel-filled) receives the
+// solution.  flags[nblk] is the ticket counter (every launch of a solve
+// draws nblk tickets, so the launch of epoch e draws (e - 1) nblk ..
+// e nblk - 1).
 template <int NR>
 constexpr int sweep_dyn_bytes() {
   return 2 * TS_B * TS_B * int(sizeof(double)) + 4 * NR * TS_B * int(sizeof(double));
@@ -1231,8 +1247,9 @@ constexpr int sweep_dyn_bytes() {
 template <bool LOWER, int NR>
 __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__ LU, int64_t lda, int64_t N,
                                                    const double* __restrict__ Dinv, const double* __restrict__ Mla,
-                                                   double* __restrict__ X, int nrhs, int* __restrict__ flags,
-                                                   int epoch, int* __restrict__ err, long long wait_cycles) {
+                                                   const double* __restrict__ In, double* __restrict__ Out, int nrhs,
+                                                   int* __restrict__ flags, int epoch, int* __restrict__ err,
+                                                   long long wait_cycles) {
   extern __shared__ __align__(16) double sw_dyn[];
   double* Ds = sw_dyn;                    // D_b, column-major
   double* Ms = sw_dyn + TS_B * TS_B;      // M_b, column-major
@@ -1259,7 +1276,7 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
   }
   for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
     const int r = e / TS_B, c = e % TS_B;
-    rs[r][c] = (r < nrhs && b0 + c < N) ? X[(int64_t)r * N + b0 + c] : 0.0;
+    rs[r][c] = (r < nrhs && b0 + c < N) ? In[(int64_t)r * N + b0 + c] : 0.0;
   }
   if (threadIdx.x == 0) s_fail = 0;
   __syncthreads();
@@ -1286,21 +1303,40 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
       for (int c = 0; c < 16; c++) lv[c] = (row < N && j0 + c < N) ? LU[row * lda + j0 + c] : 0.f;
     }
   };
-  auto load_x = [&](int64_t j0) {  // published by another CTA: read via L2
-    for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
-      const int r = e / TS_B, c = e % TS_B;
-      xs[r][c] = (r < nrhs && j0 + c < N) ? __ldcg(X + (int64_t)r * N + j0 + c) : 0.0;
+  // A block published by another CTA, polled until none of its values is the
+  // sentinel (every thread of the CTA calls it; false if the bounded wait ran
+  // out, after which s_fail is set).  Ends with the values in xs.
+  auto poll_x = [&](int64_t j0, unsigned max_ns) -> bool {
+    const long long t0 = clock64();
+    unsigned ns = 32;
+    for (;;) {
+      bool ready = true;
+      for (int e = threadIdx.x; e < NR * TS_B; e += blockDim.x) {
+        const int r = e / TS_B, c = e % TS_B;
+        double v = 0.0;
+        if (r < nrhs && j0 + c < N) {
+          v = ld_relaxed_f64(Out + (int64_t)r * N + j0 + c);
+          ready = ready && __double_as_longlong(v) != SWEEP_SENTINEL;
+        }
+        xs[r][c] = v;
+      }
+      if (__syncthreads_and(ready)) return true;
+      if (threadIdx.x == 0 && clock64() - t0 > wait_cycles) {
+        atomicExch(err, 1);
+        s_fail = 1;
+      }
+      __syncthreads();
+      if (s_fail) return false;
+      __nanosleep(ns);
+      ns = ns < max_ns ? 2 * ns : max_ns;
     }
   };
   const int nacc = q > 0 ? q - 1 : 0;  // tiles accumulated before the gate
   if (nacc > 0) load_lu(LOWER ? 0 : nblk - 1);
   for (int t = 0; t < nacc; t++) {
     const int j = LOWER ? t : nblk - 1 - t;  // finished blocks in publication order
-    if (threadIdx.x == 0 && !wait_flag(flags, j, epoch, err, 256, wait_cycles)) s_fail = 1;
-    __syncthreads();  // also: every thread is done with the previous tile's xs
-    if (s_fail) break;
-    load_x((int64_t)j * TS_B);
-    __syncthreads();
+    __syncthreads();  // every thread is done with the previous tile's xs
+    if (!poll_x((int64_t)j * TS_B, 256)) break;
     float lc[16];
 #pragma unroll
     for (int c = 0; c < 16; c++) lc[c] = lv[c];
@@ -1348,11 +1384,8 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
   // the gate: x_b = y_b - M_b x_g
   if (q > 0) {
     const int g = LOWER ? b - 1 : b + 1;
-    if (threadIdx.x == 0 && !s_fail && !wait_flag(flags, g, epoch, err, 64, wait_cycles)) s_fail = 1;
-    __syncthreads();
-    if (!s_fail) {
-      load_x((int64_t)g * TS_B);
-      __syncthreads();
+    __syncthreads();  // every thread is done with the previous tile's xs
+    if (!s_fail && poll_x((int64_t)g * TS_B, 64)) {
       double z0[RPT], z1[RPT];
 #pragma unroll
       for (int u = 0; u < RPT; u++) z0[u] = z1[u] = 0.0;
@@ -1373,12 +1406,8 @@ __global__ void __launch_bounds__(256, 2) k_trsv_sweep(const float* __restrict__
 #pragma unroll
   for (int u = 0; u < RPT; u++) {
     const int r = RPT * grp + u;
-    if (r < nrhs && row < N) X[(int64_t)r * N + row] = s_fail ? nan : y[u];
+    if (r < nrhs && row < N) st_relaxed_f64(Out + (int64_t)r * N + row, s_fail ? nan : y[u]);
   }
-  // the barrier orders every thread's stores before thread 0's release
-  // (st.release is a release pattern at GPU scope: fence.acq_rel + store)
-  __syncthreads();
-  if (threadIdx.x == 0) st_release(flags + b, epoch);
 }
 
 // X[r, j] += c[j] D[r, j]; also, per right-hand side r, the largest
@@ -1492,10 +1521,10 @@ extern "C" int tb_gemm_sub_tf32x3(float* C, int64_t ldc, const float* A, int64_t
 extern "C" int64_t tb_solve_mixed_workspace(int64_t N, int64_t nrhs) {
   if (N <= 0 || nrhs <= 0) return 0;
   const int64_t nblk = (N + TS_B - 1) / TS_B;
-  // FP32 factors, column scales, correction / residual block, 2 * nrhs
-  // maxima, inverses of the diagonal blocks of both factors and their
-  // lookahead products, sweep flags and the error word
-  return round256(N * N * 4) + round256(N * 8) + round256(nrhs * N * 8) + 256 +
+  // FP32 factors, column scales, correction / residual block, the forward
+  // sweep's output, 2 * nrhs maxima, inverses of the diagonal blocks of both
+  // factors and their lookahead products, sweep flags and the error word
+  return round256(N * N * 4) + round256(N * 8) + 2 * round256(nrhs * N * 8) + 256 +
          4 * round256(nblk * TS_B * TS_B * 8) + round256((nblk + 1) * 4) + 256 +
          round256(tb_lu_nopiv_f32_tc_workspace(N));
 }
@@ -1514,6 +1543,8 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   double* c = reinterpret_cast<double*>(w);
   w += round256(N * 8);
   double* D = reinterpret_cast<double*>(w);
+  w += round256(nrhs * N * 8);
+  double* Y = reinterpret_cast<double*>(w);  // the forward sweep's output
   w += round256(nrhs * N * 8);
   unsigned long long* maxes = reinterpret_cast<unsigned long long*>(w);
   w += 256;
@@ -1564,17 +1595,23 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
     } else {
       k_residual<2><<<unsigned((N + 15) / 16), 256, 0, s>>>(A, lda, X, F, D, N, nr);
     }
-    if (nr <= 8) {
-      k_trsv_sweep<true, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err,
+    // D -> Y (forward, unit lower), Y -> D (backward, upper); each output
+    // filled with the sentinel first
+    const size_t vec_bytes = sizeof(double) * N * nrhs;
+    if (cudaMemsetAsync(Y, 0xff, vec_bytes, s) != cudaSuccess) return CUDA_ERR;
+    if (nr <= 8)
+      k_trsv_sweep<true, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_l, mla_l, D, Y, nr, flags, ++epoch, err,
                                                                   wcyc);
-      k_trsv_sweep<false, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err,
-                                                                  wcyc);
-    } else {
-      k_trsv_sweep<true, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_l, mla_l, D, nr, flags, ++epoch, err,
-                                                                  wcyc);
-      k_trsv_sweep<false, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_u, mla_u, D, nr, flags, ++epoch, err,
-                                                                  wcyc);
-    }
+    else
+      k_trsv_sweep<true, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_l, mla_l, D, Y, nr, flags, ++epoch, err,
+                                                                   wcyc);
+    if (cudaMemsetAsync(D, 0xff, vec_bytes, s) != cudaSuccess) return CUDA_ERR;
+    if (nr <= 8)
+      k_trsv_sweep<false, 8><<<unsigned(nblk), 256, SW8, s>>>(S, N, N, dinv_u, mla_u, Y, D, nr, flags, ++epoch, err,
+                                                                   wcyc);
+    else
+      k_trsv_sweep<false, 16><<<unsigned(nblk), 256, SW16, s>>>(S, N, N, dinv_u, mla_u, Y, D, nr, flags, ++epoch,
+                                                                    err, wcyc);
     if (cudaMemsetAsync(maxes, 0, sizeof(unsigned long long) * 2 * nr, s) != cudaSuccess) return CUDA_ERR;
     {
       const int64_t bx = (N + 255) / 256;
