@@ -1001,99 +1001,173 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
 }
 
 // ---------------------------------------------------------------- mixed solve
-// c[j] = 1 / max_i |A[i, j]| (one block of 8 warps per 32 columns, rows strided over the warps)
-__global__ void k_col_maxabs(const double* __restrict__ A, int64_t lda, int64_t N, double* __restrict__ c) {
-  __shared__ double red[8][32];
-  int64_t j = blockIdx.x * 32 + (threadIdx.x & 31);
-  int w = threadIdx.x / 32;
-  double m = 0.0;
-  if (j < N)
-    for (int64_t i = w; i < N; i += 8) m = fmax(m, fabs(A[i * lda + j]));
-  red[w][threadIdx.x & 31] = m;
+// Column maxima of |A| as the bits of non-negative doubles (which order as
+// unsigned integers): a 2-D grid of column blocks (64 columns, two per lane,
+// 16-byte loads) x row slices, one atomicMax per column and CTA.
+constexpr int CM_SLICES = 16;
+__global__ void __launch_bounds__(256) k_col_maxabs(const double* __restrict__ A, int64_t lda, int64_t N,
+                                                    unsigned long long* __restrict__ maxbits) {
+  __shared__ double red[8][64];
+  const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int64_t j = blockIdx.x * 64 + 2 * lane;
+  const int64_t per = (N + CM_SLICES - 1) / CM_SLICES;
+  const int64_t r0 = blockIdx.y * per, r1 = r0 + per < N ? r0 + per : N;
+  const bool vec = (lda % 2) == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0 && j + 1 < N;
+  double m0 = 0.0, m1 = 0.0;
+  if (vec) {
+#pragma unroll 4
+    for (int64_t i = r0 + w; i < r1; i += 8) {
+      const double2 a = *reinterpret_cast<const double2*>(A + i * lda + j);
+      m0 = fmax(m0, fabs(a.x));
+      m1 = fmax(m1, fabs(a.y));
+    }
+  } else {
+    for (int64_t i = r0 + w; i < r1; i += 8) {
+      if (j < N) m0 = fmax(m0, fabs(A[i * lda + j]));
+      if (j + 1 < N) m1 = fmax(m1, fabs(A[i * lda + j + 1]));
+    }
+  }
+  red[w][2 * lane] = m0;
+  red[w][2 * lane + 1] = m1;
   __syncthreads();
-  if (w == 0 && j < N) {
-    for (int k = 1; k < 8; k++) m = fmax(m, red[k][threadIdx.x & 31]);
-    c[j] = m > 0 ? 1.0 / m : 1.0;
+  if (threadIdx.x < 64) {
+    double m = red[0][threadIdx.x];
+    for (int k = 1; k < 8; k++) m = fmax(m, red[k][threadIdx.x]);
+    const int64_t col = blockIdx.x * 64 + threadIdx.x;
+    if (col < N) atomicMax(maxbits + col, (unsigned long long)__double_as_longlong(m));
   }
 }
 
-// S (float) = A diag(c)
-__global__ void k_scale_to_f32(const double* __restrict__ A, int64_t lda, const double* __restrict__ c,
-                               float* __restrict__ S, int64_t N) {
-  int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (g >= N * N) return;
-  int64_t i = g / N, j = g % N;
-  S[g] = float(A[i * lda + j] * c[j]);
+// c[j] = 1 / max_i |A[i, j]| (1 for a zero column)
+__global__ void k_col_scale(const unsigned long long* __restrict__ maxbits, double* __restrict__ c, int64_t N) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  const double m = __longlong_as_double((long long)maxbits[j]);
+  c[j] = m > 0 ? 1.0 / m : 1.0;
 }
 
-// R[r, i] = F[r, i] - sum_j A[i, j] X[r, j] (nrhs <= 16).  A CTA of 8 warps
-// takes 8 RPW rows; X is staged in shared memory in column chunks and
-// reused by all of them, so X is read N / (8 RPW) times instead of N times
-// and the kernel streams A.
+// S (float) = A diag(c): one CTA per (row, 512-column chunk), two columns
+// per thread with 16-byte loads and 8-byte stores.
+constexpr int SC_COLS = 512;
+__global__ void __launch_bounds__(256) k_scale_to_f32(const double* __restrict__ A, int64_t lda,
+                                                      const double* __restrict__ c, float* __restrict__ S,
+                                                      int64_t N) {
+  const int64_t chunks = (N + SC_COLS - 1) / SC_COLS;
+  const int64_t i = blockIdx.x / chunks, j = (blockIdx.x % chunks) * SC_COLS + 2 * threadIdx.x;
+  if (i >= N || j >= N) return;
+  const double* a = A + i * lda + j;
+  float* o = S + i * N + j;
+  if (j + 1 < N && (lda % 2) == 0 && (N % 2) == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0) {
+    const double2 v = *reinterpret_cast<const double2*>(a);
+    const double2 cc = *reinterpret_cast<const double2*>(c + j);
+    *reinterpret_cast<float2*>(o) = make_float2(float(v.x * cc.x), float(v.y * cc.y));
+  } else {
+    o[0] = float(a[0] * c[j]);
+    if (j + 1 < N) o[1] = float(a[1] * c[j + 1]);
+  }
+}
+
+// R[r, i] = F[r, i] - sum_j A[i, j] X[r, j] (nrhs <= 16), streaming A once.
+// A persistent grid (one CTA of 8 warps per SM) walks groups of 8 RPW rows;
+// X is staged through shared memory in column chunks, double-buffered with
+// cp.async so the next chunk arrives while this one is used, and each
+// staged value serves the RPW rows of a warp.  A full chunk of in-range rows
+// reads two columns per lane with 16-byte loads, all of the chunk's loads
+// independent (enough bytes in flight to keep HBM busy).
 constexpr int MX_MAX_RHS = 16;
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int RPW>
+constexpr int residual_cols() { return RPW == 4 ? 512 : 256; }  // 32 KB of X per chunk
+template <int RPW>
+constexpr int residual_smem() { return 2 * (RPW == 4 ? 8 : 16) * residual_cols<RPW>() * int(sizeof(double)); }
+
 template <int RPW>  // rows per warp: 4 for nrhs <= 8, 2 for nrhs <= 16
-__global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, int64_t lda,
-                                                 const double* __restrict__ X, const double* __restrict__ F,
-                                                 double* __restrict__ R, int64_t N, int nrhs) {
+__global__ void __launch_bounds__(256, 1) k_residual(const double* __restrict__ A, int64_t lda,
+                                                    const double* __restrict__ X, const double* __restrict__ F,
+                                                    double* __restrict__ R, int64_t N, int nrhs) {
   constexpr int NR = RPW == 4 ? 8 : 16;
-  constexpr int RES_COLS = RPW == 4 ? 512 : 256;  // 32 KB of X per chunk
-  __shared__ __align__(16) double xs[NR][RES_COLS];
+  constexpr int RES_COLS = residual_cols<RPW>();
+  extern __shared__ __align__(16) double res_dyn[];  // [2][NR][RES_COLS]
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int64_t row0 = ((int64_t)blockIdx.x * 8 + warp) * RPW;
-  double acc[RPW][NR];
-#pragma unroll
-  for (int q = 0; q < RPW; q++)
-#pragma unroll
-    for (int r = 0; r < NR; r++) acc[q][r] = 0.0;
-  const bool vec = (lda % 2) == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0 && row0 + RPW <= N;
-  for (int64_t c0 = 0; c0 < N; c0 += RES_COLS) {
-    __syncthreads();
+  const bool avec = (lda % 2) == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0;
+  const int64_t nchunk = (N + RES_COLS - 1) / RES_COLS;
+  auto stage = [&](int64_t ch, int buf) {  // chunk ch of X into buffer buf (zeros outside)
+    double* xb = res_dyn + buf * NR * RES_COLS;
+    const int64_t c0 = ch * RES_COLS;
     for (int e = threadIdx.x; e < NR * RES_COLS; e += blockDim.x) {
       const int r = e / RES_COLS, c = e % RES_COLS;
-      xs[r][c] = (r < nrhs && c0 + c < N) ? X[(int64_t)r * N + c0 + c] : 0.0;
+      const bool in = r < nrhs && c0 + c < N;
+      cp_async8(xb + e, in ? X + (int64_t)r * N + c0 + c : X, in ? 8 : 0);
     }
-    __syncthreads();
-    if (vec && c0 + RES_COLS <= N) {
-      // a whole chunk of the warp's rows: two columns per lane and 16-byte
-      // loads, every load of the chunk independent of the others (enough
-      // bytes in flight to keep HBM busy)
+    cp_async_commit_group();
+  };
+  for (int64_t grp = blockIdx.x; grp * 8 * RPW < N; grp += gridDim.x) {
+    const int64_t row0 = (grp * 8 + warp) * RPW;
+    const bool vec = avec && row0 + RPW <= N;
+    double acc[RPW][NR];
 #pragma unroll
-      for (int c = 2 * lane; c < RES_COLS; c += 64) {
-        double2 a[RPW];
+    for (int q = 0; q < RPW; q++)
 #pragma unroll
-        for (int q = 0; q < RPW; q++) a[q] = *reinterpret_cast<const double2*>(A + (row0 + q) * lda + c0 + c);
+      for (int r = 0; r < NR; r++) acc[q][r] = 0.0;
+    __syncthreads();  // the previous group is done with both buffers
+    stage(0, 0);
+    for (int64_t ch = 0; ch < nchunk; ch++) {
+      if (ch + 1 < nchunk) {
+        stage(ch + 1, int((ch + 1) & 1));
+        cp_async_wait_group<1>();
+      } else {
+        cp_async_wait_group<0>();
+      }
+      __syncthreads();
+      const double* xb = res_dyn + (ch & 1) * NR * RES_COLS;
+      const int64_t c0 = ch * RES_COLS;
+      if (vec && c0 + RES_COLS <= N) {
 #pragma unroll
-        for (int r = 0; r < NR; r++) {
-          const double2 x = *reinterpret_cast<const double2*>(&xs[r][c]);
+        for (int c = 2 * lane; c < RES_COLS; c += 64) {
+          double2 a[RPW];
 #pragma unroll
-          for (int q = 0; q < RPW; q++) acc[q][r] = fma(a[q].y, x.y, fma(a[q].x, x.x, acc[q][r]));
+          for (int q = 0; q < RPW; q++) a[q] = *reinterpret_cast<const double2*>(A + (row0 + q) * lda + c0 + c);
+#pragma unroll
+          for (int r = 0; r < NR; r++) {
+            const double2 x = *reinterpret_cast<const double2*>(xb + r * RES_COLS + c);
+#pragma unroll
+            for (int q = 0; q < RPW; q++) acc[q][r] = fma(a[q].y, x.y, fma(a[q].x, x.x, acc[q][r]));
+          }
+        }
+      } else {
+#pragma unroll 4
+        for (int c = lane; c < RES_COLS; c += 32) {
+          if (c0 + c >= N) break;
+          double a[RPW];
+#pragma unroll
+          for (int q = 0; q < RPW; q++) a[q] = row0 + q < N ? A[(row0 + q) * lda + c0 + c] : 0.0;
+#pragma unroll
+          for (int r = 0; r < NR; r++) {
+            const double x = xb[r * RES_COLS + c];
+#pragma unroll
+            for (int q = 0; q < RPW; q++) acc[q][r] = fma(a[q], x, acc[q][r]);
+          }
         }
       }
-      continue;
+      __syncthreads();  // this buffer is staged again two chunks on
     }
-    // the warp's rows interleaved: RPW independent loads per column, and each
-    // staged x value read once for all of them
-#pragma unroll 4
-    for (int c = lane; c < RES_COLS; c += 32) {
-      if (c0 + c >= N) break;
-      double a[RPW];
 #pragma unroll
-      for (int q = 0; q < RPW; q++) a[q] = row0 + q < N ? A[(row0 + q) * lda + c0 + c] : 0.0;
+    for (int q = 0; q < RPW; q++) {
+      const int64_t i = row0 + q;
 #pragma unroll
       for (int r = 0; r < NR; r++) {
-        const double x = xs[r][c];
-#pragma unroll
-        for (int q = 0; q < RPW; q++) acc[q][r] = fma(a[q], x, acc[q][r]);
+        const double v = warp_sum(acc[q][r]);
+        if (lane == 0 && i < N && r < nrhs) R[(int64_t)r * N + i] = F[(int64_t)r * N + i] - v;
       }
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < RPW; q++) {
-    const int64_t i = row0 + q;
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-      const double v = warp_sum(acc[q][r]);
-      if (lane == 0 && i < N && r < nrhs) R[(int64_t)r * N + i] = F[(int64_t)r * N + i] - v;
     }
   }
 }
@@ -1562,8 +1636,15 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   w += 256;
   uint8_t* gemm_work = reinterpret_cast<uint8_t*>(w);  // pre-split operands of the trailing updates
 
-  k_col_maxabs<<<unsigned((N + 31) / 32), 256, 0, s>>>(A, lda, N, c);
-  k_scale_to_f32<<<unsigned((N * N + 255) / 256), 256, 0, s>>>(A, lda, c, S, N);
+  // column maxima (bits gathered in the correction buffer D, N words), scales
+  unsigned long long* maxbits = reinterpret_cast<unsigned long long*>(D);
+  if (cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long) * N, s) != cudaSuccess) return CUDA_ERR;
+  k_col_maxabs<<<dim3(unsigned((N + 63) / 64), CM_SLICES), 256, 0, s>>>(A, lda, N, maxbits);
+  k_col_scale<<<unsigned((N + 255) / 256), 256, 0, s>>>(maxbits, c, N);
+  {
+    const int64_t chunks = (N + SC_COLS - 1) / SC_COLS;
+    k_scale_to_f32<<<unsigned(N * chunks), SC_COLS / 2, 0, s>>>(A, lda, c, S, N);
+  }
   if (cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) return CUDA_ERR;
   int st = lu_nopiv_f32_tc(S, N, N, err, gemm_work, s);
   if (st != OK) return st;
@@ -1571,7 +1652,11 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
   k_diag_inverse<false><<<unsigned(nblk), TS_B, 0, s>>>(S, N, N, dinv_u, mla_u);
   if (cudaMemsetAsync(flags, 0, sizeof(int) * (nblk + 1), s) != cudaSuccess) return CUDA_ERR;
   constexpr int SW8 = sweep_dyn_bytes<8>(), SW16 = sweep_dyn_bytes<16>();
-  if (cudaFuncSetAttribute(k_trsv_sweep<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
+  if (cudaFuncSetAttribute(k_residual<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, residual_smem<4>()) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_residual<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, residual_smem<2>()) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_trsv_sweep<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
       cudaFuncSetAttribute(k_trsv_sweep<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW8) != cudaSuccess ||
       cudaFuncSetAttribute(k_trsv_sweep<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SW16) !=
           cudaSuccess ||
@@ -1590,10 +1675,15 @@ extern "C" int tb_solve_mixed(const double* A, int64_t lda, int64_t N, const dou
     if (it == 1) {
       if (cudaMemcpyAsync(D, F, sizeof(double) * N * nrhs, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
         return CUDA_ERR;
-    } else if (nr <= 8) {
-      k_residual<4><<<unsigned((N + 31) / 32), 256, 0, s>>>(A, lda, X, F, D, N, nr);
     } else {
-      k_residual<2><<<unsigned((N + 15) / 16), 256, 0, s>>>(A, lda, X, F, D, N, nr);
+      // one CTA per SM, at most one per group of rows
+      const int64_t rows = nr <= 8 ? 32 : 16;
+      int64_t grid = (N + rows - 1) / rows;
+      if (grid > num_sms()) grid = num_sms();
+      if (nr <= 8)
+        k_residual<4><<<unsigned(grid), 256, residual_smem<4>(), s>>>(A, lda, X, F, D, N, nr);
+      else
+        k_residual<2><<<unsigned(grid), 256, residual_smem<2>(), s>>>(A, lda, X, F, D, N, nr);
     }
     // D -> Y (forward, unit lower), Y -> D (backward, upper); each output
     // filled with the sentinel first
