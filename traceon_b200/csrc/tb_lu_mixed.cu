@@ -969,18 +969,27 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
     const int K = int(pe - p0);
     float* C = A + pe * lda + pe;
     uint8_t* w = work + (ss ? buf * buf_bytes : 0);
-    gemm_split(A + pe * lda + p0, lda, A + p0 * lda + pe, lda, rest, rest, K, w, s);
+    const int nk = (K + GT_K - 1) / GT_K;
+    const int64_t mbk = (rest + GT_M - 1) / GT_M, nbk = (rest + GT_N - 1) / GT_N;
+    const float* L21 = A + pe * lda + p0;
+    const float* U12 = A + p0 * lda + pe;
+    uint8_t* wb = w + mbk * nk * (int64_t)PA_BLOCK;
+    // split operands: L21 and the next panel's columns of U12 here; the rest
+    // of U12 on the side stream when it runs the rest of the update
+    k_split_a<<<dim3(unsigned(nk), unsigned(mbk)), 256, 0, s>>>(L21, lda, rest, K, w);
+    k_split_b<<<dim3(unsigned(nk), 1u), 256, 0, s>>>(U12, lda, K, rest < GT_N ? rest : GT_N, wb);
     if (bottom_pending) {  // the update below reads rows `bottom` updates
       if (cudaStreamWaitEvent(s, ss->bottom, 0) != cudaSuccess) return CUDA_ERR;
       bottom_pending = false;
     }
-    const int64_t mbk = (rest + GT_M - 1) / GT_M, nbk = (rest + GT_N - 1) / GT_N;
     if (ss && nbk > 1) {
       constexpr int64_t TOP = TC_PANEL / GT_M;  // row blocks of the next panel
       int st = gemm_persist_part(C, lda, w, rest, rest, K, 0, mbk, 0, 1, 0, err, s);
       if (st != OK) return st;
       if (cudaEventRecord(ss->fork, s) != cudaSuccess || cudaStreamWaitEvent(ss->side, ss->fork, 0) != cudaSuccess)
         return CUDA_ERR;
+      k_split_b<<<dim3(unsigned(nk), unsigned(nbk - 1)), 256, 0, ss->side>>>(U12 + GT_N, lda, K, rest - GT_N,
+                                                                          wb + nk * (int64_t)PB_BLOCK);
       const int ctas = num_sms() - reserve;
       st = gemm_persist_part(C, lda, w, rest, rest, K, 0, TOP, 1, nbk, ctas, err, ss->side);
       if (st != OK) return st;
@@ -991,6 +1000,9 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
       top_pending = bottom_pending = true;
       buf ^= 1;
     } else {
+      if (nbk > 1)
+        k_split_b<<<dim3(unsigned(nk), unsigned(nbk - 1)), 256, 0, s>>>(U12 + GT_N, lda, K, rest - GT_N,
+                                                                     wb + nk * (int64_t)PB_BLOCK);
       const int st = gemm_persist_part(C, lda, w, rest, rest, K, 0, mbk, 0, nbk, 0, err, s);
       if (st != OK) return st;
     }
