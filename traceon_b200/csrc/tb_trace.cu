@@ -602,6 +602,7 @@ constexpr int SG_MAX_SEGS = 64;
 // anything that matters for the choice between network and exact field.
 struct Seg {
   float ar, az, ur, uz, il2;
+  float rmin;  // the smallest radius of all segments (the same in every entry)
 };
 
 struct SurrogateSmem {
@@ -612,16 +613,22 @@ struct SurrogateSmem {
 };
 
 __device__ inline void load_segments(Seg* seg, const double* __restrict__ segs, int nseg) {
+  float rmin = 3.0e38f;
+  for (int i = 0; i < nseg; i++) rmin = fminf(rmin, fminf(float(segs[4 * i]), float(segs[4 * i + 2])));
   for (int i = threadIdx.x; i < nseg; i += blockDim.x) {
     const double ar = segs[4 * i], az = segs[4 * i + 1];
     const double ur = segs[4 * i + 2] - ar, uz = segs[4 * i + 3] - az;
     const double L2 = ur * ur + uz * uz;
-    seg[i] = Seg{float(ar), float(az), float(ur), float(uz), L2 > 0 ? float(1.0 / L2) : 0.f};
+    seg[i] = Seg{float(ar), float(az), float(ur), float(uz), L2 > 0 ? float(1.0 / L2) : 0.f, rmin};
   }
 }
 
 __device__ __forceinline__ bool near_segments(const Seg* seg, int nseg, double r_d, double z_d, float d2) {
   const float r = float(r_d), z = float(z_d);
+  if (nseg > 0) {  // inside the innermost radius of all segments, by more than the distance: none is near
+    const float gap = seg[0].rmin - r;
+    if (gap > 0.f && gap * gap > d2) return false;
+  }
   bool nearby = false;
   for (int i = 0; i < nseg; i++) {
     const Seg g = seg[i];
