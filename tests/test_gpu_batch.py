@@ -1,7 +1,8 @@
 """Batched fill of geometries of uneven N (the batching workload's lenses):
 one persistent launch for every off-diagonal entry and one for every self
 term give exactly the single-geometry fills, and solve_direct_batch gives
-the oracle's charges."""
+the oracle's charges; excitations assembled on the device match the host
+assembly."""
 import numpy as np
 import pytest
 
@@ -110,3 +111,23 @@ def test_graded_mesh_on_device(cuda):
     assert np.max(np.abs(v - host)) <= 2.0 ** -35 * 3e-3
     with pytest.raises(ValueError):
         G.mesh_segments_device(seg, [5, 0])
+
+
+def test_excitation_assembled_on_device(cuda):
+    """Excitation.assemble_device gives the host solver's active elements,
+    types and values (a voltage group, a dielectric group, a function group
+    and an inactive group)."""
+    from traceon_b200.excitation import Excitation, Mesh, ExcitationType as ET
+    from traceon_b200.geometry import random_lens
+    from traceon_b200.solver import ElectrostaticSolverRadial
+    geo, volts = random_lens(11, n_range=(400, 400), tubes_range=(4, 4))
+    exc = Excitation(Mesh.from_geometry(geo))
+    exc.add_voltage(**{geo.names[0]: 100.0, geo.names[1]: lambda x, y, z: 3.0 + 0 * z})
+    exc.add_dielectric(**{geo.names[2]: 4.0})
+    verts, types, values = exc.assemble_device('electrostatic')
+    s = ElectrostaticSolverRadial(exc)
+    assert np.array_equal(verts.cpu().numpy(), s.vertices)
+    assert np.array_equal(types.cpu().numpy(), s.excitation_types)
+    v, ref = values.cpu().numpy(), s.excitation_values
+    fun = s.excitation_types == int(ET.VOLTAGE_FUN)
+    assert fun.any() and np.isnan(v[fun]).all() and np.array_equal(v[~fun], ref[~fun])

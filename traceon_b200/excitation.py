@@ -147,6 +147,36 @@ class Excitation:
                  if n in self.excitation_types and type_check(self.excitation_types[n][0])}
         return self.mesh.points[elements[~inactive].astype(np.int64)], names
 
+    def assemble_device(self, type_='electrostatic'):
+        """The active elements of `type_` ('electrostatic' or
+        'magnetostatic') assembled on the device: (vertices (N, 4, 3) float64,
+        excitation types (N,) uint8, values (N,) float64), in the element order
+        of _get_active_elements (traceon/excitation.py:348-373) and with the
+        per-element type and value of traceon/solver.py:46-61 -- a scatter of
+        each named group's type and value over all lines, then one gather of
+        the active lines' points.  VOLTAGE_FUN rows get NaN values (the solver
+        evaluates the functions on the element centres)."""
+        from . import backend as B
+        torch = B._torch()
+        dev = B.device()
+        n = len(self.mesh.lines)
+        types = torch.zeros(n, dtype=torch.uint8, device=dev)
+        values = torch.zeros(n, dtype=torch.float64, device=dev)
+        active = torch.zeros(n, dtype=torch.bool, device=dev)
+        for name, (t, v) in self.excitation_types.items():
+            ok = ExcitationType(t).is_electrostatic() if type_ == 'electrostatic' else \
+                t in (ExcitationType.MAGNETIZABLE, ExcitationType.MAGNETOSTATIC_POT)
+            if not ok:
+                continue
+            idx = torch.as_tensor(np.asarray(self.mesh.physical_to_lines[name], dtype=np.int64), device=dev)
+            active[idx] = True
+            types[idx] = int(t)
+            values[idx] = float('nan') if t == ExcitationType.VOLTAGE_FUN else float(v)
+        sel = torch.nonzero(active).squeeze(1)
+        points = torch.as_tensor(self.mesh.points, dtype=torch.float64, device=dev)
+        lines = torch.as_tensor(self.mesh.lines.astype(np.int64), device=dev)
+        return points[lines[sel]].contiguous(), types[sel].contiguous(), values[sel].contiguous()
+
     def get_electrostatic_active_elements(self):
         return self._get_active_elements('electrostatic')
 
