@@ -163,9 +163,11 @@ class BatchPipeline:
                 self.gbounds.data_ptr(), C.byref(self.opts), None, None, self.status.data_ptr(),
                 self.final.data_ptr(), None, self.counters.data_ptr(), self.work.data_ptr(), B._stream())
 
-    def trace_subset(self, idx, team_warps: int):
+    def trace_subset(self, idx, team_warps: int, max_attempts: int = 2000):
         """The trace launch on the particles idx (a device index tensor) with
-        the given team size, into scratch outputs: the autotuner's sample."""
+        the given team size and attempt cap, into scratch outputs: the
+        autotuner's sample (the cap keeps the few trapped particles from
+        dominating its time)."""
         torch = B._torch()
         idx = idx.to(self.start.device)
         st, qm, geom = self.start[idx].contiguous(), self.qm[idx].contiguous(), self.geom[idx].contiguous()
@@ -176,6 +178,7 @@ class BatchPipeline:
         work = torch.empty(1, dtype=torch.int32, device=st.device)
         o = B.TbTraceOpts.from_buffer_copy(self.opts)
         o.team_warps = int(team_warps)
+        o.max_attempts = min(int(o.max_attempts), int(max_attempts))
         B._call('tb_trace_rk45_geometries', st.data_ptr(), None, qm.data_ptr(), geom.data_ptr(), m,
                 C.byref(self.field), self.batch.ring_offsets.data_ptr(), len(self.batch), self.gbounds.data_ptr(),
                 C.byref(o), None, None, status.data_ptr(), final.data_ptr(), None, counters.data_ptr(),
