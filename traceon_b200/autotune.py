@@ -93,9 +93,9 @@ def tune_batch_pipeline(pipe, sample: int = 4096) -> dict:
     """Measured launch shape of a traceon_b200.batch.BatchPipeline: the
     solve launch timed with every CTAs-per-SM candidate, the trace timed with
     every team size on `sample` of its particles spread over the batch (at
-    most 2,000 attempts each); the
-    fastest of each is set on `pipe` (before its graph is captured) and kept
-    per device and size bucket (total tiles, rings, particles).  Returns
+    most 2,000 attempts each); the fastest of each is set on `pipe` (before
+    its graph is captured) and kept per device and size bucket (total tiles,
+    rings, particles).  Returns
     {'blocks_per_sm': b, 'team_warps': tw, 'times_ms': {...}}."""
     torch = B._torch()
     bs = pipe.batch
