@@ -338,6 +338,7 @@ struct TeamState {
   double y[6];
   double k[6][6];
   double t, h, hmax, qm;
+  double bnd[6];  // many geometries: the particle's bounding box
   int64_t nrow, accepted, attempts;
   int status;
 };
@@ -367,12 +368,19 @@ __device__ void rk45_team(const TraceParams& P, int64_t idx, BemTeamField<TW, GE
     for (int c = 0; c < 7; c++) P.plane[idx * 7 + c] = __longlong_as_double(0x7ff8000000000000LL);
   const double atol = P.atol;
 
-  const double* bounds = GEOM && field.bnd ? field.bnd : P.bounds;
+  if (GEOM)  // the box in the team's shared state (no pointer held in registers)
+    for (int c = 0; c < 6; c++) S->bnd[c] = field.bnd ? field.bnd[c] : P.bounds[c];
   for (;;) {
     {
       double y[6];
       for (int c = 0; c < 6; c++) y[c] = S->y[c];
-      if (!in_bounds(bounds, y)) break;
+      if (GEOM) {
+        double b[6];
+        for (int c = 0; c < 6; c++) b[c] = S->bnd[c];
+        if (!in_bounds(b, y)) break;
+      } else if (!in_bounds(P.bounds, y)) {
+        break;
+      }
     }
     if (S->attempts >= P.max_attempts) {
       S->status = TRACE_MAX_ATTEMPTS;
