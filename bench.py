@@ -1063,12 +1063,15 @@ def _batch_judge_init(items):
 
 def _batch_judge_one(job):
     """The oracle's FP64 BEM trace of one particle of geometry g (the GPU
-    solve's charges), returned as its final state (t, x, y, z)."""
-    g, state, atol = job
-    from oracle.oracle import EM
+    solve's charges): its final state (t, x, y, z) and its position at the
+    GPU trace's final time t_gpu (cubic Hermite between accepted states)."""
+    g, state, atol, t_gpu = job
+    from oracle.oracle import EM, hermite_position_at
     q, jac, pos, bounds = _JUDGE['items'][g]
     t, s = _JUDGE['oracle'].trace_bem(state[:3], state[3:], EM, q, jac, pos, bounds, atol, max_attempts=20000)
-    return (float(t[-1]), float(s[-1, 0]), float(s[-1, 1]), float(s[-1, 2]))
+    p = hermite_position_at(t, s, t_gpu)
+    return (float(t[-1]), float(s[-1, 0]), float(s[-1, 1]), float(s[-1, 2]), float(p[0]), float(p[1]), float(p[2]),
+            len(t))
 
 
 def run_batch(args):
@@ -1169,20 +1172,29 @@ def run_batch(args):
         for g in range(ng):
             pick = np.sort(rng.choice(pipe.counts[g], min(args.batch_check, pipe.counts[g]), replace=False))
             for i in pick:
-                jobs.append((g, start_h[offs[g] + i], args.batch_atol))
+                jobs.append((g, start_h[offs[g] + i], args.batch_atol, float(final[offs[g] + i, 0])))
                 where.append(offs[g] + i)
         t1 = time.perf_counter()
         with mp.get_context('spawn').Pool(max(1, cores), _batch_judge_init, (items,)) as pool:
             ref = np.array(pool.map(_batch_judge_one, jobs, chunksize=4))
         got = final[where][:, :4]
-        d_pos = np.max(np.abs(got[:, 1:] - ref[:, 1:]), axis=1) * 1e9
+        d_pos = np.max(np.abs(got[:, 1:] - ref[:, 1:4]), axis=1) * 1e9
+        d_at = np.max(np.abs(got[:, 1:] - ref[:, 4:7]), axis=1) * 1e9
         d_t = np.abs(got[:, 0] - ref[:, 0]) / np.abs(ref[:, 0])
-        acc['endpoints_vs_oracle'] = {'particles': len(jobs), 'per_lens': args.batch_check,
-                                      'max_nm': float(d_pos.max()), 'p99_nm': float(np.percentile(d_pos, 99)),
-                                      'within_1nm': int(np.sum(d_pos <= 1.0)), 'time_rel_max': float(d_t.max()),
-                                      'oracle_s': time.perf_counter() - t1, 'oracle_workers': max(1, cores),
-                                      'note': 'final state (first point outside the lens box) of the oracle\'s '
-                                              'FP64 RKF45 through the GPU solve\'s charges'}
+        worst = np.argsort(-d_at)[:5]
+        acc['endpoints_vs_oracle'] = {
+            'particles': len(jobs), 'per_lens': args.batch_check,
+            'final_state_max_nm': float(d_pos.max()), 'final_state_p99_nm': float(np.percentile(d_pos, 99)),
+            'final_state_within_1nm': int(np.sum(d_pos <= 1.0)), 'time_rel_max': float(d_t.max()),
+            'at_gpu_time_max_nm': float(d_at.max()), 'at_gpu_time_p99_nm': float(np.percentile(d_at, 99)),
+            'at_gpu_time_within_1nm': int(np.sum(d_at <= 1.0)),
+            'worst': [{'lens': int(jobs[k][0]), 'status': int(status[where[k]]),
+                       'attempts': int(counters[where[k], 1]), 'oracle_states': int(ref[k, 7]),
+                       'time_rel': float(d_t[k]), 'final_state_nm': float(d_pos[k]), 'at_gpu_time_nm': float(d_at[k])}
+                      for k in worst],
+            'oracle_s': time.perf_counter() - t1, 'oracle_workers': max(1, cores),
+            'note': 'the oracle\'s FP64 RKF45 through the GPU solve\'s charges: its final state (first point outside '
+                    'the lens box) and its position at the GPU trace\'s final time'}
     line = {'metric': 'traced electrons/s, batching workload (fill + solve + trace of 64 lenses, one CUDA graph)',
             'value': value, 'unit': 'electrons/s', 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': float(np.mean(ms_list)), 'higher_is_better': True, 'dtype': 'f64', 'data': 'synthetic',

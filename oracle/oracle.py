@@ -458,6 +458,26 @@ def hermite_plane_crossing(times, states, z_plane):
     return None
 
 
+def hermite_position_at(times, states, t):
+    """Position (x, y, z) of a stored trajectory at time t: cubic Hermite
+    interpolation of position between the two accepted states that bracket t
+    (positions and velocities at both ends); beyond the last state, the last
+    interval's polynomial is extended.  Test infrastructure (endpoint checks
+    at equal times)."""
+    times = np.asarray(times)
+    n = len(times)
+    i = int(np.searchsorted(times, t, side='right')) - 1
+    i = min(max(i, 0), n - 2)
+    h = times[i + 1] - times[i]
+    s0, s1 = states[i], states[i + 1]
+    u = (t - times[i]) / h
+    h00 = 2 * u**3 - 3 * u**2 + 1
+    h10 = u**3 - 2 * u**2 + u
+    h01 = -2 * u**3 + 3 * u**2
+    h11 = u**3 - u**2
+    return np.array([h00 * s0[c] + h10 * h * s0[3 + c] + h01 * s1[c] + h11 * h * s1[3 + c] for c in range(3)])
+
+
 def _hermite_root(h, s0, s1, z_plane):
     def pos(u, c):
         h00 = 2 * u**3 - 3 * u**2 + 1

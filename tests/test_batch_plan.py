@@ -178,3 +178,22 @@ def test_tile_algorithm_matches_lapack(port):
     for x, A, F in zip(run_plan_numpy(A_list, F_list, tasks), A_list, F_list):
         x0 = np.linalg.solve(A, F)
         assert np.max(np.abs(x - x0)) / np.max(np.abs(x0)) < 1e-12
+
+
+def test_hermite_position_at_is_exact_for_cubics():
+    """The equal-time endpoint comparison of the batching workload: cubic
+    Hermite interpolation of stored states reproduces any cubic-in-time
+    trajectory, between states and past the last one."""
+    from oracle.oracle import hermite_position_at
+    t = np.array([0.0, 0.3, 0.7, 1.2])
+    a = np.array([[1.0, -2.0, 0.5], [0.2, 0.1, -0.3], [3.0, 0.0, 1.0], [-1.0, 0.5, 0.25]])  # x(t) = sum a_k t^k
+
+    def x(tt):
+        return sum(a[k] * tt**k for k in range(4))
+
+    def v(tt):
+        return sum(k * a[k] * tt**(k - 1) for k in range(1, 4))
+
+    states = np.array([np.concatenate([x(tt), v(tt)]) for tt in t])
+    for tt in (0.0, 0.1, 0.5, 1.0, 1.2, 1.35):
+        assert np.allclose(hermite_position_at(t, states, tt), x(tt), rtol=0, atol=1e-12)
