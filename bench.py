@@ -154,44 +154,44 @@ def oracle_charges(geo, volts, threads):
     return q, jac, pos
 
 
-# The CPU judge of endpoints: the oracle's FP64 BEM trace of each checked
+# Endpoints traced by the CPU oracle: its FP64 BEM trace of each checked
 # electron and its cubic-Hermite crossing of the exit plane, in a pool of
 # spawned processes (no CUDA in them) that runs while the GPU work proceeds.
-_JUDGE = {}
+_ORACLE = {}
 
 
-def _judge_init(q, jac, pos):
+def _oracle_init(q, jac, pos):
     try:
         os.nice(10)  # below the bench's own host thread
     except OSError:
         pass
     from oracle.oracle import Oracle
-    _JUDGE.update(oracle=Oracle('port'), q=q, jac=jac, pos=pos)
+    _ORACLE.update(oracle=Oracle('port'), q=q, jac=jac, pos=pos)
 
 
-def _judge_one(state):
+def _oracle_trace_one(state):
     from oracle.oracle import EM, hermite_plane_crossing
     from traceon_b200 import geometry as G
-    t, s = _JUDGE['oracle'].trace_bem(state[:3], state[3:], EM, _JUDGE['q'], _JUDGE['jac'], _JUDGE['pos'],
+    t, s = _ORACLE['oracle'].trace_bem(state[:3], state[3:], EM, _ORACLE['q'], _ORACLE['jac'], _ORACLE['pos'],
                                       G.LENS_BOUNDS, ATOL)
     h = hermite_plane_crossing(t, s, G.LENS_EXIT_Z)
     return (np.nan, np.nan) if h is None else (float(h[0]), float(h[1]))
 
 
-class OracleJudge:
+class OracleTraces:
     """Exit-plane crossings of electrons traced by the CPU oracle, computed
     asynchronously in `workers` spawned processes."""
 
     def __init__(self, q, jac, pos, workers):
         import multiprocessing as mp
         self.workers = workers
-        self.pool = mp.get_context('spawn').Pool(workers, _judge_init, (q, jac, pos))
+        self.pool = mp.get_context('spawn').Pool(workers, _oracle_init, (q, jac, pos))
         self.jobs = {}
         self.t0 = time.perf_counter()
 
     def submit(self, name, p0, v0):
         states = [np.concatenate([a, b]) for a, b in zip(p0, v0)]
-        self.jobs[name] = self.pool.map_async(_judge_one, states, chunksize=4)
+        self.jobs[name] = self.pool.map_async(_oracle_trace_one, states, chunksize=4)
 
     def result(self, name):
         return np.array(self.jobs[name].get(), dtype=np.float64).reshape(-1, 2)
@@ -582,8 +582,8 @@ def run_gpu(args):
     other = 'narrow' if beam == 'wide' else 'wide'
     geo, volts, p0, v0 = lens_inputs(E, beam, SEED + rank)
     _, _, p0o, v0o = lens_inputs(E, other, SEED + rank + 1000)
-    # ---- the CPU judge starts first and overlaps the GPU work (rank 0)
-    judge = None
+    # ---- the CPU oracle starts first and overlaps the GPU work (rank 0)
+    oracle_pool = None
     n_check = min(args.check, E) if rank == 0 else 0
     n_check_o = min(args.check_other, E) if rank == 0 else 0
     t_or = time.perf_counter()
@@ -591,9 +591,9 @@ def run_gpu(args):
     if n_check or n_check_o or (ws == 1 and args.cpu_seconds > 0):
         q_or, jac_or, pos_or = oracle_charges(geo, volts, cores)
     if n_check or n_check_o:
-        judge = OracleJudge(q_or, jac_or, pos_or, max(1, cores - 1))
-        judge.submit(beam, p0[:n_check], v0[:n_check])
-        judge.submit(other, p0o[:n_check_o], v0o[:n_check_o])
+        oracle_pool = OracleTraces(q_or, jac_or, pos_or, max(1, cores - 1))
+        oracle_pool.submit(beam, p0[:n_check], v0[:n_check])
+        oracle_pool.submit(other, p0o[:n_check_o], v0o[:n_check_o])
     oracle_setup_s = time.perf_counter() - t_or
 
     torch.cuda.set_device(local)
@@ -759,8 +759,8 @@ def run_gpu(args):
             arms[name] = row
 
     if rank != 0:
-        if judge is not None:
-            judge.close()
+        if oracle_pool is not None:
+            oracle_pool.close()
         if ws > 1:
             import torch.distributed as dist
             dist.barrier()
@@ -806,11 +806,11 @@ def run_gpu(args):
     # ---- accuracy against the CPU oracle (the held-out sample of each beam)
     accuracy = {'checked_against': 'CPU oracle: FP64 fill + QUADPACK diagonal + LAPACK solve on the host, FP64 BEM '
                                    'RKF45 trace, cubic-Hermite crossing of the exit plane'}
-    if judge is not None:
+    if oracle_pool is not None:
         for name, n_c in ((beam, n_check), (other, n_check_o)):
             if not n_c:
                 continue
-            ref_xy = judge.result(name)
+            ref_xy = oracle_pool.result(name)
             row = arms.get(name)
             if row is not None:
                 pl_sur, pl_ax = row['_planes']
@@ -818,8 +818,8 @@ def run_gpu(args):
                                         'axial_only': endpoint_errors_nm(pl_ax[:n_c], ref_xy)}
             elif name == beam:
                 accuracy[name] = endpoint_errors_nm(plane[:n_c], ref_xy)
-        accuracy['oracle_wall_s'] = judge.close()
-        accuracy['oracle_workers'] = judge.workers
+        accuracy['oracle_wall_s'] = oracle_pool.close()
+        accuracy['oracle_workers'] = oracle_pool.workers
     if q_or is not None:
         q_gpu = field.electrostatic_point_charges.charges
         accuracy['charges_rel_err'] = float(np.max(np.abs(q_gpu - q_or)) / np.abs(q_or).max())
@@ -917,7 +917,7 @@ def run_combined(args):
     (phi, E, H) of the 3 electrodes and 4 coils at unit strength, then
     1,048,576 electrons at 5 keV (lognormal 2 %) traced through E + B by the
     tensor-core surrogate tracer; the plain BEM tracer on a slice for the
-    comparison and as the judge of the slice's endpoints; a sample re-traced
+    comparison and as the reference for the slice's endpoints; a sample re-traced
     by the CPU oracle."""
     import torch
     ws, rank, local = dist_info()
@@ -1052,23 +1052,23 @@ def run_combined(args):
     print(json.dumps(line), flush=True)
 
 
-def _batch_judge_init(items):
+def _batch_oracle_init(items):
     try:
         os.nice(10)
     except OSError:
         pass
     from oracle.oracle import Oracle
-    _JUDGE.update(oracle=Oracle('port'), items=items)
+    _ORACLE.update(oracle=Oracle('port'), items=items)
 
 
-def _batch_judge_one(job):
+def _batch_oracle_one(job):
     """The oracle's FP64 BEM trace of one particle of geometry g (the GPU
     solve's charges): its final state (t, x, y, z) and its position at the
     GPU trace's final time t_gpu (cubic Hermite between accepted states)."""
     g, state, atol, t_gpu = job
     from oracle.oracle import EM, hermite_position_at
-    q, jac, pos, bounds = _JUDGE['items'][g]
-    t, s = _JUDGE['oracle'].trace_bem(state[:3], state[3:], EM, q, jac, pos, bounds, atol, max_attempts=20000)
+    q, jac, pos, bounds = _ORACLE['items'][g]
+    t, s = _ORACLE['oracle'].trace_bem(state[:3], state[3:], EM, q, jac, pos, bounds, atol, max_attempts=20000)
     p = hermite_position_at(t, s, t_gpu)
     return (float(t[-1]), float(s[-1, 0]), float(s[-1, 1]), float(s[-1, 2]), float(p[0]), float(p[1]), float(p[2]),
             len(t))
@@ -1175,8 +1175,8 @@ def run_batch(args):
                 jobs.append((g, start_h[offs[g] + i], args.batch_atol, float(final[offs[g] + i, 0])))
                 where.append(offs[g] + i)
         t1 = time.perf_counter()
-        with mp.get_context('spawn').Pool(max(1, cores), _batch_judge_init, (items,)) as pool:
-            ref = np.array(pool.map(_batch_judge_one, jobs, chunksize=4))
+        with mp.get_context('spawn').Pool(max(1, cores), _batch_oracle_init, (items,)) as pool:
+            ref = np.array(pool.map(_batch_oracle_one, jobs, chunksize=4))
         got = final[where][:, :4]
         d_pos = np.max(np.abs(got[:, 1:] - ref[:, 1:4]), axis=1) * 1e9
         d_at = np.max(np.abs(got[:, 1:] - ref[:, 4:7]), axis=1) * 1e9
@@ -1251,13 +1251,13 @@ def main():
     ap.add_argument('--beam', default='wide', choices=sorted(BEAMS),
                     help='beam of the headline number (the other beam is measured beside it)')
     ap.add_argument('--check', type=int, default=2621,
-                    help='electrons of the headline beam judged by the CPU oracle (default: 1 %% of 262,144)')
+                    help='electrons of the headline beam re-traced by the CPU oracle (default: 1 %% of 262,144)')
     ap.add_argument('--check-other', type=int, default=256,
-                    help='electrons of the other beam judged by the CPU oracle')
+                    help='electrons of the other beam re-traced by the CPU oracle')
     ap.add_argument('--field-points', type=int, default=1 << 20,
                     help='points of the precision workload field evaluation')
     ap.add_argument('--field-check', type=int, default=4096,
-                    help='points of the precision workload field judged by the CPU oracle')
+                    help='points of the precision workload field re-evaluated by the CPU oracle')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
     ap.add_argument('--skip-fp64-lu', action='store_true',
                     help='--workload solve: time only the mixed solve (for profiles)')
