@@ -491,8 +491,8 @@ def load_probe():
 
 def measure_fp64_peak(B, torch):
     """FP64 FMA throughput (TFLOP/s) of this GPU, measured in this run: the
-    denominator of the FP64-bound kernels' rooflines (the driver's measured
-    peaks cover HBM and bf16 only)."""
+    denominator of the FP64-bound kernels' rooflines (MEASURED_PEAKS.json
+    covers HBM and bf16 only)."""
     probe = load_probe()
     out = torch.zeros(1, dtype=torch.float64, device='cuda')
     sms = B.num_sms()

@@ -1,5 +1,5 @@
 """Float64 NumPy restatement of the surrogate network's forward and backward
-passes -- TEST INFRASTRUCTURE ONLY (the checker of traceon_b200's tb_mlp_*
+passes -- TEST INFRASTRUCTURE ONLY (the test oracle of traceon_b200's tb_mlp_*
 kernels; nothing in the product imports it).
 
 It emulates the BF16 roundings of the GPU path at the same places (inputs,

@@ -1,8 +1,8 @@
 """CPU oracle for the Traceon radial BEM path -- TEST INFRASTRUCTURE ONLY.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py`` (its CPU
-baseline and reference arms) may import this module.  It is the checker of
-the CUDA library, never a fallback for it.
+baseline and reference arms) may import this module.  It is the test oracle
+of the CUDA library, never a fallback for it.
 
 Two CPU implementations are exposed through one interface:
 

@@ -1,7 +1,7 @@
 /*
  * traceon_oracle.c -- CPU restatement of Traceon's radial-symmetric BEM path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library in
+ * TEST INFRASTRUCTURE ONLY.  This file is the test oracle of the CUDA library in
  * traceon_b200/csrc: only tests/, __graft_entry__.smoke() and bench.py's CPU
  * baseline leg may load it.  The product path never calls it.
  *

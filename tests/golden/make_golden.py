@@ -9,7 +9,7 @@ The script copies the reference tree to a temporary directory, compiles its C
 backend there with the shipped flags (setup.py:8), stubs the two imports the
 path does not use (meshio: mesher.py:10, file I/O only; matplotlib), imports
 ``traceon`` and records its outputs through its own public API.  Nothing here
-runs on the GPU box; the .npz files it writes are committed.
+runs on a GPU; the .npz files it writes are committed.
 """
 from __future__ import annotations
 
