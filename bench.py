@@ -1265,9 +1265,9 @@ def main():
                     help='elements of the precision-workload solve measured beside the tracer (0: skip)')
     ap.add_argument('--ref-seconds', type=float, default=20.0)
     # DRAM bytes (read + write) of one full-size launch of the dominant kernel
-    # from an ncu capture of this workload (k_trace_surrogate_tc: 18.67 MB read
-    # + 4.96 MB written; see the profile summary of that kernel)
-    ap.add_argument('--traffic', type=float, default=23.63e6)
+    # from an ncu capture of this workload (k_trace_surrogate_tc, wide beam:
+    # 17.08 MB read + 3.07 MB written; see the profile summary of that kernel)
+    ap.add_argument('--traffic', type=float, default=20.15e6)
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
