@@ -308,7 +308,9 @@ def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True, fp64_
     ~U[-3, 3] kV.  GPU FP64 fill (+ singular self terms), then (a) the FP64
     LU with partial pivoting (numpy.linalg.solve's factorisation) and (b) the
     mixed solve (FP32 tensor-core LU of the equilibrated matrix, FP64
-    iterative refinement).  CUDA-event times; charges of (b) against (a).
+    iterative refinement; its lookahead width tuned first by
+    autotune.tune_solve_lookahead, then the median of three solves).
+    CUDA-event times; charges of (b) against (a).
     Then potential and field of the first right-hand side's charges at
     `field_points` points, and the axial derivatives of the same charges on
     2,000 z-points; FP64 rooflines of the fill, field and axial kernels
@@ -354,8 +356,11 @@ def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True, fp64_
         _, perm = B.dev_lu_factor(LU)
         return B.dev_lu_solve(LU, perm, F)
 
-    B.dev_solve_mixed(A, F)
-    mixed_ms, (Xm, iters, rel) = timed(lambda: B.dev_solve_mixed(A, F))
+    from traceon_b200 import autotune
+    lookahead = autotune.tune_solve_lookahead(A, F)  # warms the solve up too
+    runs = [timed(lambda: B.dev_solve_mixed(A, F)) for _ in range(3)]
+    mixed_ms = float(np.median([r[0] for r in runs]))
+    Xm, iters, rel = runs[-1][1]
     lib_ms = None
     if fp64_lu:
         lu64()
@@ -371,6 +376,9 @@ def precision_solve(n, nrhs=8, seed=2, field_points=1 << 20, fp64_lu=True, fp64_
     out = {'workload': f'einzel lens, {n} cubic elements, {nrhs} right-hand sides (electrode voltages U[-3,3] kV)',
            'fill_fp64_ms': fill_ms_total, 'fill_offdiagonal_ms': fill_ms, 'self_integrals_ms': self_ms,
            'solve_fp64_lu_ms': lu_ms, 'solve_mixed_ms': mixed_ms,
+           'solve_mixed_ms_runs': [r[0] for r in runs],
+           'lookahead_reserve_sms': lookahead['reserve_sms'],
+           'lookahead_tuning_ms': {str(k): v for k, v in lookahead['times_ms'].items()},
            'mixed_iterations': iters, 'mixed_last_correction': rel, 'charges_rel_err_vs_fp64': err,
            'solve_fp64_vendor_lu_ms': lib_ms,
            'speedup_vs_vendor_fp64_lu': lib_ms / mixed_ms if lib_ms else None,

@@ -71,6 +71,33 @@ def test_mixed_solve_lookahead_same_factors(cuda, reserve):
     assert it1 == it0 and torch.equal(X0, X1)
 
 
+def test_lookahead_tuner_sets_a_candidate(cuda):
+    """autotune.tune_solve_lookahead times every candidate width on the
+    matrix, leaves the fastest set, reuses it from its table for the same
+    size bucket, and the tuned solve gives the default's charges bit for
+    bit."""
+    import torch
+    from traceon_b200 import autotune
+    A, F = _matrix(cuda, 3000)
+    Ft = torch.as_tensor(F, device='cuda')
+    X0, _, _ = cuda.dev_solve_mixed(A, Ft)
+    old = cuda.set_solve_lookahead(-1)
+    autotune.clear()
+    try:
+        hit = autotune.tune_solve_lookahead(A, Ft)
+        sms = cuda.num_sms()
+        cands = {int(round(f * sms)) for f in autotune.LOOKAHEAD_FRACTIONS}
+        assert set(hit['times_ms']) == cands and hit['reserve_sms'] in cands
+        assert hit['times_ms'][hit['reserve_sms']] == min(hit['times_ms'].values())
+        assert cuda.set_solve_lookahead(hit['reserve_sms']) == hit['reserve_sms']
+        assert autotune.tune_solve_lookahead(A, Ft) is not None and len(autotune.table()) == 1
+        X1, _, _ = cuda.dev_solve_mixed(A, Ft)
+        assert torch.equal(X0, X1)
+    finally:
+        cuda.set_solve_lookahead(old)
+        autotune.clear()
+
+
 @pytest.mark.parametrize('nrhs', [1, 9, 16])
 def test_mixed_solve_right_hand_side_counts(cuda, nrhs):
     """1, 9 and 16 (the maximum) right-hand sides against LAPACK on a

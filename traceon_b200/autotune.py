@@ -14,6 +14,10 @@ the CTAs per SM of the persistent tile-task solve (1 or 2; each CTA holds
 two 64 x 64 FP64 tiles of shared memory) and the BEM team size of the
 multi-geometry trace (on a sample of the batch's particles).
 
+`tune_solve_lookahead` times the mixed solve at several lookahead widths
+(the SMs left to the next panel's factorisation while a second stream runs
+the rest of each trailing update; 0 = no lookahead) and sets the fastest.
+
 The table is the library's only mutable global state; `clear()` empties it.
 """
 from __future__ import annotations
@@ -125,4 +129,37 @@ def tune_batch_pipeline(pipe, sample: int = 4096) -> dict:
             _table[key] = hit
     bs.blocks_per_sm = hit['blocks_per_sm']
     pipe.opts.team_warps = hit['team_warps']
+    return hit
+
+
+LOOKAHEAD_FRACTIONS = (0.0, 1 / 10, 1 / 5, 3 / 10)
+
+
+def tune_solve_lookahead(A, F) -> dict:
+    """Measured lookahead width of the mixed solve (backend.dev_solve_mixed)
+    for the size of A (n x n, FP64, on the device) and the right-hand sides F:
+    one timed solve per candidate (each fraction of the SMs in
+    LOOKAHEAD_FRACTIONS, after one warm-up solve), the fastest set with
+    backend.set_solve_lookahead and kept per device and size bucket.  Returns
+    {'reserve_sms': r, 'times_ms': {r: ms}}."""
+    torch = B._torch()
+    n = A.shape[0]
+    key = ('solve_lookahead', torch.cuda.get_device_name(A.device), _bucket(n))
+    with _lock:
+        hit = _table.get(key)
+    if hit is None:
+        sms = B.num_sms()
+        cands = sorted({int(round(f * sms)) for f in LOOKAHEAD_FRACTIONS})
+        prev = B.set_solve_lookahead(-1)
+        times = {}
+        try:
+            for r in cands:
+                B.set_solve_lookahead(r)
+                times[r] = _time_ms(lambda: B.dev_solve_mixed(A, F), reps=1)
+        finally:
+            B.set_solve_lookahead(prev)
+        hit = {'reserve_sms': min(times, key=times.get), 'times_ms': times}
+        with _lock:
+            _table[key] = hit
+    B.set_solve_lookahead(hit['reserve_sms'])
     return hit

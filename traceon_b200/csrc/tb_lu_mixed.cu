@@ -32,6 +32,30 @@ namespace tb {
 
 constexpr int MX_NB = 64;
 
+// Programmatic dependent launch of the factorisation's kernels.  A kernel
+// launched by pdl_launch may be scheduled while its predecessor in the
+// stream is still finishing; it calls pdl_wait() before its first memory
+// access, and that returns once the predecessor grid has completed and its
+// writes are visible.  The data order of the stream is therefore unchanged;
+// only the gap between dependent launches is overlapped.  In a launch
+// without the attribute pdl_wait() returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+static void pdl_launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);  // errors: launch_status() / cudaGetLastError
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) k_diag_lu(T* __restrict__ A, int64_t lda, int64_t k0, int nb) {
   __shared__ T D[MX_NB][MX_NB + 1];
@@ -160,6 +184,7 @@ __global__ void __launch_bounds__(256)
 // unrolled (k and s are constants in every iteration, so no dynamic
 // register indexing).  Rows and columns beyond nb are the identity.
 __global__ void __launch_bounds__(256) k_diag_lu_f32(float* __restrict__ A, int64_t lda, int64_t k0, int nb) {
+  pdl_wait();
   __shared__ float colk[2][MX_NB], rowk[2][MX_NB];
   const int j = threadIdx.x % MX_NB, i0 = threadIdx.x / MX_NB;
   float v[16];
@@ -245,6 +270,7 @@ __device__ __forceinline__ void solve_vectors(float (*V)[TRSM_COLS], const float
 // loads of a thread are issued before the first use (one memory latency).
 __global__ void __launch_bounds__(TRSM_COLS)
     k_trsm_right_f32(float* __restrict__ A, int64_t lda, int64_t r0, int64_t r1, int64_t k0, int nb) {
+  pdl_wait();
   __shared__ __align__(16) float U[MX_NB][MX_NB];
   __shared__ float V[MX_NB][TRSM_COLS];  // V[m][r]: element m of row r of the CTA
   const int64_t rb = r0 + blockIdx.x * (int64_t)TRSM_COLS;
@@ -301,6 +327,7 @@ __global__ void __launch_bounds__(TRSM_COLS)
 // all loads of a thread are issued before the first use.
 __global__ void __launch_bounds__(TRSM_COLS)
     k_trsm_left_f32(float* __restrict__ A, int64_t lda, int64_t c0, int64_t c1, int64_t k0, int nb) {
+  pdl_wait();
   __shared__ __align__(16) float Lt[MX_NB][MX_NB];
   __shared__ float V[MX_NB][TRSM_COLS];  // V[i][c]: row i of column c of the CTA
   const int64_t cb = c0 + blockIdx.x * (int64_t)TRSM_COLS;
@@ -440,6 +467,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1)
                       const float* __restrict__ B, int64_t ldb, int64_t M, int64_t Nc, int K, int* __restrict__ err,
                       long long wait_cycles) {
   extern __shared__ __align__(1024) unsigned char gt_raw[];
+  pdl_wait();
   const uint32_t raw = tc::smem_u32(gt_raw);
   GemmSmem& sm = *reinterpret_cast<GemmSmem*>(gt_raw + (((raw + 1023u) & ~1023u) - raw));
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
@@ -558,11 +586,11 @@ static int gemm_sub_tf32x3(float* C, int64_t ldc, const float* A, int64_t lda, c
   const bool vec = (lda % 4 == 0) && (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0) &&
                    (reinterpret_cast<uintptr_t>(C) % 16 == 0);
   if (vec)
-    k_gemm_sub_tf32x3<true><<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err,
-                                                                    wait_limit());
+    pdl_launch(k_gemm_sub_tf32x3<true>, grid, dim3(GT_THREADS), GT_SMEM_BYTES, s, C, ldc, A, lda, B, ldb, M, Nc, K,
+               err, wait_limit());
   else
-    k_gemm_sub_tf32x3<false><<<grid, GT_THREADS, GT_SMEM_BYTES, s>>>(C, ldc, A, lda, B, ldb, M, Nc, K, err,
-                                                                     wait_limit());
+    pdl_launch(k_gemm_sub_tf32x3<false>, grid, dim3(GT_THREADS), GT_SMEM_BYTES, s, C, ldc, A, lda, B, ldb, M, Nc, K,
+               err, wait_limit());
   return launch_status();
 }
 
@@ -584,6 +612,7 @@ __device__ __forceinline__ void st_global_v4(uint8_t* p, const float (&v)[4]) {
 
 __global__ void __launch_bounds__(256) k_split_a(const float* __restrict__ A, int64_t lda, int64_t M, int K,
                                                 uint8_t* __restrict__ out) {
+  pdl_wait();
   const int nk = (K + GT_K - 1) / GT_K;
   const int kc = blockIdx.x;
   const int64_t mb = blockIdx.y;
@@ -602,6 +631,7 @@ __global__ void __launch_bounds__(256) k_split_a(const float* __restrict__ A, in
 
 __global__ void __launch_bounds__(256) k_split_b(const float* __restrict__ B, int64_t ldb, int K, int64_t N,
                                                 uint8_t* __restrict__ out) {
+  pdl_wait();
   const int nk = (K + GT_K - 1) / GT_K;
   const int kc = blockIdx.x;
   const int64_t nb = blockIdx.y;
@@ -652,6 +682,7 @@ __global__ void __launch_bounds__(GQ_THREADS, 1)
                        const uint8_t* __restrict__ Bpre, int64_t M, int64_t Nc, int nk, int64_t nbn, int64_t ntiles,
                        int* __restrict__ err, long long wait_cycles) {
   extern __shared__ __align__(1024) unsigned char gq_raw[];
+  pdl_wait();
   const uint32_t raw = tc::smem_u32(gq_raw);
   GemmPersistSmem& sm = *reinterpret_cast<GemmPersistSmem*>(gq_raw + (((raw + 1023u) & ~1023u) - raw));
   volatile int* fail = &sm.fail;
@@ -860,9 +891,8 @@ static int gemm_persist_part(float* C, int64_t ldc, const uint8_t* work, int64_t
   const int64_t nbn = nb1 - nb0, ntiles = (mb1 - mb0) * nbn;
   int64_t grid = max_ctas > 0 && max_ctas < num_sms() ? max_ctas : num_sms();
   if (grid > ntiles) grid = ntiles;
-  k_gemm_sub_persist<<<unsigned(grid), GQ_THREADS, GQ_SMEM_BYTES, s>>>(C + mb0 * GT_M * ldc + nb0 * GT_N, ldc, pa, pb,
-                                                                       nrows, ncols, nk, nbn, ntiles, err,
-                                                                       wait_limit());
+  pdl_launch(k_gemm_sub_persist, dim3(unsigned(grid)), dim3(GQ_THREADS), GQ_SMEM_BYTES, s,
+             C + mb0 * GT_M * ldc + nb0 * GT_N, ldc, pa, pb, nrows, ncols, nk, nbn, ntiles, err, wait_limit());
   return launch_status();
 }
 
@@ -936,14 +966,14 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
     const int64_t pe = p0 + TC_PANEL < N ? p0 + TC_PANEL : N;
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
       const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
-      k_diag_lu_f32<<<1, 256, 0, s>>>(A, lda, k0, nb);
+      pdl_launch(k_diag_lu_f32, dim3(1), dim3(256), 0, s, A, lda, k0, nb);
       const int64_t below = N - k0 - nb, right = pe - k0 - nb;
       if (below > 0)
-        k_trsm_right_f32<<<unsigned((below + TRSM_COLS - 1) / TRSM_COLS), TRSM_COLS, 0, s>>>(A, lda, k0 + nb, N, k0,
-                                                                                            nb);
+        pdl_launch(k_trsm_right_f32, dim3(unsigned((below + TRSM_COLS - 1) / TRSM_COLS)), dim3(TRSM_COLS), 0, s, A,
+                   lda, k0 + nb, N, k0, nb);
       if (right > 0) {
-        k_trsm_left_f32<<<unsigned((right + TRSM_COLS - 1) / TRSM_COLS), TRSM_COLS, 0, s>>>(A, lda, k0 + nb, pe, k0,
-                                                                                           nb);
+        pdl_launch(k_trsm_left_f32, dim3(unsigned((right + TRSM_COLS - 1) / TRSM_COLS)), dim3(TRSM_COLS), 0, s, A,
+                   lda, k0 + nb, pe, k0, nb);
         const int st = gemm_sub_tf32x3(A + (k0 + nb) * lda + k0 + nb, lda, A + (k0 + nb) * lda + k0, lda,
                                        A + k0 * lda + k0 + nb, lda, below, right, nb, err, s);
         if (st != OK) return st;
@@ -958,7 +988,8 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
     // row block right of the panel: U12 = L11^-1 A12, 64 rows at a time
     for (int64_t k0 = p0; k0 < pe; k0 += MX_NB) {
       const int nb = pe - k0 < MX_NB ? int(pe - k0) : MX_NB;
-      k_trsm_left_f32<<<unsigned((rest + TRSM_COLS - 1) / TRSM_COLS), TRSM_COLS, 0, s>>>(A, lda, pe, N, k0, nb);
+      pdl_launch(k_trsm_left_f32, dim3(unsigned((rest + TRSM_COLS - 1) / TRSM_COLS)), dim3(TRSM_COLS), 0, s, A, lda,
+                 pe, N, k0, nb);
       const int64_t rows = pe - k0 - nb;
       if (rows > 0) {
         const int st = gemm_sub_tf32x3(A + (k0 + nb) * lda + pe, lda, A + (k0 + nb) * lda + k0, lda, A + k0 * lda + pe,
@@ -976,8 +1007,8 @@ static int lu_nopiv_f32_tc(float* A, int64_t lda, int64_t N, int* err, uint8_t* 
     uint8_t* wb = w + mbk * nk * (int64_t)PA_BLOCK;
     // split operands: L21 and the next panel's columns of U12 here; the rest
     // of U12 on the side stream when it runs the rest of the update
-    k_split_a<<<dim3(unsigned(nk), unsigned(mbk)), 256, 0, s>>>(L21, lda, rest, K, w);
-    k_split_b<<<dim3(unsigned(nk), 1u), 256, 0, s>>>(U12, lda, K, rest < GT_N ? rest : GT_N, wb);
+    pdl_launch(k_split_a, dim3(unsigned(nk), unsigned(mbk)), dim3(256), 0, s, L21, lda, rest, K, w);
+    pdl_launch(k_split_b, dim3(unsigned(nk), 1u), dim3(256), 0, s, U12, lda, K, rest < GT_N ? rest : GT_N, wb);
     if (bottom_pending) {  // the update below reads rows `bottom` updates
       if (cudaStreamWaitEvent(s, ss->bottom, 0) != cudaSuccess) return CUDA_ERR;
       bottom_pending = false;

@@ -58,6 +58,25 @@ __device__ __forceinline__ uint32_t silu2_bf16_half(float h0, float h1) {
   __nv_bfloat162 v = __floats2bfloat162_rn(fmaf(h0, tanh_fast(h0), h0), fmaf(h1, tanh_fast(h1), h1));
   return *reinterpret_cast<uint32_t*>(&v);
 }
+// The same from the accumulators a0, a1 and the halved biases b0, b1
+// (h = a + b), with the additions and the multiply-adds as packed FP32x2
+// operations (add.rn.f32x2, fma.rn.f32x2: each half rounded exactly as the
+// scalar operation, so the result equals silu2_bf16_half(a0 + b0, a1 + b1)).
+__device__ __forceinline__ uint32_t silu2_bf16_half_bias(float a0, float a1, float b0, float b1) {
+  float h0 = a0, h1 = a1;
+  asm("{.reg .b64 x, y;\n mov.b64 x, {%0, %1};\n mov.b64 y, {%2, %3};\n add.rn.f32x2 x, x, y;\n"
+      " mov.b64 {%0, %1}, x;}"
+      : "+f"(h0), "+f"(h1)
+      : "f"(b0), "f"(b1));
+  const float t0 = tanh_fast(h0), t1 = tanh_fast(h1);
+  float y0 = h0, y1 = h1;
+  asm("{.reg .b64 x, y, z;\n mov.b64 x, {%2, %3};\n mov.b64 y, {%4, %5};\n mov.b64 z, {%0, %1};\n"
+      " fma.rn.f32x2 z, x, y, z;\n mov.b64 {%0, %1}, z;}"
+      : "+f"(y0), "+f"(y1)
+      : "f"(h0), "f"(h1), "f"(t0), "f"(t1));
+  __nv_bfloat162 v = __floats2bfloat162_rn(y0, y1);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
 // BF16 pair {silu(z0), silu(z1)} (z0 in the low half).
 __device__ __forceinline__ uint32_t silu2_bf16(float z0, float z1) { return silu2_bf16_half(0.5f * z0, 0.5f * z1); }
 __device__ __forceinline__ float silu_grad(float z) {

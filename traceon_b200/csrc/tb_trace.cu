@@ -1205,8 +1205,8 @@ struct TcEngine {
           uint32_t q[8];
 #pragma unroll
           for (int j = 0; j < 8; j++)
-            q[j] = silu2_bf16_half(__uint_as_float(cur[2 * j]) + bias[16 * c + 2 * j],
-                                   __uint_as_float(cur[2 * j + 1]) + bias[16 * c + 2 * j + 1]);
+            q[j] = silu2_bf16_half_bias(__uint_as_float(cur[2 * j]), __uint_as_float(cur[2 * j + 1]),
+                                        bias[16 * c + 2 * j], bias[16 * c + 2 * j + 1]);
           // next layer's K = 16c .. 16c + 15: atom c / 4, chunks 2 (c % 4), 2 (c % 4) + 1
           const uint32_t base = act + (c >> 2) * TC_ATOM;
           tc::st_shared_v4(base + tc::sw128(row, 2 * (c & 3)), q[0], q[1], q[2], q[3]);
