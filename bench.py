@@ -1274,8 +1274,8 @@ def main():
     ap.add_argument('--ref-seconds', type=float, default=20.0)
     # DRAM bytes (read + write) of one full-size launch of the dominant kernel
     # from an ncu capture of this workload (k_trace_surrogate_tc, wide beam:
-    # 17.08 MB read + 3.07 MB written; see the profile summary of that kernel)
-    ap.add_argument('--traffic', type=float, default=20.15e6)
+    # 17.06 MB read + 2.80 MB written; see the profile summary of that kernel)
+    ap.add_argument('--traffic', type=float, default=19.86e6)
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
