@@ -981,7 +981,8 @@ def run_combined(args):
         _log(T0, f'{name} system filled and solved: {solve[name]}')
     field = fields[0] + fields[1]
     t0 = time.perf_counter()
-    tr = SurrogateTrainer(geo, electrodes=geo.names[:3], magnetizable={'pole': 1000.0}, coils=cl)
+    tr = SurrogateTrainer(geo, r_max=args.combined_r_max, electrodes=geo.names[:3], magnetizable={'pole': 1000.0},
+                          coils=cl)
     _log(T0, 'unit fields and axial tables of the 7 sources')
     model, info = tr.train(n_samples=args.train_samples, steps=args.train_steps, batch=8192, seed=0)
     _log(T0, f'surrogate trained: holdout mse {info["holdout_mse"]:.3g}')
@@ -1048,7 +1049,7 @@ def run_combined(args):
                                    f'(0 / 3 kV / 0) in an iron pole piece (mu_r 1000) of {args.combined_n} elements, '
                                    f'4 coils {np.round(cl.coil_current).tolist()} A-turns; {E} electrons at 5 keV '
                                    f'(lognormal 2 %), r0 <= 0.2 mm, +-10 mrad, RKF45 atol 1e-10 m',
-                       'electrons_per_step': E},
+                       'electrons_per_step': E, 'surrogate_r_max_m': args.combined_r_max},
             'solve': solve, 'surrogate_train_s': train_s, 'surrogate_holdout_mse': info['holdout_mse'],
             'plain_bem': plain, 'speedup_vs_plain_bem': value / plain['value'],
             'roofline': {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
@@ -1240,6 +1241,8 @@ def main():
                          'combined: the combined electro-magnetostatic workload')
     ap.add_argument('--combined-n', type=int, default=16384, help='elements of each part of the combined lens')
     ap.add_argument('--combined-electrons', type=int, default=1 << 20)
+    ap.add_argument('--combined-r-max', type=float, default=0.95e-3,
+                    help='radius of the combined surrogate\'s domain (m); points beyond it use the exact BEM sums')
     ap.add_argument('--combined-bem-electrons', type=int, default=2048)
     ap.add_argument('--combined-check', type=int, default=16,
                     help='electrons of the combined workload re-traced by the CPU oracle (~1.5 min each per core)')
