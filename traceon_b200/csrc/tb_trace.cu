@@ -665,12 +665,12 @@ __device__ __noinline__ BemSums bem_sums(const TraceParams& P, double r0, double
   double Sr = 0, Sz = 0, dummy = 0;
   const double* er = P.esrc;
   // The magnetic variant (the combined workload's fallback, two systems of
-  // rings per point) interleaves two rings per iteration: twice the
-  // independent work for the few warps that run it.  The electrostatic
-  // variant stays rolled, which keeps its callers' registers (the headline
-  // tracer) free of the extra spills.
+  // rings per point) unrolls four rings per iteration: more independent
+  // work for the few warps that run it (the accumulation order is
+  // unchanged).  The electrostatic variant stays rolled, which keeps its
+  // callers' registers (the headline tracer) free of the extra spills.
   if (MAG) {
-#pragma unroll 2
+#pragma unroll 4
     for (int64_t j = first; j < P.ne; j += stride)
       ring_field_acc<false>(r0, z, er[j], er[P.ne + j], er[2 * P.ne + j], Sr, Sz, dummy);
   } else {
@@ -682,7 +682,7 @@ __device__ __noinline__ BemSums bem_sums(const TraceParams& P, double r0, double
   if (MAG) {
     double Mr = 0, Mz = 0, Cr = 0, Cz = 0;
     const double* mr = P.msrc;
-#pragma unroll 2
+#pragma unroll 4
     for (int64_t j = first; j < P.nm; j += stride)
       ring_field_acc<false>(r0, z, mr[j], mr[P.nm + j], mr[2 * P.nm + j], Mr, Mz, dummy);
     const double* cr = P.csrc;
