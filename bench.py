@@ -1022,6 +1022,14 @@ def run_combined(args):
     evals = float(counters[:, 1].sum()) * 6
     peak = read_peaks().get('bf16_tflops') or FALLBACK_BF16_TFLOPS
     achieved = evals * MLP_FLOP_PER_EVAL / (np.mean(ms) * 1e-3) / 1e12
+    # the exact sums of the fallback points: every point sums the
+    # electrostatic and the magnetizable rings (16 per element), FP64
+    fallback_pairs = float(counters[:, 2].sum()) * 16.0 * (len(se.vertices) + len(sm.vertices))
+    fp64_peak = measure_fp64_peak(B, torch)
+    fallback_roofline = fp64_roofline(fallback_pairs, FLOP_FIELD_PAIR, float(np.mean(ms)), fp64_peak,
+                                      'k_trace_surrogate_tc<MAG> (group BEM sums of the fallback points)',
+                                      'ring-pair field evaluations (+ 1 log, 1 rsqrt, 1 reciprocal each); '
+                                      'the current rings are not counted')
     if args.combined_check > 0:
         from oracle.oracle import Oracle, EM, hermite_plane_crossing
         from concurrent.futures import ThreadPoolExecutor
@@ -1055,6 +1063,7 @@ def run_combined(args):
             'roofline': {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
                          'frac': achieved / peak, 'kernel': 'k_trace_surrogate_tc<MAG>',
                          'flop_per_unit': MLP_FLOP_PER_EVAL, 'units_per_launch': evals},
+            'roofline_fallback_fp64': fallback_roofline,
             'trace_stats': {'status_exited': int((status == 0).sum()), 'attempts_mean': float(counters[:, 1].mean()),
                             'bem_fallback_evals': int(counters[:, 2].sum())},
             'accuracy': acc, 'clocks': clk.summary()}
