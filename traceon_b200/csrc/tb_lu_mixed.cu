@@ -11,8 +11,9 @@
 // N = 1000), which is what lets FP32 factors converge under refinement.
 //
 // The mixed solve factors with lu_nopiv_f32_tc (256-column panels, trailing
-// updates on the tensor cores, below); tb_lu_nopiv_f32 / _f64 keep the plain
-// one-level blocking.  Blocked right-looking factorisation, per panel of NB
+// updates on the tensor cores, below; its kernels are launched as
+// programmatic dependents of one another, see pdl_launch); tb_lu_nopiv_f32 /
+// _f64 keep the plain one-level blocking.  Blocked right-looking factorisation, per panel of NB
 // columns:
 //   k_diag_lu      one CTA factors the NB x NB diagonal block in shared memory
 //   k_trsm_right   L21 = A21 U11^-1   (one thread per row)
