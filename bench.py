@@ -206,8 +206,12 @@ def endpoint_errors_nm(plane, ref_xy):
     """Max and p99 over electrons of max(|dx|, |dy|) at the exit plane, nm;
     electrons without a crossing on either side count as infinite."""
     d = np.max(np.abs(plane[:, 1:3] - ref_xy), axis=1) * 1e9
-    d = np.where(np.isfinite(d), d, np.inf)
-    return {'max_nm': float(np.max(d)), 'p99_nm': float(np.percentile(d, 99)), 'n': int(len(d)),
+    finite = np.isfinite(d)
+    d = np.where(finite, d, np.inf)
+    # with missing crossings, the nearest-rank percentile (interpolating
+    # between infinities would give NaN)
+    p99 = np.percentile(d, 99) if finite.all() else np.percentile(d, 99, method='higher')
+    return {'max_nm': float(np.max(d)), 'p99_nm': float(p99), 'n': int(len(d)),
             'within_1nm': int(np.sum(d <= 1.0))}
 
 
